@@ -1,0 +1,593 @@
+// engine.cu -- host orchestration of libjv (see engine.hpp).
+//
+// The time loops restate the reference's blend drivers:
+//   modelling      FD/fdtd3d_3_model_mpi_blend/fdtd3d_blend_elastic_model_mpi_meat.hpp:44-88
+//   RTM forward    same file :125-155 (VOWR pack after the CPML stress update)
+//   time reverse   RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:64-113
+// (FD = src/jarvis_cpp/jarvis/.jarvis_2_app/.jarvis_3_seismology/elastic_1_fdtd3d_model_mpi,
+//  RTM = .../elastic_1_rtm3d_model_mpi, relative to the reference root).
+#include "engine.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace jv {
+
+// ------------------------------------------------------------ helpers
+
+void diff_coeff(int order, double *c) {
+    for (int n = 0; n < order; n++) {
+        double a1 = 1, a2 = 1, a3 = 1;
+        for (int i = 0; i < order; i++) {
+            if (i != n) a1 = a1 * (2 * i + 1) * (2 * i + 1);
+            if (i < n) a2 = a2 * ((2 * n + 1) * (2 * n + 1) - (2 * i + 1) * (2 * i + 1));
+            if (i > n) a3 = a3 * ((2 * i + 1) * (2 * i + 1) - (2 * n + 1) * (2 * n + 1));
+        }
+        a1 = a1 * ((n % 2) ? -1.0 : 1.0);
+        c[n] = a1 / ((2 * n + 1) * a2 * a3);
+    }
+}
+
+int gap_num(float l, float r, float d) {
+    int n_l, n_r;
+    float v = 1.0f / d;
+    if (l > 0) n_l = (int)(l * v + 0.125f);
+    else n_l = (int)(l * v - 0.125f);
+    if (r > 0) n_r = (int)(r * v + 0.125f);
+    else n_r = (int)(r * v - 0.125f);
+    return n_r - n_l;
+}
+
+int ntime(float T, float dt) {
+    volatile float q = T / dt;
+    return (int)std::ceil(q);
+}
+
+void ricker(int nt, float fm, float dt, float *w) {
+    const double pi = 3.14159265358979323846;
+    float dura = 1.3f / fm;
+    volatile float q = dura / dt + 0.5f;
+    int n0 = (int)std::floor(q);
+    for (int i = 0; i < nt; i++) {
+        volatile float t = (float)(i - n0) * dt;
+        double a = pi * (double)fm * (double)t;
+        double a2 = a * a;
+        w[i] = (float)(1.0e4 * (1.0 - 2.0 * a2) * std::exp(-a2));
+    }
+}
+
+static long long round_up(long long v, long long a) { return (v + a - 1) / a * a; }
+
+Status Engine::cu(cudaError_t e, const char *what) const {
+    Status s;
+    if (e != cudaSuccess) {
+        s.code = (e == cudaErrorMemoryAllocation) ? JV_ENOMEM : JV_ECUDA;
+        s.msg = std::string(what) + ": " + cudaGetErrorString(e);
+    }
+    return s;
+}
+
+static Status bad(jv_status c, const std::string &m) {
+    Status s;
+    s.code = c;
+    s.msg = m;
+    return s;
+}
+
+#define JV_TRY(expr)                  \
+    do {                              \
+        Status _s = (expr);           \
+        if (!_s) return _s;           \
+    } while (0)
+#define JV_CU(expr) JV_TRY(cu((expr), #expr))
+#define JV_K(expr) JV_TRY(cu((cudaError_t)(expr), #expr))
+
+Status Engine::alloc(void **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) return Status{};
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return bad(JV_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    allocs_.push_back(*p);
+    dev_bytes_ += bytes;
+    return Status{};
+}
+
+Engine::~Engine() {
+    if (stream_) {
+        cudaSetDevice(dev_);
+        cudaStreamSynchronize(stream_);
+    }
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    for (void *p : allocs_) cudaFree(p);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+// ------------------------------------------------------------ creation
+
+Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, const float *rho, float dt, float fm,
+                      int nt, const jv_options &opt, Engine **out) {
+    *out = nullptr;
+    if (grid.nx < 8 || grid.ny < 8 || grid.nz < 8)
+        return bad(JV_EINVAL, "gridphy must have at least 8 cells per axis");
+    if (grid.pml < kPhyHalf) return bad(JV_EINVAL, "pml_num must be >= 4 (the 8th-order stencil reaches 4 cells)");
+    if (!(grid.dx > 0) || !(grid.dy > 0) || !(grid.dz > 0)) return bad(JV_EINVAL, "grid spacing must be > 0");
+    if (!(dt > 0) || !(fm > 0)) return bad(JV_EINVAL, "dt and fm must be > 0");
+    if (nt < 1) return bad(JV_EINVAL, "nt must be >= 1");
+    if (!vp || !vs || !rho) return bad(JV_EINVAL, "model arrays must not be NULL");
+    int rw = opt.rec_width == 0 ? 1 : opt.rec_width;
+    if (rw < 1 || rw > kPhyHalf || rw > grid.pml) return bad(JV_EINVAL, "rec_width must be in 1..4 and <= pml_num");
+    if (opt.precision != JV_FP32) return bad(JV_ENOTSUP, "only FP32 wavefield storage is built");
+    long long next = (long long)(grid.nx + 2 * grid.pml) * (grid.ny + 2 * grid.pml) * (grid.nz + 2 * grid.pml);
+    if (next > (1LL << 34)) return bad(JV_EINVAL, "grid too large");
+
+    Engine *E = new Engine();
+    E->grid_ = grid;
+    E->opt_ = opt;
+    E->opt_.rec_width = rw;
+    if (E->opt_.graph_steps <= 0) E->opt_.graph_steps = 32;
+    E->dt_ = dt;
+    E->fm_ = fm;
+    E->nt_ = nt;
+    E->dev_ = opt.device;
+    Status s = E->alloc_all(vp, vs, rho);
+    if (!s) {
+        delete E;
+        return s;
+    }
+    *out = E;
+    return Status{};
+}
+
+Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
+    JV_CU(cudaSetDevice(dev_));
+    JV_CU(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    JV_CU(cudaEventCreate(&ev0_));
+    JV_CU(cudaEventCreate(&ev1_));
+
+    // coefficient tables (universal constants; uploaded per device)
+    float list[5][4] = {};
+    for (int o = 1; o <= 4; o++) {
+        double c[4];
+        diff_coeff(o, c);
+        for (int i = 0; i < o; i++) list[o][i] = (float)c[i];
+    }
+    double c2[2];
+    diff_coeff(2, c2);
+    float dc2[2] = {(float)c2[0], (float)c2[1]};
+    JV_K(upload_coefficients(list, dc2));
+
+    // pitched gridext layout
+    const int m = grid_.pml;
+    g_.m = m;
+    g_.px = grid_.nx; g_.py = grid_.ny; g_.pz = grid_.nz;
+    g_.nx = grid_.nx + 2 * m; g_.ny = grid_.ny + 2 * m; g_.nz = grid_.nz + 2 * m;
+    g_.xoff = (32 - (m % 32)) % 32;
+    g_.sy = round_up(g_.xoff + g_.nx, 32);
+    g_.sz = g_.sy * g_.ny;
+    g_.dx = grid_.dx; g_.dy = grid_.dy; g_.dz = grid_.dz;
+    field_elems_ = (size_t)round_up(g_.sz * g_.nz + 64, 64);
+
+    // model
+    void *p;
+    JV_TRY(alloc(&p, 4 * field_elems_ * sizeof(float)));
+    float *mb = (float *)p;
+    vp_ = mb; rho_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    float *tmp = nullptr;
+    JV_CU(cudaMalloc(&tmp, 3 * nphy * sizeof(float)));
+    cudaError_t e1 = cudaMemcpyAsync(tmp, vp, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    cudaError_t e2 = cudaMemcpyAsync(tmp + nphy, vs, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    cudaError_t e3 = cudaMemcpyAsync(tmp + 2 * nphy, rho, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    int ek = k_model_prep(g_, tmp, tmp + nphy, tmp + 2 * nphy, vp_, rho_, lam_, mu_, stream_);
+    cudaError_t e4 = cudaStreamSynchronize(stream_);
+    cudaFree(tmp);
+    JV_CU(e1); JV_CU(e2); JV_CU(e3); JV_K(ek); JV_CU(e4);
+
+    // forward/backward wavefield (13 components, one arena)
+    JV_TRY(alloc(&p, kNumFld * field_elems_ * sizeof(float)));
+    for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + f * field_elems_;
+
+    // CPML slabs for one wavefield
+    auto make_cpml = [&](CpmlDev &c) -> Status {
+        const int NX = g_.nx, NY = g_.ny, NZ = g_.nz;
+        int bx[6][6] = {
+            {2, NX - 2, 2, NY - 2, 2, m},           {2, NX - 2, 2, NY - 2, NZ - m, NZ - 2},
+            {2, NX - 2, 2, m, m, NZ - m},           {2, NX - 2, NY - m, NY - 2, m, NZ - m},
+            {2, m, m, NY - m, m, NZ - m},           {NX - m, NX - 2, m, NY - m, m, NZ - m},
+        };
+        int na[6] = {3, 3, 2, 2, 1, 1};
+        long long first = 0, psi_total = 0;
+        for (int s = 0; s < 6; s++) {
+            SlabDev &S = c.s[s];
+            S.x0 = bx[s][0]; S.x1 = bx[s][1]; S.y0 = bx[s][2]; S.y1 = bx[s][3]; S.z0 = bx[s][4]; S.z1 = bx[s][5];
+            S.naxes = na[s];
+            S.ncell = (long long)(S.x1 - S.x0) * (S.y1 - S.y0) * (S.z1 - S.z0);
+            if (S.ncell < 0) S.ncell = 0;
+            S.first = first;
+            first += S.ncell;
+            psi_total += 6LL * S.naxes * S.ncell;
+        }
+        c.total = first;
+        void *q;
+        JV_TRY(alloc(&q, (size_t)psi_total * sizeof(float)));
+        long long off = 0;
+        for (int s = 0; s < 6; s++) {
+            c.s[s].psi = (float *)q + off;
+            off += 6LL * c.s[s].naxes * c.s[s].ncell;
+        }
+        c.fm = fm_;
+        c.dt = dt_;
+        c.l10x7 = std::log10(1.0f / 0.001f) * 7.0f;
+        c.N = (float)(m - kPmlHalf);
+        c.twoNdx = 2.0f * c.N * grid_.dx;
+        c.twoNdy = 2.0f * c.N * grid_.dy;
+        c.twoNdz = 2.0f * c.N * grid_.dz;
+        c.alpha_max = (float)(3.14159265358979323846 * (double)fm_);
+        return Status{};
+    };
+    JV_TRY(make_cpml(cpF_));
+
+    // wavelet and step state
+    std::vector<float> w(nt_);
+    ricker(nt_, fm_, dt_, w.data());
+    JV_TRY(alloc(&p, nt_ * sizeof(float)));
+    wavelet_ = (float *)p;
+    JV_CU(cudaMemcpy(wavelet_, w.data(), nt_ * sizeof(float), cudaMemcpyHostToDevice));
+    JV_TRY(alloc(&p, sizeof(StepState)));
+    st_ = (StepState *)p;
+
+    // images
+    JV_TRY(alloc(&p, 5 * nphy * sizeof(double)));
+    double *ib = (double *)p;
+    img_.ip = ib; img_.pp = ib + nphy; img_.ps = ib + 2 * nphy; img_.sp = ib + 3 * nphy; img_.ss = ib + 4 * nphy;
+    JV_CU(cudaMemset(ib, 0, 5 * nphy * sizeof(double)));
+
+    // VOWR face boxes (FD/fdtd3d_0_base_module/fdtd3d_base_5_wave_recon_meat.hpp:19-30;
+    // face frames .jarvis_0_meta/.jarvis_3_operator/jarvis_1_mpicu_halo_store_operator_meat.hpp:129-134)
+    {
+        const int r = opt_.rec_width;
+        const int W[10][6] = {
+            {r - 1, r, r - 1, r, r, r - 1}, {r - 1, r, r, r - 1, r - 1, r}, {r, r - 1, r - 1, r, r - 1, r},
+            {0, 0, 0, 0, r - 1, r},         {0, 0, r - 1, r, 0, 0},         {r - 1, r, 0, 0, 0, 0},
+            {r - 1, r, r - 1, r, r - 1, r}, {0, 0, r, r - 1, r, r - 1},     {r, r - 1, 0, 0, r, r - 1},
+            {r, r - 1, r, r - 1, 0, 0}};
+        const int flds[10] = {VX, VY, VZ, SXX, SYY, SZZ, SAU, SXY, SXZ, SYZ};
+        const int X0 = m, X1 = m + g_.px, Y0 = m, Y1 = m + g_.py, Z0 = m, Z1 = m + g_.pz;
+        long long off = 0, blk = 0;
+        for (int f = 0; f < 10; f++)
+            for (int face = 0; face < 6; face++) {
+                int wd = W[f][face];
+                if (wd <= 0) continue;
+                int x0 = X0, x1 = X1, y0 = Y0, y1 = Y1, z0 = Z0, z1 = Z1;
+                switch (face) {
+                case 0: z0 = Z0 - wd; z1 = Z0; break;
+                case 1: z0 = Z1; z1 = Z1 + wd; break;
+                case 2: y0 = Y0 - wd; y1 = Y0; break;
+                case 3: y0 = Y1; y1 = Y1 + wd; break;
+                case 4: x0 = X0 - wd; x1 = X0; break;
+                default: x0 = X1; x1 = X1 + wd; break;
+                }
+                SegDev sg{};
+                sg.fld = flds[f];
+                sg.x0 = x0; sg.nxb = x1 - x0; sg.y0 = y0; sg.nyb = y1 - y0; sg.z0 = z0; sg.nzb = z1 - z0;
+                sg.off = off;
+                sg.nblk_first = blk;
+                long long cnt = (long long)sg.nxb * sg.nyb * sg.nzb;
+                off += cnt;
+                blk += (cnt + 255) / 256;
+                segs_h_.push_back(sg);
+            }
+        per_step_ = off;
+        seg_blocks_ = blk;
+        if (!segs_h_.empty()) {
+            JV_TRY(alloc(&p, segs_h_.size() * sizeof(SegDev)));
+            segs_d_ = (SegDev *)p;
+            JV_CU(cudaMemcpy(segs_d_, segs_h_.data(), segs_h_.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+        }
+        nslot_ = nt_ > 1 ? nt_ - 1 : 0;
+    }
+    return Status{};
+}
+
+Status Engine::set_geometry(int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz) {
+    if (n_shot < 0 || n_recv < 0 || (n_shot > 0 && !shot_xyz) || (n_recv > 0 && !recv_xyz))
+        return bad(JV_EINVAL, "bad geometry arguments");
+    JV_CU(cudaSetDevice(dev_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    shots_.assign(shot_xyz, shot_xyz + 3 * (size_t)n_shot);
+    nshot_ = n_shot;
+    // receivers inside gridphy, file order (jarvis_device_geometry_meat.hpp:98-127)
+    const float rx = (float)(grid_.nx - 1) * grid_.dx, ry = (float)(grid_.ny - 1) * grid_.dy,
+                rz = (float)(grid_.nz - 1) * grid_.dz;
+    const float lx = -(float)grid_.pml * grid_.dx, ly = -(float)grid_.pml * grid_.dy, lz = -(float)grid_.pml * grid_.dz;
+    rec_h_.clear();
+    for (int r = 0; r < n_recv; r++) {
+        const float *q = recv_xyz + 3 * r;
+        if (!(q[0] >= 0.0f && q[0] <= rx && q[1] >= 0.0f && q[1] <= ry && q[2] >= 0.0f && q[2] <= rz)) continue;
+        int i = gap_num(lx, q[0], grid_.dx), j = gap_num(ly, q[1], grid_.dy), k = gap_num(lz, q[2], grid_.dz);
+        rec_h_.push_back(g_.xoff + i + g_.sy * j + g_.sz * k);
+    }
+    nrec_ = (int)rec_h_.size();
+    if (rec_d_) {
+        cudaFree(rec_d_);
+        for (auto &a : allocs_)
+            if (a == rec_d_) a = nullptr;
+        rec_d_ = nullptr;
+    }
+    if (nrec_ > 0) {
+        void *p;
+        JV_TRY(alloc(&p, nrec_ * sizeof(long long)));
+        rec_d_ = (long long *)p;
+        JV_CU(cudaMemcpy(rec_d_, rec_h_.data(), nrec_ * sizeof(long long), cudaMemcpyHostToDevice));
+    }
+    // the graphs bake the receiver count and pointer
+    for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
+    return Status{};
+}
+
+Status Engine::check_shot(int shot, long long *src) const {
+    if (shot < 0 || shot >= nshot_) return bad(JV_EINVAL, "shot index out of range");
+    const float *q = &shots_[3 * (size_t)shot];
+    const float rx = (float)(grid_.nx - 1) * grid_.dx, ry = (float)(grid_.ny - 1) * grid_.dy,
+                rz = (float)(grid_.nz - 1) * grid_.dz;
+    if (!(q[0] >= 0.0f && q[0] <= rx && q[1] >= 0.0f && q[1] <= ry && q[2] >= 0.0f && q[2] <= rz))
+        return bad(JV_EINVAL, "shot " + std::to_string(shot) + " lies outside gridphy");
+    const float lx = -(float)grid_.pml * grid_.dx, ly = -(float)grid_.pml * grid_.dy, lz = -(float)grid_.pml * grid_.dz;
+    int i = gap_num(lx, q[0], grid_.dx), j = gap_num(ly, q[1], grid_.dy), k = gap_num(lz, q[2], grid_.dz);
+    *src = g_.xoff + i + g_.sy * j + g_.sz * k;
+    return Status{};
+}
+
+Status Engine::set_state(int it, long long src, float *const tr[3], const float *const obs[3]) {
+    StepState h{};
+    h.it = it;
+    h.src = src;
+    for (int q = 0; q < 3; q++) {
+        h.tr[q] = tr ? tr[q] : nullptr;
+        h.obs[q] = obs ? obs[q] : nullptr;
+    }
+    JV_CU(cudaMemcpyAsync(st_, &h, sizeof(h), cudaMemcpyHostToDevice, stream_));
+    return Status{};
+}
+
+Status Engine::zero_wave(const WaveDev &w, int nfld) {
+    JV_CU(cudaMemsetAsync(w.f[0], 0, (size_t)nfld * field_elems_ * sizeof(float), stream_));
+    return Status{};
+}
+
+Status Engine::zero_psi(const CpmlDev &c) {
+    long long n = 0;
+    for (int s = 0; s < 6; s++) n += 6LL * c.s[s].naxes * c.s[s].ncell;
+    if (n > 0) JV_CU(cudaMemsetAsync(c.s[0].psi, 0, (size_t)n * sizeof(float), stream_));
+    return Status{};
+}
+
+// ------------------------------------------------------------ stepping
+
+Status Engine::launch_step(int kind) {
+    void *s = (void *)stream_;
+    const float dt = dt_;
+    const int rw = opt_.rec_width;
+    switch (kind) {
+    case kStepModel:
+        JV_K(k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
+        JV_K(k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_K(k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, s));
+        JV_K(k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_K(k_record(F_, rec_d_, nrec_, nt_, st_, s));
+        JV_K(k_step_advance(st_, +1, s));
+        break;
+    case kStepRtmFwd:
+        JV_K(k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
+        JV_K(k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_K(k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, s));
+        JV_K(k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, 0, nslot_, 1, 0, s));
+        JV_K(k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_K(k_step_advance(st_, +1, s));
+        break;
+    case kStepRtmRev:
+        // UPDATE 1: source subtraction (fused) + backward stress, receiver
+        // injection + reverse velocity, stress boundary layers of step it-1
+        JV_K(k_inject_rec(R_, rec_d_, nrec_, nt_, st_, s));
+        JV_K(k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, s));
+        JV_K(k_vel_pml(g_, cpR_, R_, rho_, vp_, s));
+        JV_K(k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_K(k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 2, s));
+        // UPDATE 2: backward velocity with the imaging condition fused,
+        // reverse stress, velocity boundary layers of step it-1
+        JV_K(k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, s));
+        JV_K(k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, s));
+        JV_K(k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_K(k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 1, s));
+        JV_K(k_step_advance(st_, -1, s));
+        break;
+    default: return bad(JV_EINVAL, "unknown step kind");
+    }
+    return Status{};
+}
+
+Status Engine::run_loop(int kind, int nsteps) {
+    if (nsteps <= 0) return Status{};
+    if (!opt_.use_graphs) {
+        for (int i = 0; i < nsteps; i++) JV_TRY(launch_step(kind));
+        return Status{};
+    }
+    const int S = opt_.graph_steps;
+    auto get = [&](int steps, cudaGraphExec_t *ex) -> Status {
+        long long key = (long long)kind * 1000000LL + steps;
+        auto it = graphs_.find(key);
+        if (it != graphs_.end()) {
+            *ex = it->second;
+            return Status{};
+        }
+        cudaGraph_t gr;
+        JV_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        Status st;
+        for (int i = 0; i < steps && st; i++) st = launch_step(kind);
+        cudaError_t e = cudaStreamEndCapture(stream_, &gr);
+        if (!st) {
+            if (e == cudaSuccess) cudaGraphDestroy(gr);
+            return st;
+        }
+        JV_CU(e);
+        cudaError_t ei = cudaGraphInstantiate(ex, gr, 0);
+        cudaGraphDestroy(gr);
+        JV_CU(ei);
+        graphs_[key] = *ex;
+        return Status{};
+    };
+    const int full = nsteps / S, rem = nsteps % S;
+    if (full > 0) {
+        cudaGraphExec_t ex;
+        JV_TRY(get(S, &ex));
+        for (int i = 0; i < full; i++) JV_CU(cudaGraphLaunch(ex, stream_));
+    }
+    if (rem > 0) {
+        cudaGraphExec_t ex;
+        JV_TRY(get(rem, &ex));
+        JV_CU(cudaGraphLaunch(ex, stream_));
+    }
+    return Status{};
+}
+
+// ------------------------------------------------------------ public ops
+
+Status Engine::forward(int shot, float *d_vx, float *d_vy, float *d_vz) {
+    JV_CU(cudaSetDevice(dev_));
+    long long src;
+    JV_TRY(check_shot(shot, &src));
+    float *tr[3] = {d_vx, d_vy, d_vz};
+    JV_CU(cudaEventRecord(ev0_, stream_));
+    JV_TRY(zero_wave(F_, 9));
+    JV_TRY(zero_psi(cpF_));
+    JV_TRY(set_state(0, src, tr, nullptr));
+    JV_TRY(run_loop(kStepModel, nt_));
+    JV_CU(cudaEventRecord(ev1_, stream_));
+    JV_CU(cudaEventSynchronize(ev1_));
+    JV_CU(cudaGetLastError());
+    float ms = 0.f;
+    JV_CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    last_ms_ = ms;
+    return Status{};
+}
+
+Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
+    JV_CU(cudaSetDevice(dev_));
+    long long src;
+    JV_TRY(check_shot(shot, &src));
+    if (nrec_ > 0 && (!d_ox || !d_oy || !d_oz)) return bad(JV_EINVAL, "observed traces must not be NULL");
+    // lazily allocate the receiver wavefield and the boundary store
+    if (!R_.f[0]) {
+        void *p;
+        JV_TRY(alloc(&p, kNumFld * field_elems_ * sizeof(float)));
+        for (int f = 0; f < kNumFld; f++) R_.f[f] = (float *)p + f * field_elems_;
+        JV_TRY([&]() -> Status {
+            CpmlDev c = cpF_;
+            long long n = 0;
+            for (int s = 0; s < 6; s++) n += 6LL * c.s[s].naxes * c.s[s].ncell;
+            void *q;
+            JV_TRY(alloc(&q, (size_t)n * sizeof(float)));
+            long long off = 0;
+            for (int s = 0; s < 6; s++) {
+                c.s[s].psi = (float *)q + off;
+                off += 6LL * c.s[s].naxes * c.s[s].ncell;
+            }
+            cpR_ = c;
+            return Status{};
+        }());
+    }
+    if (!store_ && per_step_ > 0 && nslot_ > 0) {
+        size_t bytes = (size_t)per_step_ * nslot_ * sizeof(float);
+        size_t freeb = 0, totalb = 0;
+        JV_CU(cudaMemGetInfo(&freeb, &totalb));
+        size_t budget = opt_.store_budget ? opt_.store_budget : (freeb > (2ULL << 30) ? freeb - (2ULL << 30) : 0);
+        if (opt_.store_mode == JV_STORE_HOST || bytes > budget)
+            return bad(JV_ENOTSUP, "boundary store of " + std::to_string(bytes) +
+                                       " bytes does not fit the device budget; host streaming is not built");
+        void *p;
+        JV_TRY(alloc(&p, bytes));
+        store_ = (float *)p;
+    }
+    const float *obs[3] = {d_ox, d_oy, d_oz};
+    JV_CU(cudaEventRecord(ev0_, stream_));
+    // forward with boundary store (rtm_forward)
+    JV_TRY(zero_wave(F_, kNumFld));
+    JV_TRY(zero_psi(cpF_));
+    JV_TRY(set_state(0, src, nullptr, obs));
+    JV_TRY(run_loop(kStepRtmFwd, nt_));
+    // time reverse: backward (reconstruction) + reverse (receivers) + image
+    JV_TRY(zero_wave(R_, kNumFld));
+    JV_TRY(zero_psi(cpR_));
+    JV_TRY(set_state(nt_ - 1, src, nullptr, obs));
+    JV_TRY(run_loop(kStepRtmRev, nt_));
+    JV_CU(cudaEventRecord(ev1_, stream_));
+    JV_CU(cudaEventSynchronize(ev1_));
+    JV_CU(cudaGetLastError());
+    float ms = 0.f;
+    JV_CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    last_ms_ = ms;
+    return Status{};
+}
+
+Status Engine::image_reset() {
+    JV_CU(cudaSetDevice(dev_));
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    JV_CU(cudaMemsetAsync(img_.ip, 0, 5 * nphy * sizeof(double), stream_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return Status{};
+}
+
+Status Engine::image_get(int kind, double *out) {
+    JV_CU(cudaSetDevice(dev_));
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    double *src[5] = {img_.ip, img_.pp, img_.ps, img_.sp, img_.ss};
+    if (kind < 0 || kind > 4 || !out) return bad(JV_EINVAL, "bad image kind / output");
+    JV_CU(cudaMemcpyAsync(out, src[kind], nphy * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return Status{};
+}
+
+Status Engine::image_finalize(float *out[8]) {
+    JV_CU(cudaSetDevice(dev_));
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    if (!fin_) {
+        void *p;
+        JV_TRY(alloc(&p, 8 * nphy * sizeof(float)));
+        fin_ = (float *)p;
+    }
+    JV_K(k_image_finalize(g_, img_, fin_, stream_));
+    for (int q = 0; q < 8; q++)
+        if (out[q]) JV_CU(cudaMemcpyAsync(out[q], fin_ + q * nphy, nphy * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return Status{};
+}
+
+Status Engine::sync() {
+    JV_CU(cudaSetDevice(dev_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return Status{};
+}
+
+void Engine::info(jv_info *i) const {
+    memset(i, 0, sizeof(*i));
+    i->grid = grid_;
+    i->nt = nt_;
+    i->n_shot = nshot_;
+    i->n_recv = nrec_;
+    i->rec_width = opt_.rec_width;
+    i->precision = opt_.precision;
+    i->n_ext = (long long)g_.nx * g_.ny * g_.nz;
+    i->n_phy = (long long)g_.px * g_.py * g_.pz;
+    i->store_bytes_per_step = (size_t)per_step_ * sizeof(float);
+    i->device_bytes = dev_bytes_;
+    i->store_on_device = 1;
+}
+
+}  // namespace jv

@@ -1,0 +1,117 @@
+// engine.hpp -- one modelling/RTM problem resident on one GPU.
+//
+// The Engine owns every device buffer of a problem (model, two wavefields,
+// CPML memory variables, VOWR boundary store, traces, FP64 images) and runs
+// the time loops of the reference's blend modules with the kernels of
+// kernels.cu, replaying each chunk of time steps as one CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "jv/jv.h"
+#include "jv_internal.hpp"
+
+namespace jv {
+
+// Staggered-grid Taylor coefficients of half-order `order`
+// (src/jarvis_cpp/jarvis/.jarvis_1_util/.jarvis_2_geometry/
+// jarvis_device_geometry_bones.hpp:29-49).
+void diff_coeff(int order, double *c);
+// get_gap_num (.jarvis_0_meta/.jarvis_2_field/jarvis_3_device_field_meat.hpp:9-22)
+int gap_num(float l, float r, float d);
+// ntime = ceil(T/dt) in float (FD/fdtd3d_0_base_module/fdtd3d_base_4_seisrecord_meat.hpp:278)
+int ntime(float T, float dt);
+// Ricker wavelet as the reference builds it (seisrecord_meat.hpp:279-285)
+void ricker(int nt, float fm, float dt, float *w);
+
+struct Status {
+    jv_status code = JV_OK;
+    std::string msg;
+    explicit operator bool() const { return code == JV_OK; }
+};
+
+class Engine {
+   public:
+    ~Engine();
+    static Status create(const jv_grid &grid, const float *vp, const float *vs, const float *rho, float dt, float fm,
+                         int nt, const jv_options &opt, Engine **out);
+
+    Status set_geometry(int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz);
+    Status forward(int shot, float *d_vx, float *d_vy, float *d_vz);
+    Status rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz);
+    Status image_reset();
+    Status image_get(int kind, double *host_out);
+    Status image_finalize(float *host_out[8]);
+    Status sync();
+    void info(jv_info *i) const;
+    double last_ms() const { return last_ms_; }
+    int nrec() const { return nrec_; }
+    int nt() const { return nt_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // project bookkeeping (jv_open)
+    std::string output_path;
+
+   private:
+    Engine() = default;
+    Status alloc_all(const float *vp, const float *vs, const float *rho);
+    Status check_shot(int shot, long long *src) const;
+    Status run_loop(int kind, int nsteps);
+    Status launch_step(int kind);
+    Status cu(cudaError_t e, const char *what) const;
+    Status zero_wave(const WaveDev &w, int nfld);
+    Status zero_psi(const CpmlDev &c);
+    Status set_state(int it, long long src, float *const tr[3], const float *const obs[3]);
+
+    jv_grid grid_{};
+    jv_options opt_{};
+    float dt_ = 0.f, fm_ = 0.f;
+    int nt_ = 0;
+    int dev_ = 0;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    double last_ms_ = 0.0;
+
+    GridDev g_{};
+    size_t field_elems_ = 0;  // elements per pitched field
+    std::vector<void *> allocs_;
+    size_t dev_bytes_ = 0;
+
+    float *vp_ = nullptr, *rho_ = nullptr, *lam_ = nullptr, *mu_ = nullptr;
+    WaveDev F_{}, R_{};
+    CpmlDev cpF_{}, cpR_{};
+    float *wavelet_ = nullptr;
+    StepState *st_ = nullptr;
+
+    // geometry
+    std::vector<float> shots_;      // all shots (x,y,z)
+    std::vector<long long> rec_h_;  // element index of kept receivers
+    long long *rec_d_ = nullptr;
+    int nrec_ = 0;
+    int nshot_ = 0;
+
+    // VOWR store
+    std::vector<SegDev> segs_h_;
+    SegDev *segs_d_ = nullptr;
+    long long seg_blocks_ = 0;
+    long long per_step_ = 0;
+    float *store_ = nullptr;
+    int nslot_ = 0;
+
+    ImageDev img_{};
+    float *fin_ = nullptr;  // 8 * n_phy finalize buffer
+
+    // graphs: key = kind * 100000 + steps
+    std::map<long long, cudaGraphExec_t> graphs_;
+
+    Status alloc(void **p, size_t bytes);
+};
+
+// kinds of time-loop steps
+enum StepKind : int { kStepModel = 0, kStepRtmFwd = 1, kStepRtmRev = 2 };
+
+}  // namespace jv

@@ -1,0 +1,104 @@
+// jv_internal.hpp -- device data layout and kernel interfaces of libjv.
+//
+// Layout in HBM
+//   Every wavefield component and model parameter covers gridext
+//   (gridphy + pml cells per face) in one pitched array:
+//       elem(i, j, k) = base + xoff + i + sy * j + sz * k
+//   with the row pitch sy a multiple of 32 floats and xoff chosen so that
+//   the first gridphy column (i = pml) starts on a 128-byte boundary.
+//   Absorbing-layer memory variables live only in the six boundary slabs
+//   (slab-local dense indexing), not on the full grid.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace jv {
+
+constexpr int kPhyHalf = 4;  // GeoConst::phy_fdorder_half (8th-order interior)
+constexpr int kPmlHalf = 2;  // GeoConst::pml_fdorder_half (4th-order CPML)
+
+// SimulateType of FD/fdtd3d_0_base_module/fdtd3d_base_1_interface.hpp:19-26
+enum Mode : int { kFwd = 0, kRtmFwd = 1, kBwd = 2, kRev = 3 };
+
+// wavefield components
+enum Fld : int { VX = 0, VY, VZ, SXX, SYY, SZZ, SXY, SXZ, SYZ, SAU, VXP, VYP, VZP, kNumFld };
+
+struct GridDev {
+    int nx, ny, nz;   // gridext
+    int m;            // margin (pml_num)
+    int px, py, pz;   // gridphy
+    long long sy, sz; // pitches in elements
+    long long xoff;   // offset of gridext (0,0,0) from the array base
+    float dx, dy, dz; // spacing
+};
+
+struct WaveDev {
+    float *f[kNumFld];
+};
+
+// One CPML slab: cells [x0,x1) x [y0,y1) x [z0,z1) of gridext, memory
+// variables at psi + q * ncell + local index (q = 3*axis + t for the
+// velocity update, 3*naxes + 3*axis + t for the stress update).
+struct SlabDev {
+    int x0, x1, y0, y1, z0, z1;
+    int naxes;          // 3 (top/bottom), 2 (front/back), 1 (right/left)
+    long long ncell;
+    long long first;    // first global cell id of this slab
+    float *psi;
+};
+
+struct CpmlDev {
+    SlabDev s[6];
+    long long total;    // cells over all slabs
+    float fm, dt;       // dominant frequency, |time step|
+    float l10x7;        // log10(1/R) * DAMP_COEF, R = 0.001, DAMP_COEF = 7
+    float twoNdx, twoNdy, twoNdz;  // 2 N delta per axis, N = pml - 2
+    float N;            // pml - 2
+    float alpha_max;    // pi * fm
+};
+
+struct ImageDev {
+    double *ip, *pp, *ps, *sp, *ss;  // gridphy, dense x-fastest
+};
+
+struct SegDev {          // one VOWR face box
+    int fld;
+    int x0, nxb, y0, nyb, z0, nzb;
+    long long off;       // offset in the packed per-step record
+    long long nblk_first;
+};
+
+// Per-step state in device memory, read by the kernels of a captured
+// time loop, so one CUDA graph serves every shot and every step.
+struct StepState {
+    int it;              // current time step
+    int pad;
+    long long src;       // element index of the shot's source node
+    float *tr[3];        // recorded traces (vx, vy, vz), [nrec][nt]
+    const float *obs[3]; // traces injected into the receiver wavefield
+};
+
+// kernels.cu ------------------------------------------------------------
+int k_model_prep(const GridDev &g, const float *d_vp_phy, const float *d_vs_phy, const float *d_rho_phy,
+                 float *vp, float *rho, float *lam, float *mu, void *stream);
+int k_zero_range(float *p, size_t n, void *stream);
+
+int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w,
+              const WaveDev *rev, const ImageDev *img, void *stream);
+int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,
+                 int rec_w, const float *wavelet, const StepState *st, void *stream);
+int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
+              void *stream);
+int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
+                 const float *vp, int with_sau, void *stream);
+
+int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream);
+int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream);
+int k_vowr(const GridDev &g, const WaveDev &w, const SegDev *segs, int nseg, long long nblk, long long per_step,
+           float *store, const StepState *st, int slot_shift, int nslot, int pack, int which, void *stream);
+int k_step_advance(StepState *st, int delta, void *stream);
+int k_image_finalize(const GridDev &g, const ImageDev &img, float *out /* 8 arrays */, void *stream);
+int upload_coefficients(const float list[5][4], const float dc2[2]);
+
+}  // namespace jv

@@ -1,0 +1,576 @@
+// kernels.cu -- sm_100a CUDA kernels of libjv: interior 8th-order staggered
+// velocity/stress updates (with the rtm_backward variable-order rim and the
+// fused imaging condition), the 4th-order CPML slab updates, receivers,
+// VOWR pack/unpack, model preparation and the image epilogue.
+//
+// Reference kernels restated here (paths relative to the reference root,
+// FD = src/jarvis_cpp/jarvis/.jarvis_2_app/.jarvis_3_seismology/
+// elastic_1_fdtd3d_model_mpi, RTM = .../elastic_1_rtm3d_model_mpi):
+//   interior velocity   FD/fdtd3d_2_phy_mpi_module/fdtd3d_phy_mpi_2_vel_kernel.hpp:7-2088
+//   interior stress     FD/fdtd3d_2_phy_mpi_module/fdtd3d_phy_mpi_3_stress_kernel.hpp:7-1364
+//   CPML                FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_2_kernel_device_{x,y,z}_meat.hpp
+//   damping profile     FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620
+//   receivers           FD/fdtd3d_0_base_module/fdtd3d_base_4_seisrecord_meat.hpp:57-107
+//   imaging             RTM/rtm3d_0_image_module/rtm3d_iamge_kernel.hpp:6-51,118-135,184-200
+#include <cuda_runtime.h>
+
+#include "jv_internal.hpp"
+
+namespace jv {
+
+__constant__ float c_list[5][4];  // c_list[o] = staggered coefficients of half-order o (1..4)
+__constant__ float c_dc2[2];      // half-order 2 (CPML)
+
+namespace {
+
+constexpr int kTX = 32, kTY = 8;
+
+__device__ __forceinline__ float ld(const float *__restrict__ p, long long i) { return __ldg(p + i); }
+
+// Dp f = sum_r c_r (f[i+(r+1)s] - f[i-rs]);  Dm f = sum_r c_r (f[i+rs] - f[i-(r+1)s])
+template <int O>
+__device__ __forceinline__ float dp(const float *__restrict__ f, long long i, long long s, const float *c) {
+    float t = 0.f;
+#pragma unroll
+    for (int r = 0; r < O; r++) t += c[r] * (ld(f, i + (r + 1) * s) - ld(f, i - r * s));
+    return t;
+}
+template <int O>
+__device__ __forceinline__ float dm(const float *__restrict__ f, long long i, long long s, const float *c) {
+    float t = 0.f;
+#pragma unroll
+    for (int r = 0; r < O; r++) t += c[r] * (ld(f, i + r * s) - ld(f, i - (r + 1) * s));
+    return t;
+}
+// runtime order 1..4 (rtm_backward rim)
+__device__ __forceinline__ float dpv(const float *__restrict__ f, long long i, long long s, const float *c, int o) {
+    float t = 0.f;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        if (r < o) t += c[r] * (ld(f, i + (r + 1) * s) - ld(f, i - r * s));
+    return t;
+}
+__device__ __forceinline__ float dmv(const float *__restrict__ f, long long i, long long s, const float *c, int o) {
+    float t = 0.f;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        if (r < o) t += c[r] * (ld(f, i + r * s) - ld(f, i - (r + 1) * s));
+    return t;
+}
+
+// Order of one axis in the rtm_backward rim: within 4 cells of a gridphy
+// face the order drops to e+1 (e = distance to the face) but never below
+// rec_width (FD/fdtd3d_2_phy_mpi_module/fdtd3d_phy_mpi_2_vel_kernel.hpp:132-152,240-261).
+__device__ __forceinline__ int rim_order(int p, int np, int w) {
+    int e = p < kPhyHalf ? p : (np - 1 - p < kPhyHalf ? np - 1 - p : kPhyHalf);
+    if (e >= kPhyHalf) return kPhyHalf;
+    return e < w ? w : e + 1;
+}
+
+template <int MODE, bool IMG>
+__global__ void __launch_bounds__(kTX *kTY) vel_phy(GridDev g, WaveDev w, const float *__restrict__ rho, float dt,
+                                                   int rec_w, WaveDev rv, ImageDev img) {
+    const int pi = blockIdx.x * kTX + threadIdx.x;
+    const int pj = blockIdx.y * kTY + threadIdx.y;
+    const int pk = blockIdx.z;
+    if (pi >= g.px || pj >= g.py) return;
+    const long long sy = g.sy, sz = g.sz;
+    const long long i = g.xoff + (pi + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
+    const float *sxx = w.f[SXX], *syy = w.f[SYY], *szz = w.f[SZZ];
+    const float *sxy = w.f[SXY], *sxz = w.f[SXZ], *syz = w.f[SYZ];
+    float sxx_x, syx_x, szx_x, sxy_y, syy_y, szy_y, sxz_z, syz_z, szz_z;
+    float sau_x = 0.f, sau_y = 0.f, sau_z = 0.f;
+    constexpr bool kP = (MODE == kBwd || MODE == kRev);
+    if (MODE == kBwd) {
+        const int ox = rim_order(pi, g.px, rec_w), oy = rim_order(pj, g.py, rec_w), oz = rim_order(pk, g.pz, rec_w);
+        const float *cx = c_list[ox], *cy = c_list[oy], *cz = c_list[oz];
+        sxx_x = dpv(sxx, i, 1, cx, ox);
+        syx_x = dmv(sxy, i, 1, cx, ox);
+        szx_x = dmv(sxz, i, 1, cx, ox);
+        sxy_y = dmv(sxy, i, sy, cy, oy);
+        syy_y = dpv(syy, i, sy, cy, oy);
+        szy_y = dmv(syz, i, sy, cy, oy);
+        sxz_z = dmv(sxz, i, sz, cz, oz);
+        syz_z = dmv(syz, i, sz, cz, oz);
+        szz_z = dpv(szz, i, sz, cz, oz);
+        const float *sau = w.f[SAU];
+        sau_x = dpv(sau, i, 1, cx, ox);
+        sau_y = dpv(sau, i, sy, cy, oy);
+        sau_z = dpv(sau, i, sz, cz, oz);
+    } else {
+        const float *c = c_list[kPhyHalf];
+        sxx_x = dp<4>(sxx, i, 1, c);
+        syx_x = dm<4>(sxy, i, 1, c);
+        szx_x = dm<4>(sxz, i, 1, c);
+        sxy_y = dm<4>(sxy, i, sy, c);
+        syy_y = dp<4>(syy, i, sy, c);
+        szy_y = dm<4>(syz, i, sy, c);
+        sxz_z = dm<4>(sxz, i, sz, c);
+        syz_z = dm<4>(syz, i, sz, c);
+        szz_z = dp<4>(szz, i, sz, c);
+        if (kP) {
+            const float *sau = w.f[SAU];
+            sau_x = dp<4>(sau, i, 1, c);
+            sau_y = dp<4>(sau, i, sy, c);
+            sau_z = dp<4>(sau, i, sz, c);
+        }
+    }
+    const float dtr = dt / ld(rho, i);
+    const float a = dtr / g.dx, b = dtr / g.dy, c = dtr / g.dz;
+    const float vx = w.f[VX][i] + (a * sxx_x + b * sxy_y + c * sxz_z);
+    const float vy = w.f[VY][i] + (a * syx_x + b * syy_y + c * syz_z);
+    const float vz = w.f[VZ][i] + (a * szx_x + b * szy_y + c * szz_z);
+    w.f[VX][i] = vx;
+    w.f[VY][i] = vy;
+    w.f[VZ][i] = vz;
+    if (kP) {
+        const float px = w.f[VXP][i] + a * sau_x;
+        const float py = w.f[VYP][i] + b * sau_y;
+        const float pz = w.f[VZP][i] + c * sau_z;
+        w.f[VXP][i] = px;
+        w.f[VYP][i] = py;
+        w.f[VZP][i] = pz;
+        if (IMG) {
+            // zero-lag imaging: s = this (reconstructed source) wavefield,
+            // r = the receiver wavefield, already advanced this step
+            const float rpx = ld(rv.f[VXP], i), rpy = ld(rv.f[VYP], i), rpz = ld(rv.f[VZP], i);
+            const float rsx = ld(rv.f[VX], i) - rpx, rsy = ld(rv.f[VY], i) - rpy, rsz = ld(rv.f[VZ], i) - rpz;
+            const float ssx = vx - px, ssy = vy - py, ssz = vz - pz;
+            const long long o = pi + (long long)g.px * (pj + (long long)g.py * pk);
+            img.ip[o] += (double)(px * px + py * py + pz * pz);
+            img.pp[o] += (double)(px * rpx + py * rpy + pz * rpz);
+            img.ps[o] += (double)(px * rsx + py * rsy + pz * rsz);
+            img.sp[o] += (double)(ssx * rpx + ssy * rpy + ssz * rpz);
+            img.ss[o] += (double)(ssx * rsx + ssy * rsy + ssz * rsz);
+        }
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kTX *kTY) stress_phy(GridDev g, WaveDev w, const float *__restrict__ lam,
+                                                      const float *__restrict__ mu, float dt, int rec_w,
+                                                      const float *__restrict__ wavelet,
+                                                      const StepState *__restrict__ st) {
+    const int pi = blockIdx.x * kTX + threadIdx.x;
+    const int pj = blockIdx.y * kTY + threadIdx.y;
+    const int pk = blockIdx.z;
+    if (pi >= g.px || pj >= g.py) return;
+    const long long sy = g.sy, sz = g.sz;
+    const long long i = g.xoff + (pi + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
+    const float *vx = w.f[VX], *vy = w.f[VY], *vz = w.f[VZ];
+    float vx_x, vy_x, vz_x, vx_y, vy_y, vz_y, vx_z, vy_z, vz_z;
+    if (MODE == kBwd) {
+        const int ox = rim_order(pi, g.px, rec_w), oy = rim_order(pj, g.py, rec_w), oz = rim_order(pk, g.pz, rec_w);
+        const float *cx = c_list[ox], *cy = c_list[oy], *cz = c_list[oz];
+        vx_x = dmv(vx, i, 1, cx, ox);
+        vy_x = dpv(vy, i, 1, cx, ox);
+        vz_x = dpv(vz, i, 1, cx, ox);
+        vx_y = dpv(vx, i, sy, cy, oy);
+        vy_y = dmv(vy, i, sy, cy, oy);
+        vz_y = dpv(vz, i, sy, cy, oy);
+        vx_z = dpv(vx, i, sz, cz, oz);
+        vy_z = dpv(vy, i, sz, cz, oz);
+        vz_z = dmv(vz, i, sz, cz, oz);
+    } else {
+        const float *c = c_list[kPhyHalf];
+        vx_x = dm<4>(vx, i, 1, c);
+        vy_x = dp<4>(vy, i, 1, c);
+        vz_x = dp<4>(vz, i, 1, c);
+        vx_y = dp<4>(vx, i, sy, c);
+        vy_y = dm<4>(vy, i, sy, c);
+        vz_y = dp<4>(vz, i, sy, c);
+        vx_z = dp<4>(vx, i, sz, c);
+        vy_z = dp<4>(vy, i, sz, c);
+        vz_z = dm<4>(vz, i, sz, c);
+    }
+    const float a = dt / g.dx, b = dt / g.dy, c = dt / g.dz;
+    const float l = ld(lam, i), m = ld(mu, i);
+    const float l2m = l + 2.0f * m;
+    float sxx = w.f[SXX][i], syy = w.f[SYY][i], szz = w.f[SZZ][i];
+    if (MODE != kRev && i == st->src) {
+        // explosive source, applied before the stress update of step it
+        // (FD/fdtd3d_2_phy_mpi_module/fdtd3d_phy_mpi_3_stress_kernel.hpp:1308-1364)
+        const float s = wavelet[st->it];
+        if (MODE == kBwd) {
+            sxx -= s; syy -= s; szz -= s;
+        } else {
+            sxx += s; syy += s; szz += s;
+        }
+    }
+    w.f[SXX][i] = sxx + (a * l2m * vx_x + b * l * vy_y + c * l * vz_z);
+    w.f[SYY][i] = syy + (a * l * vx_x + b * l2m * vy_y + c * l * vz_z);
+    w.f[SZZ][i] = szz + (a * l * vx_x + b * l * vy_y + c * l2m * vz_z);
+    w.f[SXY][i] += a * m * vy_x + b * m * vx_y;
+    w.f[SXZ][i] += a * m * vz_x + c * m * vx_z;
+    w.f[SYZ][i] += b * m * vz_y + c * m * vy_z;
+    if (MODE != kFwd) w.f[SAU][i] += a * l2m * vx_x + b * l2m * vy_y + c * l2m * vz_z;
+}
+
+// ---------------------------------------------------------------- CPML
+
+// Damping coefficients of one axis at extended index c
+// (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620):
+// low side s = m - c (integer nodes) / m - c - 0.5 (half nodes); high side
+// s = c-(n-m-1) - 0.5 / c-(n-m-1); d = temp (s/N)^2, alpha = pi fm (1 - s/N),
+// b = exp(-(d+alpha) dt), a = d (b-1) / (d+alpha).
+__device__ __forceinline__ bool cpml_ab(int c, int n, int m, float vp, const CpmlDev &P, float twoNd, float &A,
+                                        float &B, float &Ah, float &Bh) {
+    float s, sh;
+    if (c >= kPmlHalf && c < m) {
+        s = (float)(m - c);
+        sh = s - 0.5f;
+    } else if (c >= n - m && c < n - kPmlHalf) {
+        sh = (float)(c - (n - m - 1));
+        s = sh - 0.5f;
+    } else {
+        return false;
+    }
+    const float temp = P.l10x7 * vp / twoNd;
+    const float q = s / P.N, qh = sh / P.N;
+    const float d = temp * (q * q), dh = temp * (qh * qh);
+    const float al = fmaxf(P.alpha_max * (1.0f - q), 0.f), alh = fmaxf(P.alpha_max * (1.0f - qh), 0.f);
+    B = expf(-(d + al) * P.dt);
+    Bh = expf(-(dh + alh) * P.dt);
+    A = d * (B - 1.0f) / (d + al);
+    Ah = dh * (Bh - 1.0f) / (dh + alh);
+    return true;
+}
+
+__device__ __forceinline__ SlabDev pick_slab(const CpmlDev &P, long long gid) {
+    SlabDev S = P.s[0];
+#pragma unroll
+    for (int q = 1; q < 6; q++)
+        if (gid >= P.s[q].first) S = P.s[q];
+    return S;
+}
+
+__device__ __forceinline__ float psi_step(float *p, float b, float a, float d) {
+    const float v = b * *p + a * d;
+    *p = v;
+    return v;
+}
+
+__global__ void __launch_bounds__(256) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
+                                               const float *__restrict__ vpm) {
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= P.total) return;
+    const SlabDev S = pick_slab(P, gid);
+    const long long loc = gid - S.first;
+    const int wx = S.x1 - S.x0, wy = S.y1 - S.y0;
+    const int x = S.x0 + (int)(loc % wx);
+    const long long t = loc / wx;
+    const int y = S.y0 + (int)(t % wy);
+    const int z = S.z0 + (int)(t / wy);
+    const long long sy = g.sy, sz = g.sz;
+    const long long i = g.xoff + x + sy * y + sz * z;
+    const float *c = c_dc2;
+    float sxx_x = dp<2>(w.f[SXX], i, 1, c) / g.dx;
+    float syx_x = dm<2>(w.f[SXY], i, 1, c) / g.dx;
+    float szx_x = dm<2>(w.f[SXZ], i, 1, c) / g.dx;
+    float sxy_y = dm<2>(w.f[SXY], i, sy, c) / g.dy;
+    float syy_y = dp<2>(w.f[SYY], i, sy, c) / g.dy;
+    float szy_y = dm<2>(w.f[SYZ], i, sy, c) / g.dy;
+    float sxz_z = dm<2>(w.f[SXZ], i, sz, c) / g.dz;
+    float syz_z = dm<2>(w.f[SYZ], i, sz, c) / g.dz;
+    float szz_z = dp<2>(w.f[SZZ], i, sz, c) / g.dz;
+    const float vp = ld(vpm, i);
+    float *psi = S.psi + loc;
+    const long long n = S.ncell;
+    float A, B, Ah, Bh;
+    if (cpml_ab(x, g.nx, g.m, vp, P, P.twoNdx, A, B, Ah, Bh)) {
+        sxx_x += psi_step(psi + 0 * n, Bh, Ah, sxx_x);
+        syx_x += psi_step(psi + 1 * n, B, A, syx_x);
+        szx_x += psi_step(psi + 2 * n, B, A, szx_x);
+    }
+    if (cpml_ab(y, g.ny, g.m, vp, P, P.twoNdy, A, B, Ah, Bh)) {
+        sxy_y += psi_step(psi + 3 * n, B, A, sxy_y);
+        syy_y += psi_step(psi + 4 * n, Bh, Ah, syy_y);
+        szy_y += psi_step(psi + 5 * n, B, A, szy_y);
+    }
+    if (cpml_ab(z, g.nz, g.m, vp, P, P.twoNdz, A, B, Ah, Bh)) {
+        sxz_z += psi_step(psi + 6 * n, B, A, sxz_z);
+        syz_z += psi_step(psi + 7 * n, B, A, syz_z);
+        szz_z += psi_step(psi + 8 * n, Bh, Ah, szz_z);
+    }
+    const float dtr = P.dt / ld(rho, i);
+    w.f[VX][i] += dtr * (sxx_x + sxy_y + sxz_z);
+    w.f[VY][i] += dtr * (syx_x + syy_y + syz_z);
+    w.f[VZ][i] += dtr * (szx_x + szy_y + szz_z);
+}
+
+template <bool SAU>
+__global__ void __launch_bounds__(256) stress_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ lam,
+                                                  const float *__restrict__ mu, const float *__restrict__ vpm) {
+    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (gid >= P.total) return;
+    const SlabDev S = pick_slab(P, gid);
+    const long long loc = gid - S.first;
+    const int wx = S.x1 - S.x0, wy = S.y1 - S.y0;
+    const int x = S.x0 + (int)(loc % wx);
+    const long long t = loc / wx;
+    const int y = S.y0 + (int)(t % wy);
+    const int z = S.z0 + (int)(t / wy);
+    const long long sy = g.sy, sz = g.sz;
+    const long long i = g.xoff + x + sy * y + sz * z;
+    const float *c = c_dc2;
+    float vx_x = dm<2>(w.f[VX], i, 1, c) / g.dx;
+    float vy_x = dp<2>(w.f[VY], i, 1, c) / g.dx;
+    float vz_x = dp<2>(w.f[VZ], i, 1, c) / g.dx;
+    float vx_y = dp<2>(w.f[VX], i, sy, c) / g.dy;
+    float vy_y = dm<2>(w.f[VY], i, sy, c) / g.dy;
+    float vz_y = dp<2>(w.f[VZ], i, sy, c) / g.dy;
+    float vx_z = dp<2>(w.f[VX], i, sz, c) / g.dz;
+    float vy_z = dp<2>(w.f[VY], i, sz, c) / g.dz;
+    float vz_z = dm<2>(w.f[VZ], i, sz, c) / g.dz;
+    const float vp = ld(vpm, i);
+    float *psi = S.psi + loc + 3 * S.naxes * S.ncell;
+    const long long n = S.ncell;
+    float A, B, Ah, Bh;
+    if (cpml_ab(x, g.nx, g.m, vp, P, P.twoNdx, A, B, Ah, Bh)) {
+        vx_x += psi_step(psi + 0 * n, B, A, vx_x);
+        vy_x += psi_step(psi + 1 * n, Bh, Ah, vy_x);
+        vz_x += psi_step(psi + 2 * n, Bh, Ah, vz_x);
+    }
+    if (cpml_ab(y, g.ny, g.m, vp, P, P.twoNdy, A, B, Ah, Bh)) {
+        vy_y += psi_step(psi + 3 * n, B, A, vy_y);
+        vx_y += psi_step(psi + 4 * n, Bh, Ah, vx_y);
+        vz_y += psi_step(psi + 5 * n, Bh, Ah, vz_y);
+    }
+    if (cpml_ab(z, g.nz, g.m, vp, P, P.twoNdz, A, B, Ah, Bh)) {
+        vz_z += psi_step(psi + 6 * n, B, A, vz_z);
+        vx_z += psi_step(psi + 7 * n, Bh, Ah, vx_z);
+        vy_z += psi_step(psi + 8 * n, Bh, Ah, vy_z);
+    }
+    const float l = ld(lam, i), m = ld(mu, i);
+    const float l2m = l + 2.0f * m;
+    const float dt = P.dt;
+    w.f[SXX][i] += dt * (l2m * vx_x + l * vy_y + l * vz_z);
+    w.f[SYY][i] += dt * (l * vx_x + l2m * vy_y + l * vz_z);
+    w.f[SZZ][i] += dt * (l * vx_x + l * vy_y + l2m * vz_z);
+    if (SAU) w.f[SAU][i] += dt * (l2m * vx_x + l2m * vy_y + l2m * vz_z);
+    w.f[SXY][i] += dt * m * (vy_x + vx_y);
+    w.f[SXZ][i] += dt * m * (vz_x + vx_z);
+    w.f[SYZ][i] += dt * m * (vz_y + vy_z);
+}
+
+// ------------------------------------------------------------ receivers
+
+__global__ void record(WaveDev w, const long long *__restrict__ rec, int nrec, int nt,
+                       const StepState *__restrict__ st) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    const int it = st->it;
+    float *tx = st->tr[0], *ty = st->tr[1], *tz = st->tr[2];
+    const long long i = rec[r];
+    const long long o = (long long)r * nt + it;
+    if (tx) tx[o] = w.f[VX][i];
+    if (ty) ty[o] = w.f[VY][i];
+    if (tz) tz[o] = w.f[VZ][i];
+}
+
+__global__ void inject_rec(WaveDev w, const long long *__restrict__ rec, int nrec, int nt,
+                           const StepState *__restrict__ st) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrec) return;
+    const int it = st->it;
+    const float *tx = st->obs[0], *ty = st->obs[1], *tz = st->obs[2];
+    const long long i = rec[r];
+    const long long o = (long long)r * nt + it;
+    atomicAdd(w.f[VX] + i, tx[o]);
+    atomicAdd(w.f[VY] + i, ty[o]);
+    atomicAdd(w.f[VZ] + i, tz[o]);
+}
+
+// ---------------------------------------------------------------- VOWR
+
+// One block per 256 elements of one face box; the block finds its box by
+// the prefix of block counts.  pack: field -> store[slot]; else the
+// reverse.  which: 0 all fields, 1 velocities only, 2 stresses only.
+__global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, const SegDev *__restrict__ segs, int nseg,
+                                            long long per_step, float *store, const StepState *__restrict__ st,
+                                            int slot_shift, int nslot, int pack, int which) {
+    const int slot = st->it + slot_shift;
+    if (slot < 0 || slot >= nslot) return;
+    const long long b = blockIdx.x;
+    int s = 0;
+    while (s + 1 < nseg && segs[s + 1].nblk_first <= b) s++;
+    const SegDev S = segs[s];
+    const bool isvel = S.fld <= VZ;
+    if ((which == 1 && !isvel) || (which == 2 && isvel)) return;
+    const long long e = (b - S.nblk_first) * 256 + threadIdx.x;
+    const long long cnt = (long long)S.nxb * S.nyb * S.nzb;
+    if (e >= cnt) return;
+    const int x = S.x0 + (int)(e % S.nxb);
+    const long long t = e / S.nxb;
+    const int y = S.y0 + (int)(t % S.nyb);
+    const int z = S.z0 + (int)(t / S.nyb);
+    const long long i = g.xoff + x + g.sy * y + g.sz * z;
+    float *rec = store + (long long)slot * per_step + S.off + e;
+    if (pack) *rec = w.f[S.fld][i];
+    else w.f[S.fld][i] = *rec;
+}
+
+__global__ void step_advance(StepState *st, int delta) { st->it += delta; }
+
+// ---------------------------------------------------------- model prep
+
+// gridext model: nearest-cell extension of gridphy (the 26 regions of
+// FD/fdtd3d_0_base_module/fdtd3d_base_3_geomodel_meat.hpp:101-364) and
+// lambda = rho (vp^2 - 2 vs^2), mu = rho vs^2 with the reference's
+// float operation order (:454-460).
+__global__ void model_prep(GridDev g, const float *__restrict__ vp0, const float *__restrict__ vs0,
+                           const float *__restrict__ rho0, float *vp, float *rho, float *lam, float *mu) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.nx) return;
+    const int px = min(max(x - g.m, 0), g.px - 1);
+    const int py = min(max(y - g.m, 0), g.py - 1);
+    const int pz = min(max(z - g.m, 0), g.pz - 1);
+    const long long s = px + (long long)g.px * (py + (long long)g.py * pz);
+    const long long i = g.xoff + x + g.sy * y + g.sz * z;
+    const float a = vp0[s], b = vs0[s], r = rho0[s];
+    vp[i] = a;
+    rho[i] = r;
+    const float b2 = __fmul_rn(b, b);
+    lam[i] = __fmul_rn(r, __fsub_rn(__fmul_rn(a, a), __fmul_rn(2.0f, b2)));
+    mu[i] = __fmul_rn(r, b2);
+}
+
+__global__ void zero_range(float *p, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = 0.f;
+}
+
+// ------------------------------------------------------- image epilogue
+
+// out: 8 float arrays of gridphy: compensated pp, ps, sp, ss, then the
+// Laplacians of the uncompensated images (cells 2..n-3, zero elsewhere).
+__global__ void image_finalize(GridDev g, ImageDev img, float *out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (x >= g.px) return;
+    const long long sy = g.px, sz = (long long)g.px * g.py, n = sz * g.pz;
+    const long long o = x + sy * y + sz * z;
+    const double *src[4] = {img.pp, img.ps, img.sp, img.ss};
+    const double ip = img.ip[o];
+    const bool in = x >= 2 && x <= g.px - 3 && y >= 2 && y <= g.py - 3 && z >= 2 && z <= g.pz - 3;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const double *f = src[q];
+        const double v = f[o];
+        out[q * n + o] = (float)(ip > 3.4e-38 ? v / ip : v);
+        double l = 0.0;
+        if (in) l = f[o + 1] + f[o - 1] + f[o + sy] + f[o - sy] + f[o + sz] + f[o - sz] - 6.0 * v;
+        out[(4 + q) * n + o] = (float)l;
+    }
+}
+
+inline int cerr() { return (int)cudaGetLastError(); }
+
+}  // namespace
+
+// --------------------------------------------------------------- hosts
+
+int upload_coefficients(const float list[5][4], const float dc2[2]) {
+    cudaError_t e = cudaMemcpyToSymbol(c_list, list, sizeof(float) * 20);
+    if (e != cudaSuccess) return (int)e;
+    return (int)cudaMemcpyToSymbol(c_dc2, dc2, sizeof(float) * 2);
+}
+
+int k_model_prep(const GridDev &g, const float *vp0, const float *vs0, const float *rho0, float *vp, float *rho,
+                 float *lam, float *mu, void *stream) {
+    dim3 b(128), gr((g.nx + 127) / 128, g.ny, g.nz);
+    model_prep<<<gr, b, 0, (cudaStream_t)stream>>>(g, vp0, vs0, rho0, vp, rho, lam, mu);
+    return cerr();
+}
+
+int k_zero_range(float *p, size_t n, void *stream) {
+    if (n == 0) return 0;
+    size_t blocks = (n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    zero_range<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(p, n);
+    return cerr();
+}
+
+int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w, const WaveDev *rev,
+              const ImageDev *img, void *stream) {
+    dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
+    cudaStream_t s = (cudaStream_t)stream;
+    WaveDev rv = rev ? *rev : WaveDev{};
+    ImageDev im = img ? *img : ImageDev{};
+    switch (mode) {
+    case kFwd: vel_phy<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kRtmFwd: vel_phy<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kRev: vel_phy<kRev, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kBwd:
+        if (img && rev) vel_phy<kBwd, true><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        else vel_phy<kBwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return cerr();
+}
+
+int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt, int rec_w,
+                 const float *wavelet, const StepState *st, void *stream) {
+    dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (mode) {
+    case kFwd: stress_phy<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kRtmFwd: stress_phy<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kBwd: stress_phy<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kRev: stress_phy<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return cerr();
+}
+
+int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp, void *stream) {
+    if (c.total <= 0) return 0;
+    const long long blocks = (c.total + 255) / 256;
+    vel_pml<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, rho, vp);
+    return cerr();
+}
+
+int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
+                 const float *vp, int with_sau, void *stream) {
+    if (c.total <= 0) return 0;
+    const long long blocks = (c.total + 255) / 256;
+    if (with_sau) stress_pml<true><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
+    else stress_pml<false><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
+    return cerr();
+}
+
+int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream) {
+    if (nrec <= 0) return 0;
+    record<<<(nrec + 127) / 128, 128, 0, (cudaStream_t)stream>>>(w, rec, nrec, nt, st);
+    return cerr();
+}
+
+int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream) {
+    if (nrec <= 0) return 0;
+    inject_rec<<<(nrec + 127) / 128, 128, 0, (cudaStream_t)stream>>>(w, rec, nrec, nt, st);
+    return cerr();
+}
+
+int k_vowr(const GridDev &g, const WaveDev &w, const SegDev *segs, int nseg, long long nblk, long long per_step,
+           float *store, const StepState *st, int slot_shift, int nslot, int pack, int which, void *stream) {
+    if (nseg <= 0 || nblk <= 0) return 0;
+    vowr<<<(unsigned)nblk, 256, 0, (cudaStream_t)stream>>>(g, w, segs, nseg, per_step, store, st, slot_shift, nslot,
+                                                            pack, which);
+    return cerr();
+}
+
+int k_step_advance(StepState *st, int delta, void *stream) {
+    step_advance<<<1, 1, 0, (cudaStream_t)stream>>>(st, delta);
+    return cerr();
+}
+
+int k_image_finalize(const GridDev &g, const ImageDev &img, float *out, void *stream) {
+    dim3 b(128), gr((g.px + 127) / 128, g.py, g.pz);
+    image_finalize<<<gr, b, 0, (cudaStream_t)stream>>>(g, img, out);
+    return cerr();
+}
+
+}  // namespace jv

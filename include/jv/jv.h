@@ -1,0 +1,184 @@
+/*
+ * jv.h -- C ABI of libjv, a single-GPU (NVIDIA B200, sm_100a) elastic 3D
+ * staggered-grid FDTD modelling and VOWR reverse-time-migration library.
+ *
+ * It is a drop-in for the modelling and RTM calls of the jarvis
+ * `fdtd3d_blend_elastic_model_mpi` modules.  The reference exposes those
+ * calls as C++ template classes driven by one cross-compiler function;
+ * each entry point below names the reference interface it replaces
+ * (paths relative to the reference project root;
+ *  FD  = src/jarvis_cpp/jarvis/.jarvis_2_app/.jarvis_3_seismology/elastic_1_fdtd3d_model_mpi,
+ *  RTM = src/jarvis_cpp/jarvis/.jarvis_2_app/.jarvis_3_seismology/elastic_1_rtm3d_model_mpi).
+ *
+ * Conventions
+ *  - Grids are the reference's Frame: x fastest ("rows"), then y ("cols"),
+ *    then z ("slices").  Model arrays and images cover gridphy
+ *    (nx*ny*nz floats); the library adds `pml` cells per face (gridext).
+ *  - Positions are metres in the reference's convention (gridphy origin at
+ *    0, node k at k*d); points outside gridphy are dropped as the
+ *    reference's SubGeometry does.
+ *  - Traces are [n_recv][nt] float32, time fastest.
+ *  - Every call returns a jv_status; no call aborts the process.  The
+ *    message of the last failure on the calling thread is available from
+ *    jv_last_error().
+ *  - A context is bound to one CUDA device and one stream; calls on one
+ *    context must not overlap (distinct contexts are independent).
+ *  - `*_device` entry points take device pointers (no host copies); the
+ *    others take host pointers and do the copies inside the call.
+ */
+#ifndef JV_JV_H
+#define JV_JV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JV_ABI_VERSION 1
+
+typedef enum jv_status {
+    JV_OK = 0,
+    JV_EINVAL = -1,    /* bad argument / unsupported problem                */
+    JV_ENOMEM = -2,    /* device or host allocation failed                  */
+    JV_ECUDA = -3,     /* a CUDA runtime call failed                        */
+    JV_EIO = -4,       /* file missing / unreadable / malformed             */
+    JV_ETIMEOUT = -5,  /* a bounded wait ran out                            */
+    JV_ECANCELED = -6, /* job cancelled                                     */
+    JV_ESTATE = -7,    /* call not valid in the context's current state     */
+    JV_ENOTSUP = -8    /* feature not built / not supported on this device  */
+} jv_status;
+
+typedef struct jv_ctx jv_ctx;
+
+/* gridphy and spacing: the fields of Frame gridphy plus pml_num
+ * (.jarvis_0_meta/.jarvis_2_field/jarvis_0_frame_bones.hpp:9-51;
+ *  FD/fdtd3d_0_base_module/fdtd3d_base_1_interface.hpp:41). */
+typedef struct jv_grid {
+    int nx, ny, nz; /* gridphy cells; each >= 8                          */
+    int pml;        /* cells added per face; 4 <= pml                    */
+    float dx, dy, dz;
+} jv_grid;
+
+/* Wavefield storage precision (all arithmetic is FP32). */
+typedef enum jv_precision { JV_FP32 = 0, JV_BF16 = 1, JV_FP16 = 2 } jv_precision;
+
+/* Boundary-store placement for VOWR. */
+typedef enum jv_store_mode { JV_STORE_AUTO = 0, JV_STORE_DEVICE = 1, JV_STORE_HOST = 2 } jv_store_mode;
+
+typedef struct jv_options {
+    int device;         /* CUDA device ordinal                                   */
+    int rec_width;      /* GeoConst::rec_width, 1..4 (0 -> 1)                    */
+    int precision;      /* jv_precision                                          */
+    int store_mode;     /* jv_store_mode                                         */
+    int use_graphs;     /* capture the time loop in CUDA graphs (default on)     */
+    int graph_steps;    /* time steps per captured graph (0 -> library default)  */
+    size_t store_budget;/* max bytes of HBM for the boundary store (0 -> auto)   */
+} jv_options;
+
+/* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,
+ * graphs on). */
+void jv_options_default(jv_options *o);
+
+/* Creates a context from host model arrays on gridphy (vp, vs, rho).
+ * Replaces elasticGeoModel<global/local>::initialize
+ * (FD/fdtd3d_0_base_module/fdtd3d_base_3_geomodel_meat.hpp:405-577) with the
+ * model given in memory; dt, fm and nt are ArgList::dt, fm and
+ * ceil(T/dt) (FD/fdtd3d_0_base_module/fdtd3d_base_4_seisrecord_meat.hpp:
+ * 273-285). */
+jv_status jv_create(const jv_grid *grid, const float *vp, const float *vs, const float *rho, float dt, float fm,
+                    int nt, const jv_options *opt, jv_ctx **out);
+
+/* Reads a reference project directory: proj_path + "argfile.json" (the
+ * ArgList schema, FD/fdtd3d_0_base_module/fdtd3d_base_1_interface.hpp:50-112),
+ * shot/rece geometry (src/jarvis_cpp/jarvis/.jarvis_1_util/.jarvis_2_geometry/
+ * jarvis_device_geometry_meat.hpp:6-128) and model_path (.gms with vp, vs,
+ * rho, src/jarvis_cpp/jarvis/.jarvis_1_util/.jarvis_0_gms/
+ * jarvis_device_gms_meat.hpp:11-79).  x/y/z_divide_num must be 1.  The
+ * optional argfile keys "rec_width" and "precision" override opt. */
+jv_status jv_open(const char *proj_path, const jv_options *opt, jv_ctx **out);
+
+/* Sets the survey: shot and receiver positions (x,y,z metres).  Only the
+ * points inside gridphy are kept (SubGeometry::get_sub_shot_and_recv,
+ * jarvis_device_geometry_meat.hpp:65-128).  Shots keep their input index. */
+jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz);
+
+/* Sizes of the context's problem. */
+typedef struct jv_info {
+    jv_grid grid;
+    int nt;
+    int n_shot;          /* shots in the list (inside or not)        */
+    int n_recv;          /* receivers kept (inside gridphy)          */
+    int rec_width;
+    int precision;
+    long long n_ext;     /* cells of gridext                          */
+    long long n_phy;     /* cells of gridphy                          */
+    size_t store_bytes_per_step; /* VOWR bytes per time step          */
+    size_t device_bytes; /* device memory held by the context         */
+    int store_on_device; /* 1: boundary store in HBM, 0: pinned host  */
+} jv_info;
+jv_status jv_get_info(const jv_ctx *c, jv_info *info);
+
+/* Forward modelling of one shot: replaces
+ * fdtd3d_blend_elastic_model_mpi_module<pure_forward>::reset_for_next_shot
+ * + mpi_sub_forward + SeisRecord::copy_seis_into_host
+ * (FD/fdtd3d_3_model_mpi_blend/fdtd3d_blend_elastic_model_mpi_meat.hpp:38-88;
+ *  FD/fdtd3d_0_base_module/fdtd3d_base_4_seisrecord_meat.hpp:312-321).
+ * Outputs [n_recv][nt] (may be NULL to skip a component). */
+jv_status jv_forward(jv_ctx *c, int shot, float *vx, float *vy, float *vz);
+jv_status jv_forward_device(jv_ctx *c, int shot, float *d_vx, float *d_vy, float *d_vz);
+
+/* Migrates one shot and stacks it into the context's images: replaces the
+ * per-shot body of rtm3d_blend_model_mpi_module::mpi_sub_rtm3d
+ * (RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:50-113):
+ * forward with VOWR boundary store, then the fused time-reverse loop
+ * (source reconstruction, receiver back-propagation, zero-lag imaging).
+ * obs_*: the shot's observed traces [n_recv][nt]. */
+jv_status jv_rtm_shot(jv_ctx *c, int shot, const float *obs_vx, const float *obs_vy, const float *obs_vz);
+jv_status jv_rtm_shot_device(jv_ctx *c, int shot, const float *d_obs_vx, const float *d_obs_vy,
+                             const float *d_obs_vz);
+
+/* Image selectors. */
+typedef enum jv_image_kind { JV_IMG_IP = 0, JV_IMG_PP = 1, JV_IMG_PS = 2, JV_IMG_SP = 3, JV_IMG_SS = 4 } jv_image_kind;
+
+/* Zeroes the stacked images (MigImage::initialize). */
+jv_status jv_image_reset(jv_ctx *c);
+/* Copies one raw stacked accumulator (FP64, gridphy) to host memory. */
+jv_status jv_image_get(jv_ctx *c, int kind, double *out);
+/* The reference's final image step (rtm3d_blend_elastic_model_mpi_meat.hpp:
+ * 123-124; RTM/rtm3d_0_image_module/rtm3d_iamge_kernel.hpp:118-135,184-200):
+ * 7-point Laplacian of the UNcompensated pp/ps/sp/ss into lap (4 arrays of
+ * gridphy, may be NULL), then source compensation I /= Ip where
+ * Ip > 3.4e-38 into img (4 arrays: pp, ps, sp, ss; may be NULL).  Outputs are
+ * float32 host arrays, as the reference saves them; the stacked
+ * accumulators are not modified. */
+jv_status jv_image_finalize(jv_ctx *c, float *img_pp, float *img_ps, float *img_sp, float *img_ss, float *lap_pp,
+                            float *lap_ps, float *lap_sp, float *lap_ss);
+
+/* Whole reference job: rtm3d_blend_model_mpi_module::mpi_sub_rtm3d
+ * (RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:18-135):
+ * model every shot and write {output_path}v?_seis_0_{shot}.txt, migrate every
+ * shot, then write image_pp_0*.raw and image_pp_laplace_0*.raw with the
+ * reference's names and formats.  Only for contexts made by jv_open. */
+jv_status jv_run_project(jv_ctx *c);
+
+/* Device time (ms) of the last jv_forward* / jv_rtm_shot* call, measured
+ * with CUDA events around its kernels. */
+jv_status jv_last_timing(const jv_ctx *c, double *ms);
+
+/* Waits for all work of the context. */
+jv_status jv_sync(jv_ctx *c);
+
+jv_status jv_close(jv_ctx *c);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *jv_last_error(void);
+
+/* Library / kernel build facts, for diagnostics. */
+const char *jv_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JV_JV_H */

@@ -1,0 +1,75 @@
+"""The oracle against the reference itself.
+
+tests/golden/ref_*.npz hold the outputs of the reference's own RTM driver
+(oracle/build_ref.sh, run on a B200 by tests/golden/make_golden.py): the
+traces it writes for every shot and its saved images.  The oracle, run on
+the same regenerated inputs, must reproduce them:
+
+* traces: relative L2 <= 5e-6 (the reference prints 7 significant digits
+  and computes in FP32);
+* uncompensated images (the reference saves I/Ip; multiplying back by its
+  saved Ip recovers I): relative L2 <= 2e-5;
+* Ip and the Laplacian of the uncompensated pp image: <= 5e-5;
+* compensated images: <= 2e-3 -- dividing by the illumination amplifies
+  the reference's own FP32 noise in dimly lit cells.
+"""
+import numpy as np
+import pytest
+
+import make_golden as mg
+from conftest import rel_l2
+
+CASES = list(mg.CASES)
+
+
+def _problem(O, s):
+    return O.Problem(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.dt, s.fm, s.T, s.rec_width, s.shots, s.recvs,
+                     s.vp, s.vs, s.rho)
+
+
+@pytest.fixture(scope="module")
+def runs(oracle):
+    out = {}
+    for name in CASES:
+        s = mg.case_survey(name)
+        p = _problem(oracle, s)
+        traces, imgs = [], None
+        for sh in range(s.shots.shape[0]):
+            tr = oracle.forward(p, sh)
+            traces.append(tr)
+            imgs = oracle.rtm_shot(p, tr, sh, images=imgs)
+        comp, lap = oracle.finalize_image(imgs, s.nx, s.ny, s.nz)
+        out[name] = (s, traces, imgs, comp, lap)
+    return out
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_traces_match_reference(runs, name):
+    s, traces, _, _, _ = runs[name]
+    f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_{name}.npz")
+    for sh, tr in enumerate(traces):
+        for c, t in zip(("vx", "vy", "vz"), tr):
+            ref = f[f"tr_{c}_{sh}"]
+            assert ref.shape == t.shape
+            assert rel_l2(t, ref) <= 5e-6, (name, sh, c, rel_l2(t, ref))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_images_match_reference(runs, name):
+    s, _, imgs, comp, lap = runs[name]
+    f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_{name}.npz")
+    ip = f["img_ip"].astype(np.float64)
+    assert rel_l2(imgs["ip"], ip) <= 5e-5
+    assert rel_l2(lap["pp"], f["lap_pp"]) <= 5e-5
+    for k in ("pp", "ps", "sp", "ss"):
+        unc = f["img_" + k].astype(np.float64) * np.where(ip > 3.4e-38, ip, 1.0)
+        assert rel_l2(imgs[k], unc) <= 2e-5, (name, k, rel_l2(imgs[k], unc))
+        assert rel_l2(comp[k], f["img_" + k]) <= 2e-3, (name, k)
+
+
+def test_fixture_layout():
+    for name in CASES:
+        f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_{name}.npz")
+        s = mg.case_survey(name)
+        assert f["img_pp"].shape == (s.nz, s.ny, s.nx)
+        assert f["tr_vx_0"].shape[1] == s.nt
