@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""RTM throughput on B200: shots/h and Gcell-updates/s.
+
+Workload (default): plain single-shot RTM on a 200^3 interior + 20 CPML
+cells per face (240^3 gridext), d = 5 m, dt = 0.4 ms, 2000 steps, seeded
+6-layer model with a Gaussian vp anomaly, source at cell (100,100,5),
+200 x 200 receivers at z = 5, VOWR rec_width 1, FP32.  Synthetic seeded
+inputs (no public data ship with the reference).
+
+One step = one RTM shot: forward modelling with the VOWR boundary store,
+then the time-reverse loop (source reconstruction, receiver
+back-propagation, zero-lag imaging into FP64 stacks).  Observed traces are
+modelled on the GPU once before timing.  Cell-updates per shot =
+nt * (2 N_ext + N_phy).
+
+  value  device-resident inputs; per-shot device time from CUDA events on
+         the library's stream (jv_last_timing), max over ranks.
+  e2e    the same shot through the host-pointer C ABI: H2D of the observed
+         traces from pinned memory and D2H of the finalized images inside
+         the timed region (host clock around the synchronous calls).
+
+--impl reference times the reference path's CPU implementation: the FP64
+OpenMP restatement in oracle/ (the reference itself is GPU-only), on all
+host cores, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): shot replicas, one process per GPU, no collective
+on the data path; value = shots of all ranks / max rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RTM shots/h & Gcell-updates/s, batched+served vs plain, 1 B200, rel-L2≤1e-3"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel: str):
+    """dram bytes per launch of `kernel` from the committed ncu summary."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        with open(os.path.join(d, fn)) as f:
+            for line in f:
+                m = re.match(r"\s*traffic_bytes_per_launch\[(\w+)\]\s*[:=]\s*([0-9.eE+]+)", line)
+                if m and m.group(1) == kernel:
+                    return float(m.group(2))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.p = None
+        self.path = f"/tmp/jv_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        with open(self.path) as f:
+            for line in f:
+                c = [x.strip() for x in line.split(",")]
+                if len(c) < 9:
+                    continue
+                try:
+                    sm.append(float(c[1]))
+                    mx = max(mx, float(c[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, c[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def survey(args, synth):
+    if args.n == 200 and args.nt == 2000:
+        return synth.cfg2(rec_width=args.rec_width)
+    return synth.scaled_cfg2(args.n, args.nt, rec_width=args.rec_width)
+
+
+# algorithmic bytes per cell (FP32 fields, FP64 image stacks): every array
+# read once and written once per launch, neighbours reused on chip
+BYTES_PER_CELL = {
+    "vel_phy_bwd_image": 4 * (7 + 1 + 3 + 3 + 6) + 8 * 5 + 4 * 6 + 8 * 5,
+    "vel_phy_rev": 4 * (7 + 1 + 6) + 4 * 6,
+    "vel_phy_rtmfwd": 4 * (6 + 1 + 3) + 4 * 3,
+    "vel_phy_fwd": 4 * (6 + 1 + 3) + 4 * 3,
+    "stress_phy_bwd": 4 * (3 + 2 + 7) + 4 * 7,
+    "stress_phy_rev": 4 * (3 + 2 + 7) + 4 * 7,
+    "stress_phy_rtmfwd": 4 * (3 + 2 + 7) + 4 * 7,
+    "stress_phy_fwd": 4 * (3 + 2 + 6) + 4 * 6,
+}
+
+
+def pml_bytes(s, name):
+    """Algorithmic bytes of one CPML launch: per slab cell the fields, plus
+    3 memory variables read+written per axis on which the cell absorbs."""
+    m = s.pml
+    NX, NY, NZ = s.nx + 2 * m, s.ny + 2 * m, s.nz + 2 * m
+
+    def act(n):  # per-index: in the absorbing range of that axis
+        a = np.zeros(n, bool)
+        a[2:m] = True
+        a[n - m:n - 2] = True
+        return a
+
+    ax, ay, az = act(NX), act(NY), act(NZ)
+    ix = np.zeros(NX, bool); ix[2:NX - 2] = True
+    iy = np.zeros(NY, bool); iy[2:NY - 2] = True
+    iz = np.zeros(NZ, bool); iz[2:NZ - 2] = True
+    px = np.zeros(NX, bool); px[m:NX - m] = True
+    py = np.zeros(NY, bool); py[m:NY - m] = True
+    pz = np.zeros(NZ, bool); pz[m:NZ - m] = True
+    cells_all = ix.sum() * iy.sum() * iz.sum()
+    cells = cells_all - px.sum() * py.sum() * pz.sum()
+    # sum over PML cells of the number of absorbing axes: absorbing cells of
+    # an axis are never physical, so count them over the inner box
+    axes = ax[ix].sum() * iy.sum() * iz.sum() + ay[iy].sum() * ix.sum() * iz.sum() + az[iz].sum() * ix.sum() * iy.sum()
+    if name == "vel_pml":
+        per = 4 * (6 + 1 + 1 + 3) + 4 * 3
+    else:
+        per = 4 * (3 + 3 + 7) + 4 * 7
+    return float(cells * per + axes * 3 * 8)
+
+
+def kernel_bytes(s, name):
+    if name in BYTES_PER_CELL:
+        return float(BYTES_PER_CELL[name] * s.n_phy)
+    if name in ("vel_pml", "stress_pml", "stress_pml_sau"):
+        return pml_bytes(s, name)
+    return None
+
+
+def cpu_sample(s, oracle, seconds_target=20.0, max_steps=200):
+    """FP64 oracle on all host cores: a bounded sample of one RTM shot."""
+    p = oracle.Problem(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.dt, s.fm, s.T, s.rec_width, s.shots,
+                       s.recvs, s.vp, s.vs, s.rho, nthreads=os.cpu_count() or 1)
+    steps = 4
+    t0 = time.perf_counter()
+    cells = oracle.rtm_sample(p, steps)
+    dt = time.perf_counter() - t0
+    per_step = dt / steps
+    steps2 = int(min(max_steps, max(4, seconds_target / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    cells = oracle.rtm_sample(p, steps2)
+    dt = time.perf_counter() - t0
+    sec_per_shot = dt / steps2 * s.nt
+    return {"shots_per_h": 3600.0 / sec_per_shot, "gcells": cells / dt / 1e9, "steps": steps2, "seconds": dt}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    synth = importlib.import_module("domain-decomposition-release_b200.synth")
+    s = survey(args, synth)
+    p = O.Problem(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.dt, s.fm, s.T, s.rec_width, s.shots, s.recvs, s.vp,
+                  s.vs, s.rho, nthreads=os.cpu_count() or 1)
+    sample_steps = args.ref_sample_steps
+    for _ in range(args.warmup):
+        O.rtm_sample(p, max(2, sample_steps // 4))
+    times, cells = [], 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cells = O.rtm_sample(p, sample_steps)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    sec_per_shot = tot / args.steps / sample_steps * s.nt
+    value = 3600.0 / sec_per_shot
+    sample = (f"{sample_steps} of {s.nt} time steps of each propagation of one RTM shot "
+              f"({s.nx}^3 + {s.pml} CPML, {s.recvs.shape[0]} receivers), scaled to a full shot")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "shots/h", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * sec_per_shot, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "gcell_updates_per_s": round(cells * args.steps / tot / 1e9, 4),
+        "config": {"workload": s.name, "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt,
+                   "rec_width": s.rec_width, "n_recv": int(s.recvs.shape[0]), "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "shots/h", "cores": os.cpu_count(), "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "shots/h", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="jv", choices=["jv", "reference"])
+    ap.add_argument("--n", type=int, default=200, help="interior cells per axis")
+    ap.add_argument("--nt", type=int, default=2000)
+    ap.add_argument("--rec-width", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-profile", action="store_true")
+    ap.add_argument("--ref-sample-steps", type=int, default=40)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("bench.py: --warmup must be >= 3", file=sys.stderr)
+        return 2
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+
+    jv = importlib.import_module("domain-decomposition-release_b200")
+    s = survey(args, jv.synth)
+    ctx = jv.Context.from_survey(s, device=local)
+    info = ctx.info()
+    nrec, nt = info.n_recv, info.nt
+    obs = torch.empty((3, nrec, nt), dtype=torch.float32, device=f"cuda:{local}")
+    ptrs = [obs[i].data_ptr() for i in range(3)]
+    ctx.forward_device(0, ptrs)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        ctx.image_reset()
+        ctx.rtm_shot_device(0, ptrs)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    dev_ms = 0.0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.rtm_shot_device(0, ptrs)
+        dev_ms += ctx.last_ms()
+    barrier()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+
+    dev_s = dev_ms / 1000.0
+    if dist is not None:
+        t = torch.tensor([dev_s], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_s = float(t.item())
+    cells_per_shot = nt * (2 * info.n_ext + info.n_phy)
+    shots = args.steps * world
+    value = shots / dev_s * 3600.0
+    gcells = shots * cells_per_shot / dev_s / 1e9
+
+    # per-kernel device times (one instrumented shot, events on the library stream)
+    roof = None
+    prof = {}
+    if not args.no_profile:
+        ctx.set_profiling(True)
+        ctx.rtm_shot_device(0, ptrs)
+        prof = ctx.profile()
+        ctx.set_profiling(False)
+        tot = sum(v[0] for v in prof.values())
+        name, (ms, n) = max(prof.items(), key=lambda kv: kv[1][0])
+        b = kernel_bytes(s, name)
+        peak, peak_kind = load_peaks()
+        if b is not None and n > 0:
+            avg_s = ms / n / 1000.0
+            ach = b / avg_s / 1e9
+            tr = traffic_from_profiles(name)
+            roof = {"bound": "hbm", "kernel": name, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "peak_source": peak_kind,
+                    "traffic": tr, "algorithmic_bytes_per_launch": b, "avg_launch_us": round(avg_s * 1e6, 2),
+                    "share": round(ms / tot, 4) if tot > 0 else None}
+
+    # end to end through the host-pointer ABI: pinned H2D of the traces,
+    # D2H of the 8 finalized images, every step
+    e2e = None
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
+    if e2e_steps > 0:
+        host = torch.empty((3, nrec, nt), dtype=torch.float32, pin_memory=True)
+        host.copy_(obs.cpu())
+        hobs = [host[i].numpy() for i in range(3)]
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ctx.rtm_shot(0, hobs)
+            ctx.finalize()
+        barrier()
+        te = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([te], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": round(e2e_steps * world / te * 3600.0, 3), "unit": "shots/h",
+               "h2d_bytes_per_step": int(3 * nrec * nt * 4), "d2h_bytes_per_step": int(8 * info.n_phy * 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        c = cpu_sample(s, O)
+        cpu = {"value": round(c["shots_per_h"], 4), "unit": "shots/h", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"FP64 oracle, {c['steps']} of {s.nt} time steps of each propagation of one shot, "
+                         f"{c['seconds']:.1f} s, scaled to a full shot",
+               "gcell_updates_per_s": round(c["gcells"], 4)}
+
+    launches = sum(v[1] for v in prof.values()) if prof else None
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "shots/h", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1000 * dev_s / args.steps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "gcell_updates_per_s": round(gcells, 3),
+        "config": {"workload": s.name, "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt,
+                   "rec_width": s.rec_width, "n_recv": nrec, "mode": "plain one-shot-per-call, graph time loop",
+                   "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        "gpu_launches": launches * args.steps if launches else None,
+        "wall_s": round(wall, 3),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

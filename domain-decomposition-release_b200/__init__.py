@@ -1,0 +1,274 @@
+"""jv -- single-B200 elastic FDTD modelling and VOWR RTM (Python front end).
+
+This package is the Python mirror of the reference's modelling/RTM calls
+(jarvis ``fdtd3d_blend_elastic_model_mpi`` / ``rtm3d_blend_model_mpi_module``)
+over the C ABI of ``libjv.so`` (include/jv/jv.h).  All computation runs in
+the CUDA library; there is no CPU fallback: importing works anywhere, but
+creating a context raises ``JvError`` when libjv.so is missing or no CUDA
+device is usable.
+
+Typical use::
+
+    jv = importlib.import_module("domain-decomposition-release_b200")
+    s = jv.synth.small_case()
+    with jv.Context.from_survey(s) as ctx:
+        vx, vy, vz = ctx.forward(0)
+        ctx.rtm_shot(0, (vx, vy, vz))
+        img = ctx.finalize()
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from . import project, synth  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libjv.so")
+
+JV_OK, JV_EINVAL, JV_ENOMEM, JV_ECUDA, JV_EIO, JV_ETIMEOUT, JV_ECANCELED, JV_ESTATE, JV_ENOTSUP = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8)
+JV_FP32, JV_BF16, JV_FP16 = 0, 1, 2
+JV_STORE_AUTO, JV_STORE_DEVICE, JV_STORE_HOST = 0, 1, 2
+IMG_IP, IMG_PP, IMG_PS, IMG_SP, IMG_SS = range(5)
+
+# every symbol include/jv/jv.h declares
+EXPORTS = (
+    "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_get_info", "jv_forward",
+    "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
+    "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
+    "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info",
+)
+
+
+class JvError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"jv error {code}: {msg}")
+        self.code = code
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int), ("pml", C.c_int),
+                ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float)]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int), ("rec_width", C.c_int), ("precision", C.c_int), ("store_mode", C.c_int),
+                ("use_graphs", C.c_int), ("graph_steps", C.c_int), ("store_budget", C.c_size_t)]
+
+
+class Info(C.Structure):
+    _fields_ = [("grid", Grid), ("nt", C.c_int), ("n_shot", C.c_int), ("n_recv", C.c_int),
+                ("rec_width", C.c_int), ("precision", C.c_int), ("n_ext", C.c_longlong),
+                ("n_phy", C.c_longlong), ("store_bytes_per_step", C.c_size_t), ("device_bytes", C.c_size_t),
+                ("store_on_device", C.c_int)]
+
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compiles libjv.so for sm_100a in-tree (nvcc; no GPU needed)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc"), "-j8"], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    """Loads libjv.so (raising JvError if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise JvError(JV_ENOTSUP, f"{LIB_PATH} is not built (run build())")
+    L = C.CDLL(LIB_PATH)
+    fp, dp, vp = C.POINTER(C.c_float), C.POINTER(C.c_double), C.c_void_p
+    ctxp = C.c_void_p
+    L.jv_options_default.argtypes = [C.POINTER(Options)]
+    L.jv_options_default.restype = None
+    L.jv_create.argtypes = [C.POINTER(Grid), fp, fp, fp, C.c_float, C.c_float, C.c_int, C.POINTER(Options),
+                            C.POINTER(ctxp)]
+    L.jv_open.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(ctxp)]
+    L.jv_set_geometry.argtypes = [ctxp, C.c_int, fp, C.c_int, fp]
+    L.jv_get_info.argtypes = [ctxp, C.POINTER(Info)]
+    L.jv_forward.argtypes = [ctxp, C.c_int, fp, fp, fp]
+    L.jv_forward_device.argtypes = [ctxp, C.c_int, vp, vp, vp]
+    L.jv_rtm_shot.argtypes = [ctxp, C.c_int, fp, fp, fp]
+    L.jv_rtm_shot_device.argtypes = [ctxp, C.c_int, vp, vp, vp]
+    L.jv_image_reset.argtypes = [ctxp]
+    L.jv_image_get.argtypes = [ctxp, C.c_int, dp]
+    L.jv_image_finalize.argtypes = [ctxp] + [fp] * 8
+    L.jv_image_get_device.argtypes = [ctxp, C.c_int, vp]
+    L.jv_set_profiling.argtypes = [ctxp, C.c_int]
+    L.jv_profile_entry.argtypes = [ctxp, C.c_int, C.POINTER(C.c_char_p), dp, C.POINTER(C.c_longlong)]
+    L.jv_run_project.argtypes = [ctxp]
+    L.jv_last_timing.argtypes = [ctxp, dp]
+    L.jv_sync.argtypes = [ctxp]
+    L.jv_close.argtypes = [ctxp]
+    L.jv_last_error.argtypes = []
+    L.jv_last_error.restype = C.c_char_p
+    L.jv_build_info.argtypes = []
+    L.jv_build_info.restype = C.c_char_p
+    for n in EXPORTS:
+        if n not in ("jv_options_default", "jv_last_error", "jv_build_info"):
+            getattr(L, n).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int) -> None:
+    if rc != JV_OK:
+        msg = lib().jv_last_error().decode(errors="replace")
+        raise JvError(rc, msg)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().jv_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Context:
+    """One problem resident on one GPU (a jv_ctx)."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+
+    # -- construction -----------------------------------------------------
+    @classmethod
+    def create(cls, nx, ny, nz, pml, dx, dy, dz, vp, vs, rho, dt, fm, nt, **opts) -> "Context":
+        L = lib()
+        g = Grid(nx, ny, nz, pml, dx, dy, dz)
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho)]
+        for a in arrs:
+            if a.size != nx * ny * nz:
+                raise JvError(JV_EINVAL, "model array size does not match the grid")
+        o = default_options(**opts)
+        h = C.c_void_p()
+        _check(L.jv_create(C.byref(g), _fptr(arrs[0]), _fptr(arrs[1]), _fptr(arrs[2]), dt, fm, int(nt), C.byref(o),
+                           C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_survey(cls, s, **opts) -> "Context":
+        opts.setdefault("rec_width", s.rec_width)
+        c = cls.create(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt, **opts)
+        c.set_geometry(s.shots, s.recvs)
+        return c
+
+    @classmethod
+    def open(cls, proj_path: str, **opts) -> "Context":
+        """Reads a reference project directory (argfile.json + geometry + .gms)."""
+        L = lib()
+        o = default_options(**opts)
+        h = C.c_void_p()
+        _check(L.jv_open(proj_path.encode(), C.byref(o), C.byref(h)))
+        return cls(h)
+
+    def set_geometry(self, shots, recvs) -> None:
+        sh = np.ascontiguousarray(shots, dtype=np.float32).reshape(-1, 3)
+        rc = np.ascontiguousarray(recvs, dtype=np.float32).reshape(-1, 3)
+        _check(lib().jv_set_geometry(self._h, sh.shape[0], _fptr(sh), rc.shape[0], _fptr(rc)))
+
+    # -- queries ------------------------------------------------------------
+    def info(self) -> Info:
+        i = Info()
+        _check(lib().jv_get_info(self._h, C.byref(i)))
+        return i
+
+    def last_ms(self) -> float:
+        v = C.c_double()
+        _check(lib().jv_last_timing(self._h, C.byref(v)))
+        return v.value
+
+    # -- modelling / migration ---------------------------------------------
+    def forward(self, shot: int):
+        """Traces (vx, vy, vz), each float32 [n_recv, nt] (host arrays)."""
+        i = self.info()
+        out = [np.zeros((i.n_recv, i.nt), np.float32) for _ in range(3)]
+        _check(lib().jv_forward(self._h, shot, _fptr(out[0]), _fptr(out[1]), _fptr(out[2])))
+        return tuple(out)
+
+    def forward_device(self, shot: int, ptrs) -> None:
+        """Device-pointer variant: ptrs = 3 device addresses (ints)."""
+        _check(lib().jv_forward_device(self._h, shot, *[C.c_void_p(int(p)) if p else None for p in ptrs]))
+
+    def rtm_shot(self, shot: int, obs) -> None:
+        o = [np.ascontiguousarray(a, dtype=np.float32) for a in obs]
+        _check(lib().jv_rtm_shot(self._h, shot, _fptr(o[0]), _fptr(o[1]), _fptr(o[2])))
+
+    def rtm_shot_device(self, shot: int, ptrs) -> None:
+        _check(lib().jv_rtm_shot_device(self._h, shot, *[C.c_void_p(int(p)) for p in ptrs]))
+
+    def image_reset(self) -> None:
+        _check(lib().jv_image_reset(self._h))
+
+    def image(self, kind: int) -> np.ndarray:
+        i = self.info()
+        out = np.zeros((i.grid.nz, i.grid.ny, i.grid.nx), np.float64)
+        _check(lib().jv_image_get(self._h, kind, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def images(self) -> dict:
+        return {k: self.image(v) for k, v in (("ip", IMG_IP), ("pp", IMG_PP), ("ps", IMG_PS), ("sp", IMG_SP),
+                                              ("ss", IMG_SS))}
+
+    def finalize(self):
+        """(compensated {pp,ps,sp,ss}, laplacian {pp,ps,sp,ss}) float32."""
+        i = self.info()
+        shp = (i.grid.nz, i.grid.ny, i.grid.nx)
+        arr = [np.zeros(shp, np.float32) for _ in range(8)]
+        _check(lib().jv_image_finalize(self._h, *[_fptr(a) for a in arr]))
+        keys = ("pp", "ps", "sp", "ss")
+        return dict(zip(keys, arr[:4])), dict(zip(keys, arr[4:]))
+
+    def image_to_device(self, kind: int, dev_ptr: int) -> None:
+        """Copies one FP64 accumulator into device memory at dev_ptr."""
+        _check(lib().jv_image_get_device(self._h, kind, C.c_void_p(int(dev_ptr))))
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib().jv_set_profiling(self._h, 1 if on else 0))
+
+    def profile(self) -> dict:
+        """{kernel name: (total ms, launches)} since profiling was switched on."""
+        out, i = {}, 0
+        L = lib()
+        while True:
+            nm, ms, n = C.c_char_p(), C.c_double(), C.c_longlong()
+            if L.jv_profile_entry(self._h, i, C.byref(nm), C.byref(ms), C.byref(n)) != JV_OK:
+                break
+            out[nm.value.decode()] = (ms.value, n.value)
+            i += 1
+        return out
+
+    def run_project(self) -> None:
+        _check(lib().jv_run_project(self._h))
+
+    def sync(self) -> None:
+        _check(lib().jv_sync(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().jv_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

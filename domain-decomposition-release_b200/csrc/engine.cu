@@ -102,6 +102,7 @@ Engine::~Engine() {
         cudaStreamSynchronize(stream_);
     }
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
+    for (cudaEvent_t e : prof_pool_) cudaEventDestroy(e);
     for (void *p : allocs_) cudaFree(p);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -371,42 +372,105 @@ Status Engine::zero_psi(const CpmlDev &c) {
 
 // ------------------------------------------------------------ stepping
 
+int Engine::prof_id(const char *name) {
+    for (size_t i = 0; i < prof_names_.size(); i++)
+        if (prof_names_[i] == name) return (int)i;
+    prof_names_.push_back(name);
+    prof_ms_.push_back(0.0);
+    prof_n_.push_back(0);
+    return (int)prof_names_.size() - 1;
+}
+
+cudaEvent_t Engine::prof_event() {
+    if (prof_used_ == prof_pool_.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        prof_pool_.push_back(e);
+    }
+    return prof_pool_[prof_used_++];
+}
+
+Status Engine::prof_collect() {
+    if (prof_pending_.empty()) return Status{};
+    JV_CU(cudaStreamSynchronize(stream_));
+    for (const ProfRec &r : prof_pending_) {
+        float ms = 0.f;
+        JV_CU(cudaEventElapsedTime(&ms, r.a, r.b));
+        prof_ms_[r.id] += ms;
+        prof_n_[r.id] += 1;
+    }
+    prof_pending_.clear();
+    prof_used_ = 0;
+    return Status{};
+}
+
+void Engine::set_profiling(bool on) {
+    prof_ = on;
+    prof_names_.clear();
+    prof_ms_.clear();
+    prof_n_.clear();
+    prof_pending_.clear();
+    prof_used_ = 0;
+}
+
+bool Engine::profile_entry(int i, const char **name, double *ms, long long *launches) const {
+    if (i < 0 || i >= (int)prof_names_.size()) return false;
+    *name = prof_names_[i].c_str();
+    *ms = prof_ms_[i];
+    *launches = prof_n_[i];
+    return true;
+}
+
+// launch one kernel, bracketed by timing events when profiling
+#define JV_L(name, expr)                                                    \
+    do {                                                                    \
+        if (prof_) {                                                        \
+            ProfRec _r{prof_id(name), prof_event(), prof_event()};          \
+            JV_CU(cudaEventRecord(_r.a, stream_));                          \
+            JV_K(expr);                                                     \
+            JV_CU(cudaEventRecord(_r.b, stream_));                          \
+            prof_pending_.push_back(_r);                                    \
+        } else {                                                            \
+            JV_K(expr);                                                     \
+        }                                                                   \
+    } while (0)
+
 Status Engine::launch_step(int kind) {
     void *s = (void *)stream_;
     const float dt = dt_;
     const int rw = opt_.rec_width;
     switch (kind) {
     case kStepModel:
-        JV_K(k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
-        JV_K(k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
-        JV_K(k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, s));
-        JV_K(k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
-        JV_K(k_record(F_, rec_d_, nrec_, nt_, st_, s));
-        JV_K(k_step_advance(st_, +1, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
+        JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, s));
+        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, s));
+        JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
-        JV_K(k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
-        JV_K(k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
-        JV_K(k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, s));
-        JV_K(k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, 0, nslot_, 1, 0, s));
-        JV_K(k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
-        JV_K(k_step_advance(st_, +1, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
+        JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, s));
+        JV_L("vowr_pack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, 0, nslot_, 1, 0, s));
+        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmRev:
         // UPDATE 1: source subtraction (fused) + backward stress, receiver
         // injection + reverse velocity, stress boundary layers of step it-1
-        JV_K(k_inject_rec(R_, rec_d_, nrec_, nt_, st_, s));
-        JV_K(k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, s));
-        JV_K(k_vel_pml(g_, cpR_, R_, rho_, vp_, s));
-        JV_K(k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, s));
-        JV_K(k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 2, s));
+        JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, s));
+        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, s));
+        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
-        JV_K(k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, s));
-        JV_K(k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, s));
-        JV_K(k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, s));
-        JV_K(k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 1, s));
-        JV_K(k_step_advance(st_, -1, s));
+        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, s));
+        JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, s));
+        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 1, s));
+        JV_L("step_advance", k_step_advance(st_, -1, s));
         break;
     default: return bad(JV_EINVAL, "unknown step kind");
     }
@@ -415,8 +479,12 @@ Status Engine::launch_step(int kind) {
 
 Status Engine::run_loop(int kind, int nsteps) {
     if (nsteps <= 0) return Status{};
-    if (!opt_.use_graphs) {
-        for (int i = 0; i < nsteps; i++) JV_TRY(launch_step(kind));
+    if (!opt_.use_graphs || prof_) {
+        for (int i = 0; i < nsteps; i++) {
+            JV_TRY(launch_step(kind));
+            if (prof_ && prof_pending_.size() > 4096) JV_TRY(prof_collect());
+        }
+        if (prof_) JV_TRY(prof_collect());
         return Status{};
     }
     const int S = opt_.graph_steps;
@@ -565,6 +633,16 @@ Status Engine::image_finalize(float *out[8]) {
     JV_K(k_image_finalize(g_, img_, fin_, stream_));
     for (int q = 0; q < 8; q++)
         if (out[q]) JV_CU(cudaMemcpyAsync(out[q], fin_ + q * nphy, nphy * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return Status{};
+}
+
+Status Engine::image_get_device(int kind, double *out) {
+    JV_CU(cudaSetDevice(dev_));
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    double *src[5] = {img_.ip, img_.pp, img_.ps, img_.sp, img_.ss};
+    if (kind < 0 || kind > 4 || !out) return bad(JV_EINVAL, "bad image kind / output");
+    JV_CU(cudaMemcpyAsync(out, src[kind], nphy * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     JV_CU(cudaStreamSynchronize(stream_));
     return Status{};
 }

@@ -46,6 +46,12 @@ class Engine {
     Status image_reset();
     Status image_get(int kind, double *host_out);
     Status image_finalize(float *host_out[8]);
+    Status image_get_device(int kind, double *dev_out);
+
+    // per-kernel timing with CUDA events (direct launches, no graphs)
+    void set_profiling(bool on);
+    int profile_count() const { return (int)prof_names_.size(); }
+    bool profile_entry(int i, const char **name, double *ms, long long *launches) const;
     Status sync();
     void info(jv_info *i) const;
     double last_ms() const { return last_ms_; }
@@ -109,6 +115,19 @@ class Engine {
     std::map<long long, cudaGraphExec_t> graphs_;
 
     Status alloc(void **p, size_t bytes);
+
+    // profiling state
+    bool prof_ = false;
+    std::vector<std::string> prof_names_;
+    std::vector<double> prof_ms_;
+    std::vector<long long> prof_n_;
+    struct ProfRec { int id; cudaEvent_t a, b; };
+    std::vector<ProfRec> prof_pending_;
+    std::vector<cudaEvent_t> prof_pool_;
+    size_t prof_used_ = 0;
+    int prof_id(const char *name);
+    cudaEvent_t prof_event();
+    Status prof_collect();
 };
 
 // kinds of time-loop steps

@@ -1,0 +1,300 @@
+// jv_abi.cu -- the extern "C" boundary of libjv (include/jv/jv.h).
+// Every entry point converts the C++ engine's Status into a jv_status and
+// keeps the message for jv_last_error(); nothing here aborts.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "jv/jv.h"
+#include "project_io.hpp"
+
+namespace {
+thread_local std::string g_err;
+
+jv_status ret(const jv::Status &s) {
+    g_err = s.msg;
+    return s.code;
+}
+jv_status fail(jv_status c, const std::string &m) {
+    g_err = m;
+    return c;
+}
+}  // namespace
+
+struct jv_ctx {
+    std::unique_ptr<jv::Engine> eng;
+    bool from_project = false;
+    jv::ArgFile arg;
+    std::vector<float> shots, recvs;
+    // device scratch for host-pointer calls
+    float *d_tr = nullptr;
+    size_t d_tr_elems = 0;
+    ~jv_ctx() {
+        if (d_tr) cudaFree(d_tr);
+    }
+};
+
+static jv_status ensure_traces(jv_ctx *c, size_t elems) {
+    if (c->d_tr_elems >= elems) return JV_OK;
+    if (c->d_tr) cudaFree(c->d_tr);
+    c->d_tr = nullptr;
+    c->d_tr_elems = 0;
+    if (elems == 0) return JV_OK;
+    cudaError_t e = cudaMalloc(&c->d_tr, elems * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(JV_ENOMEM, std::string("trace buffer: ") + cudaGetErrorString(e));
+    }
+    c->d_tr_elems = elems;
+    return JV_OK;
+}
+
+extern "C" {
+
+void jv_options_default(jv_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->device = 0;
+    o->rec_width = 1;
+    o->precision = JV_FP32;
+    o->store_mode = JV_STORE_AUTO;
+    o->use_graphs = 1;
+    o->graph_steps = 0;
+    o->store_budget = 0;
+}
+
+jv_status jv_create(const jv_grid *grid, const float *vp, const float *vs, const float *rho, float dt, float fm,
+                    int nt, const jv_options *opt, jv_ctx **out) {
+    if (!grid || !out) return fail(JV_EINVAL, "jv_create: NULL argument");
+    *out = nullptr;
+    jv_options o;
+    jv_options_default(&o);
+    if (opt) o = *opt;
+    jv::Engine *e = nullptr;
+    jv::Status s = jv::Engine::create(*grid, vp, vs, rho, dt, fm, nt, o, &e);
+    if (!s) return ret(s);
+    jv_ctx *c = new jv_ctx();
+    c->eng.reset(e);
+    *out = c;
+    g_err.clear();
+    return JV_OK;
+}
+
+jv_status jv_open(const char *proj_path, const jv_options *opt, jv_ctx **out) {
+    if (!proj_path || !out) return fail(JV_EINVAL, "jv_open: NULL argument");
+    *out = nullptr;
+    jv::ArgFile a;
+    std::string m = jv::read_argfile(proj_path, &a);
+    if (!m.empty()) return fail(JV_EIO, m);
+    if (a.x_divide_num > 1 || a.y_divide_num > 1 || a.z_divide_num > 1)
+        return fail(JV_EINVAL, "x/y/z_divide_num must be 1: the whole model is resident on one GPU");
+    jv::GmsModel g;
+    m = jv::read_gms(a.model_path, &g);
+    if (!m.empty()) return fail(JV_EIO, m);
+    std::vector<float> shots, recvs;
+    m = jv::read_points(a.shot_path, &shots);
+    if (!m.empty()) return fail(JV_EIO, m);
+    m = jv::read_points(a.recv_path, &recvs);
+    if (!m.empty()) return fail(JV_EIO, m);
+    jv_options o;
+    jv_options_default(&o);
+    if (opt) o = *opt;
+    if (a.rec_width > 0) o.rec_width = a.rec_width;
+    if (a.precision == "bf16") o.precision = JV_BF16;
+    else if (a.precision == "fp16") o.precision = JV_FP16;
+    jv_grid gr{g.nx, g.ny, g.nz, a.pml_num, g.dx, g.dy, g.dz};
+    const int nt = jv::ntime(a.T, a.dt);
+    jv_ctx *c = nullptr;
+    jv_status st = jv_create(&gr, g.params[0].data(), g.params[1].data(), g.params[2].data(), a.dt, a.fm, nt, &o, &c);
+    if (st != JV_OK) return st;
+    c->from_project = true;
+    c->arg = a;
+    c->eng->output_path = a.output_path;
+    st = jv_set_geometry(c, (int)(shots.size() / 3), shots.data(), (int)(recvs.size() / 3), recvs.data());
+    if (st != JV_OK) {
+        delete c;
+        return st;
+    }
+    *out = c;
+    return JV_OK;
+}
+
+jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    jv::Status s = c->eng->set_geometry(n_shot, shot_xyz, n_recv, recv_xyz);
+    if (s) {
+        c->shots.assign(shot_xyz, shot_xyz + 3 * (size_t)n_shot);
+        c->recvs.assign(recv_xyz, recv_xyz + 3 * (size_t)n_recv);
+    }
+    return ret(s);
+}
+
+jv_status jv_get_info(const jv_ctx *c, jv_info *info) {
+    if (!c || !info) return fail(JV_EINVAL, "NULL argument");
+    c->eng->info(info);
+    return JV_OK;
+}
+
+jv_status jv_forward_device(jv_ctx *c, int shot, float *d_vx, float *d_vy, float *d_vz) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->forward(shot, d_vx, d_vy, d_vz));
+}
+
+jv_status jv_forward(jv_ctx *c, int shot, float *vx, float *vy, float *vz) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
+    jv_status st = ensure_traces(c, 3 * per);
+    if (st != JV_OK) return st;
+    float *d = c->d_tr;
+    st = jv_forward_device(c, shot, vx ? d : nullptr, vy ? d + per : nullptr, vz ? d + 2 * per : nullptr);
+    if (st != JV_OK) return st;
+    float *h[3] = {vx, vy, vz};
+    for (int q = 0; q < 3; q++)
+        if (h[q] && per) {
+            cudaError_t e = cudaMemcpyAsync(h[q], d + q * per, per * sizeof(float), cudaMemcpyDeviceToHost,
+                                            c->eng->stream());
+            if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+        }
+    cudaError_t e = cudaStreamSynchronize(c->eng->stream());
+    if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+    return JV_OK;
+}
+
+jv_status jv_rtm_shot_device(jv_ctx *c, int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->rtm_shot(shot, d_ox, d_oy, d_oz));
+}
+
+jv_status jv_rtm_shot(jv_ctx *c, int shot, const float *ox, const float *oy, const float *oz) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
+    if (per && (!ox || !oy || !oz)) return fail(JV_EINVAL, "observed traces must not be NULL");
+    jv_status st = ensure_traces(c, 3 * per);
+    if (st != JV_OK) return st;
+    const float *h[3] = {ox, oy, oz};
+    for (int q = 0; q < 3 && per; q++) {
+        cudaError_t e = cudaMemcpyAsync(c->d_tr + q * per, h[q], per * sizeof(float), cudaMemcpyHostToDevice,
+                                        c->eng->stream());
+        if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+    }
+    return jv_rtm_shot_device(c, shot, c->d_tr, c->d_tr + per, c->d_tr + 2 * per);
+}
+
+jv_status jv_image_reset(jv_ctx *c) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->image_reset());
+}
+
+jv_status jv_image_get(jv_ctx *c, int kind, double *out) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->image_get(kind, out));
+}
+
+jv_status jv_image_finalize(jv_ctx *c, float *img_pp, float *img_ps, float *img_sp, float *img_ss, float *lap_pp,
+                            float *lap_ps, float *lap_sp, float *lap_ss) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    float *o[8] = {img_pp, img_ps, img_sp, img_ss, lap_pp, lap_ps, lap_sp, lap_ss};
+    return ret(c->eng->image_finalize(o));
+}
+
+jv_status jv_image_get_device(jv_ctx *c, int kind, double *d_out) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->image_get_device(kind, d_out));
+}
+
+jv_status jv_set_profiling(jv_ctx *c, int on) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    c->eng->set_profiling(on != 0);
+    return JV_OK;
+}
+
+jv_status jv_profile_entry(const jv_ctx *c, int idx, const char **name, double *total_ms, long long *launches) {
+    if (!c || !name || !total_ms || !launches) return fail(JV_EINVAL, "NULL argument");
+    if (!c->eng->profile_entry(idx, name, total_ms, launches)) return fail(JV_EINVAL, "no such profile entry");
+    return JV_OK;
+}
+
+jv_status jv_run_project(jv_ctx *c) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    if (!c->from_project) return fail(JV_ESTATE, "jv_run_project needs a context made by jv_open");
+    jv_info inf;
+    c->eng->info(&inf);
+    const int nshot = inf.n_shot, nrec = inf.n_recv, nt = inf.nt;
+    const size_t per = (size_t)nrec * nt;
+    // phase 1: model every shot, keep its traces (mpi_sub_rtm3d :20-38)
+    std::vector<float> all((size_t)nshot * 3 * per);
+    for (int s = 0; s < nshot; s++) {
+        float *t = all.data() + (size_t)s * 3 * per;
+        jv_status st = jv_forward(c, s, t, t + per, t + 2 * per);
+        if (st != JV_OK) return st;
+        if (nrec > 0) {
+            const char *nm[3] = {"vx_seis_0_", "vy_seis_0_", "vz_seis_0_"};
+            for (int q = 0; q < 3; q++) {
+                std::string m = jv::write_traces(c->arg.output_path + nm[q] + std::to_string(s), t + q * per, nrec, nt);
+                if (!m.empty()) return fail(JV_EIO, m);
+            }
+        }
+    }
+    // phase 2: migrate every shot into one image (:45-122)
+    jv_status st = jv_image_reset(c);
+    if (st != JV_OK) return st;
+    for (int s = 0; s < nshot; s++) {
+        float *t = all.data() + (size_t)s * 3 * per;
+        st = jv_rtm_shot(c, s, t, t + per, t + 2 * per);
+        if (st != JV_OK) return st;
+    }
+    // Laplacian, compensation, save (:123-134)
+    const size_t n = (size_t)inf.n_phy;
+    std::vector<float> im(8 * n);
+    float *o[8];
+    for (int q = 0; q < 8; q++) o[q] = im.data() + q * n;
+    st = jv_image_finalize(c, o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7]);
+    if (st != JV_OK) return st;
+    const std::string suf = jv::size_info(inf.grid.nx, inf.grid.ny, inf.grid.nz, 0.f, 0.f, 0.f) + ".raw";
+    const char *names[6] = {"image_pp_0", "image_pp_laplace_0", "image_ps_0", "image_sp_0", "image_ss_0", nullptr};
+    const float *srcs[5] = {o[0], o[4], o[1], o[2], o[3]};
+    for (int q = 0; q < 5; q++) {
+        std::string m = jv::write_raw(c->arg.output_path + names[q] + suf, srcs[q], n);
+        if (!m.empty()) return fail(JV_EIO, m);
+    }
+    // source illumination, as a float raw image
+    std::vector<double> ip(n);
+    st = jv_image_get(c, JV_IMG_IP, ip.data());
+    if (st != JV_OK) return st;
+    std::vector<float> ipf(ip.begin(), ip.end());
+    std::string m = jv::write_raw(c->arg.output_path + "image_ipfd_0" + suf, ipf.data(), n);
+    if (!m.empty()) return fail(JV_EIO, m);
+    return JV_OK;
+}
+
+jv_status jv_last_timing(const jv_ctx *c, double *ms) {
+    if (!c || !ms) return fail(JV_EINVAL, "NULL argument");
+    *ms = c->eng->last_ms();
+    return JV_OK;
+}
+
+jv_status jv_sync(jv_ctx *c) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->sync());
+}
+
+jv_status jv_close(jv_ctx *c) {
+    delete c;
+    return JV_OK;
+}
+
+const char *jv_last_error(void) { return g_err.c_str(); }
+
+const char *jv_build_info(void) {
+    static char buf[128];
+    std::snprintf(buf, sizeof(buf), "libjv abi %d, sm_100a, nvcc %d.%d", JV_ABI_VERSION, __CUDACC_VER_MAJOR__,
+                  __CUDACC_VER_MINOR__);
+    return buf;
+}
+
+}  // extern "C"

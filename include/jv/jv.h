@@ -156,6 +156,11 @@ jv_status jv_image_get(jv_ctx *c, int kind, double *out);
 jv_status jv_image_finalize(jv_ctx *c, float *img_pp, float *img_ps, float *img_sp, float *img_ss, float *lap_pp,
                             float *lap_ps, float *lap_sp, float *lap_ss);
 
+/* Device-to-device copy of one raw stacked accumulator (FP64, gridphy) into
+ * caller memory on the context's device, e.g. to reduce images of shot
+ * replicas on several GPUs with a collective. */
+jv_status jv_image_get_device(jv_ctx *c, int kind, double *d_out);
+
 /* Whole reference job: rtm3d_blend_model_mpi_module::mpi_sub_rtm3d
  * (RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:18-135):
  * model every shot and write {output_path}v?_seis_0_{shot}.txt, migrate every
@@ -166,6 +171,16 @@ jv_status jv_run_project(jv_ctx *c);
 /* Device time (ms) of the last jv_forward* / jv_rtm_shot* call, measured
  * with CUDA events around its kernels. */
 jv_status jv_last_timing(const jv_ctx *c, double *ms);
+
+/* Per-kernel timing: with profiling on, the time loops launch kernels
+ * directly (no graphs) and bracket each launch with CUDA events on the
+ * context's stream; jv_profile_entry returns, for entry idx, the kernel
+ * name, the summed device time and the launch count since profiling was
+ * switched on (JV_EINVAL past the last entry).  The reference prints
+ * per-shot times only (cuda_tic/cuda_toc, .jarvis_0_meta/.jarvis_0_math/
+ * jarvis_2_device_math_bones.hpp:26-38). */
+jv_status jv_set_profiling(jv_ctx *c, int on);
+jv_status jv_profile_entry(const jv_ctx *c, int idx, const char **name, double *total_ms, long long *launches);
 
 /* Waits for all work of the context. */
 jv_status jv_sync(jv_ctx *c);

@@ -892,24 +892,21 @@ void jvo_finalize_image(int nx, int ny, int nz, const double *ip, double *pp, do
 double jvo_rtm_sample(const jvo_problem *p, const float *vp, const float *vs, const float *rho, int shot,
                       int steps)
 {
-    /* modelling sample */
+    /* One RTM shot's propagations (forward with boundary store, then the
+     * reverse loop with reconstruction, receiver propagation and imaging),
+     * `steps` time steps of each, on zero data of the right size. */
     ctx_t c;
     if (ctx_init(&c, p, vp, vs, rho, shot)) return -1.0;
     int nt = c.nt;
     int nrun = steps < nt ? steps : nt;
-    wave_t w;
-    if (alloc_wave(&c.g, &w, 1)) { ctx_free(&c); return -1.0; }
-    for (int it = 0; it < nrun; it++) step_forward(&c, &w, it, M_FWD, NULL, 0, NULL);
-    free_wave(&w);
     double n_ext = (double)c.g.n, n_phy = (double)c.g.px * c.g.py * c.g.pz;
     int nrec = c.nrec;
     ctx_free(&c);
-    /* migration sample on zero data of the right size */
     size_t tr = (size_t)(nrec > 0 ? nrec : 1) * (size_t)nt;
     double *z = (double *)calloc(3 * tr, sizeof(double));
     if (!z) return -1.0;
     int rc = rtm_core(p, vp, vs, rho, shot, z, z + tr, z + 2 * tr, NULL, NULL, NULL, NULL, NULL, NULL, nrun);
     free(z);
     if (rc) return -1.0;
-    return (double)nrun * (n_ext + n_ext + n_phy + n_ext);
+    return (double)nrun * (n_ext + n_phy + n_ext);
 }

@@ -101,8 +101,9 @@ void jvo_finalize_image(int nx, int ny, int nz, const double *ip,
                         double *lap_ss);
 
 /* Bounded work sample for the CPU baseline: `steps` time steps of each
- * propagation of one RTM shot (modelling, forward-with-store, and the
- * reverse loop with imaging) on the full grid.  Returns cell-updates done. */
+ * propagation of one RTM shot (forward with boundary store, and the
+ * reverse loop with reconstruction, receiver propagation and imaging) on
+ * the full grid.  Returns the cell-updates done (steps * (2 N_ext + N_phy)). */
 double jvo_rtm_sample(const jvo_problem *p, const float *vp, const float *vs,
                       const float *rho, int shot, int steps);
 

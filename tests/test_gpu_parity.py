@@ -1,0 +1,161 @@
+"""CUDA path (libjv.so, called through its C ABI) against the oracle and
+against the reference's own outputs.
+
+Tolerances (relative L2), FP32 GPU arithmetic:
+  traces vs FP64 oracle ............................. 2e-5
+  traces vs reference (7-digit text, FP32) .......... 1e-5
+  raw stacked images / Ip vs FP64 oracle ............ 5e-5
+  uncompensated images vs reference ................. 3e-5
+  Laplacian of uncompensated pp ..................... 5e-5
+  compensated images (division by small Ip) ......... 2e-3
+"""
+import numpy as np
+import pytest
+
+import make_golden as mg
+from conftest import pkg, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+jv = pkg()
+
+
+def _problem(O, s, w=None):
+    return O.Problem(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.dt, s.fm, s.T, w or s.rec_width, s.shots,
+                     s.recvs, s.vp, s.vs, s.rho)
+
+
+SMALL = [
+    dict(n=(24, 20, 18), pml=6, nt=150, seed=3),
+    dict(n=(17, 23, 13), pml=4, nt=120, seed=5, shot_idx=[(3, 20, 2)]),   # source near faces, pml at minimum
+    dict(n=(40, 9, 11), pml=9, nt=100, seed=8, nrec=30),                  # random receivers anywhere
+    dict(n=(8, 8, 8), pml=5, nt=60, seed=9, shot_idx=[(4, 4, 4)]),        # smallest allowed grid
+]
+
+
+@pytest.mark.parametrize("kw", SMALL)
+@pytest.mark.parametrize("graphs", [1, 0])
+def test_forward_vs_oracle(oracle, synth, kw, graphs):
+    s = synth.small_case(**kw)
+    ref = oracle.forward(_problem(oracle, s))
+    with jv.Context.from_survey(s, use_graphs=graphs, graph_steps=7) as ctx:
+        tr = ctx.forward(0)
+    assert tr[0].shape == ref[0].shape
+    for a, b in zip(tr, ref):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
+
+
+@pytest.mark.parametrize("name", list(mg.CASES))
+def test_pins_vs_reference(synth, name):
+    """Traces and images of the full reference job against the reference's
+    own outputs (tests/golden/ref_*.npz)."""
+    s = mg.case_survey(name)
+    f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_{name}.npz")
+    with jv.Context.from_survey(s) as ctx:
+        ctx.image_reset()
+        for sh in range(s.shots.shape[0]):
+            tr = ctx.forward(sh)
+            for c, t in zip(("vx", "vy", "vz"), tr):
+                assert rel_l2(t, f[f"tr_{c}_{sh}"]) <= 1e-5, (sh, c, rel_l2(t, f[f"tr_{c}_{sh}"]))
+            ctx.rtm_shot(sh, tr)
+        raw = ctx.images()
+        comp, lap = ctx.finalize()
+    ip = f["img_ip"].astype(np.float64)
+    assert rel_l2(raw["ip"], ip) <= 5e-5
+    assert rel_l2(lap["pp"], f["lap_pp"]) <= 5e-5
+    for k in ("pp", "ps", "sp", "ss"):
+        unc = f["img_" + k].astype(np.float64) * np.where(ip > 3.4e-38, ip, 1.0)
+        assert rel_l2(raw[k], unc) <= 3e-5, (k, rel_l2(raw[k], unc))
+        assert rel_l2(comp[k], f["img_" + k]) <= 2e-3, (k, rel_l2(comp[k], f["img_" + k]))
+
+
+@pytest.mark.parametrize("w", [1, 2, 3, 4])
+def test_rtm_vs_oracle(oracle, synth, w):
+    s = synth.small_case(n=(22, 18, 20), pml=6, nt=140, seed=21, rec_width=w, anomaly=(0.1, 3.0),
+                         shot_idx=[(11, 9, 3)])
+    p = _problem(oracle, s, w)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    obs32 = [o.astype(np.float32) for o in obs]
+    with jv.Context.from_survey(s) as ctx:
+        ctx.rtm_shot(0, obs32)
+        raw = ctx.images()
+        comp, lap = ctx.finalize()
+    for k in ("ip", "pp", "ps", "sp", "ss"):
+        assert np.all(np.isfinite(raw[k]))
+        assert rel_l2(raw[k], ref[k]) <= 5e-5, (w, k, rel_l2(raw[k], ref[k]))
+    rc, rl = oracle.finalize_image(ref, s.nx, s.ny, s.nz)
+    for k in ("pp", "ps", "sp", "ss"):
+        assert rel_l2(lap[k], rl[k]) <= 5e-5
+        assert rel_l2(comp[k], rc[k]) <= 2e-3
+
+
+def test_images_stack_over_shots(synth):
+    s = synth.small_case(n=(20, 16, 14), pml=5, nt=90, seed=4, shot_idx=[(5, 5, 2), (14, 10, 3)])
+    with jv.Context.from_survey(s) as ctx:
+        obs = [ctx.forward(i) for i in range(2)]
+        singles = []
+        for i in range(2):
+            ctx.image_reset()
+            ctx.rtm_shot(i, obs[i])
+            singles.append(ctx.images())
+        ctx.image_reset()
+        for i in range(2):
+            ctx.rtm_shot(i, obs[i])
+        both = ctx.images()
+    for k in both:
+        assert rel_l2(both[k], singles[0][k] + singles[1][k]) <= 1e-12
+
+
+def test_repeatable_and_graph_equivalent(synth):
+    s = synth.small_case(n=(21, 19, 17), pml=6, nt=75, seed=12)
+    outs = []
+    for graphs, steps in ((1, 32), (1, 5), (0, 0)):
+        with jv.Context.from_survey(s, use_graphs=graphs, graph_steps=steps) as ctx:
+            a = ctx.forward(0)
+            b = ctx.forward(0)
+            ctx.rtm_shot(0, a)
+            outs.append((a, b, ctx.image(jv.IMG_PP)))
+    for a, b, im in outs:
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+        assert np.array_equal(im, outs[0][2])
+        for x, y in zip(a, outs[0][0]):
+            assert np.array_equal(x, y)
+
+
+def test_project_roundtrip(tmp_path, synth, project):
+    """jv_open + jv_run_project write the reference's files, readable with
+    the reference's formats and equal to the in-memory results."""
+    s = mg.case_survey("pin_w1")
+    d = str(tmp_path / "proj")
+    project.write_project(d, s)
+    f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_pin_w1.npz")
+    with jv.Context.open(d + "/") as ctx:
+        i = ctx.info()
+        assert (i.grid.nx, i.grid.ny, i.grid.nz, i.nt, i.n_recv) == (s.nx, s.ny, s.nz, s.nt, s.recvs.shape[0])
+        ctx.run_project()
+    for sh in range(s.shots.shape[0]):
+        for c in ("vx", "vy", "vz"):
+            t = project.read_traces(f"{d}/out/{c}_seis_0_{sh}.txt")
+            assert rel_l2(t, f[f"tr_{c}_{sh}"]) <= 1e-5
+    suf = project.size_info(s.nx, s.ny, s.nz)
+    pp = np.fromfile(f"{d}/out/image_pp_0{suf}.raw", np.float32).reshape(s.nz, s.ny, s.nx)
+    lp = np.fromfile(f"{d}/out/image_pp_laplace_0{suf}.raw", np.float32).reshape(s.nz, s.ny, s.nx)
+    assert rel_l2(pp, f["img_pp"]) <= 2e-3
+    assert rel_l2(lp, f["lap_pp"]) <= 5e-5
+
+
+def test_errors_are_status_codes(synth):
+    s = synth.small_case(n=(12, 12, 12), pml=5, nt=20)
+    with jv.Context.from_survey(s) as ctx:
+        with pytest.raises(jv.JvError) as e:
+            ctx.forward(5)
+        assert e.value.code == jv.JV_EINVAL
+        with pytest.raises(jv.JvError):
+            ctx.image(9)
+        ctx.set_geometry(np.array([[1e6, 0, 0]], np.float32), s.recvs)
+        with pytest.raises(jv.JvError) as e:
+            ctx.forward(0)
+        assert "outside gridphy" in str(e.value)
