@@ -57,7 +57,8 @@ class Grid(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("rec_width", C.c_int), ("precision", C.c_int), ("store_mode", C.c_int),
-                ("use_graphs", C.c_int), ("graph_steps", C.c_int), ("store_budget", C.c_size_t)]
+                ("use_graphs", C.c_int), ("graph_steps", C.c_int), ("store_budget", C.c_size_t),
+                ("kernel_variant", C.c_int), ("zchunk", C.c_int)]
 
 
 class Info(C.Structure):

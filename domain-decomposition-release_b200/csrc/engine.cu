@@ -10,6 +10,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace jv {
@@ -136,6 +137,10 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     E->fm_ = fm;
     E->nt_ = nt;
     E->dev_ = opt.device;
+    E->kc_.variant = opt.kernel_variant;
+    E->kc_.zchunk = opt.zchunk;
+    const char *cf = std::getenv("JV_CHECK_FINITE");
+    E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
     if (!s) {
         delete E;
@@ -421,6 +426,44 @@ bool Engine::profile_entry(int i, const char **name, double *ms, long long *laun
     return true;
 }
 
+Status Engine::check_finite(const char *after) {
+    if (!nf_) {
+        void *p;
+        JV_TRY(alloc(&p, 8 * sizeof(unsigned long long)));
+        nf_ = (unsigned long long *)p;
+    }
+    JV_CU(cudaMemsetAsync(nf_, 0, 8 * sizeof(unsigned long long), stream_));
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    JV_K(k_count_nonfinite(F_.f[0], kNumFld * field_elems_, 0, nf_ + 0, stream_));
+    if (R_.f[0]) JV_K(k_count_nonfinite(R_.f[0], kNumFld * field_elems_, 0, nf_ + 1, stream_));
+    JV_K(k_count_nonfinite(img_.ip, 5 * nphy, 1, nf_ + 2, stream_));
+    unsigned long long h[8];
+    JV_CU(cudaMemcpyAsync(h, nf_, sizeof(h), cudaMemcpyDeviceToHost, stream_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    if (h[0] || h[1] || h[2]) {
+        StepState sh;
+        JV_CU(cudaMemcpy(&sh, st_, sizeof(sh), cudaMemcpyDeviceToHost));
+        int fld[2] = {-1, -1};
+        for (int w = 0; w < 2; w++) {
+            const WaveDev &W = w == 0 ? F_ : R_;
+            if (!h[w] || !W.f[0]) continue;
+            for (int f = 0; f < kNumFld && fld[w] < 0; f++) {
+                JV_CU(cudaMemsetAsync(nf_ + 4, 0, sizeof(unsigned long long), stream_));
+                JV_K(k_count_nonfinite(W.f[f], field_elems_, 0, nf_ + 4, stream_));
+                unsigned long long c = 0;
+                JV_CU(cudaMemcpy(&c, nf_ + 4, sizeof(c), cudaMemcpyDeviceToHost));
+                if (c) fld[w] = f;
+            }
+        }
+        return bad(JV_ECUDA, std::string("non-finite values after ") + after + " (step kind " +
+                                 std::to_string(cur_kind_) + ", it " + std::to_string(sh.it) +
+                                 "): F " + std::to_string(h[0]) + " (first field " + std::to_string(fld[0]) +
+                                 "), R " + std::to_string(h[1]) + " (first field " + std::to_string(fld[1]) +
+                                 "), images " + std::to_string(h[2]));
+    }
+    return Status{};
+}
+
 // launch one kernel, bracketed by timing events when profiling
 #define JV_L(name, expr)                                                    \
     do {                                                                    \
@@ -433,42 +476,44 @@ bool Engine::profile_entry(int i, const char **name, double *ms, long long *laun
         } else {                                                            \
             JV_K(expr);                                                     \
         }                                                                   \
+        if (check_finite_) JV_TRY(check_finite(name));                      \
     } while (0)
 
 Status Engine::launch_step(int kind) {
+    cur_kind_ = kind;
     void *s = (void *)stream_;
     const float dt = dt_;
     const int rw = opt_.rec_width;
     switch (kind) {
     case kStepModel:
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
-        JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, s));
-        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
         JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, s));
         JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
-        JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, s));
         JV_L("vowr_pack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, 0, nslot_, 1, 0, s));
-        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
         JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmRev:
         // UPDATE 1: source subtraction (fused) + backward stress, receiver
         // injection + reverse velocity, stress boundary layers of step it-1
         JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, s));
-        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, s));
+        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, kc_, s));
         JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, s));
-        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, s));
+        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
-        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, s));
+        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, kc_, s));
         JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, s));
-        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, s));
+        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 1, s));
         JV_L("step_advance", k_step_advance(st_, -1, s));
         break;
@@ -479,7 +524,7 @@ Status Engine::launch_step(int kind) {
 
 Status Engine::run_loop(int kind, int nsteps) {
     if (nsteps <= 0) return Status{};
-    if (!opt_.use_graphs || prof_) {
+    if (!opt_.use_graphs || prof_ || check_finite_) {
         for (int i = 0; i < nsteps; i++) {
             JV_TRY(launch_step(kind));
             if (prof_ && prof_pending_.size() > 4096) JV_TRY(prof_collect());

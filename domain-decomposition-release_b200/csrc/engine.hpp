@@ -83,6 +83,7 @@ class Engine {
     double last_ms_ = 0.0;
 
     GridDev g_{};
+    KCfg kc_{};
     size_t field_elems_ = 0;  // elements per pitched field
     std::vector<void *> allocs_;
     size_t dev_bytes_ = 0;
@@ -128,6 +129,13 @@ class Engine {
     int prof_id(const char *name);
     cudaEvent_t prof_event();
     Status prof_collect();
+
+    // JV_CHECK_FINITE=1: after every launch, count non-finite values of
+    // both wavefields and the image stacks (direct launches, no graphs)
+    bool check_finite_ = false;
+    unsigned long long *nf_ = nullptr;
+    int cur_kind_ = -1;
+    Status check_finite(const char *after);
 };
 
 // kinds of time-loop steps

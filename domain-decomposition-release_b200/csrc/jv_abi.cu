@@ -66,6 +66,8 @@ void jv_options_default(jv_options *o) {
     o->use_graphs = 1;
     o->graph_steps = 0;
     o->store_budget = 0;
+    o->kernel_variant = 1;
+    o->zchunk = 0;
 }
 
 jv_status jv_create(const jv_grid *grid, const float *vp, const float *vs, const float *rho, float dt, float fm,

@@ -79,15 +79,22 @@ struct StepState {
     const float *obs[3]; // traces injected into the receiver wavefield
 };
 
+// interior-kernel choice: variant 0 = one z plane per block, 1 = z-marching
+// over chunks of zchunk planes (0: the whole column)
+struct KCfg {
+    int variant = 1;
+    int zchunk = 0;
+};
+
 // kernels.cu ------------------------------------------------------------
 int k_model_prep(const GridDev &g, const float *d_vp_phy, const float *d_vs_phy, const float *d_rho_phy,
                  float *vp, float *rho, float *lam, float *mu, void *stream);
 int k_zero_range(float *p, size_t n, void *stream);
 
 int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w,
-              const WaveDev *rev, const ImageDev *img, void *stream);
+              const WaveDev *rev, const ImageDev *img, const KCfg &kc, void *stream);
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,
-                 int rec_w, const float *wavelet, const StepState *st, void *stream);
+                 int rec_w, const float *wavelet, const StepState *st, const KCfg &kc, void *stream);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
               void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
@@ -100,5 +107,6 @@ int k_vowr(const GridDev &g, const WaveDev &w, const SegDev *segs, int nseg, lon
 int k_step_advance(StepState *st, int delta, void *stream);
 int k_image_finalize(const GridDev &g, const ImageDev &img, float *out /* 8 arrays */, void *stream);
 int upload_coefficients(const float list[5][4], const float dc2[2]);
+int k_count_nonfinite(const void *p, size_t n, int is_double, unsigned long long *out, void *stream);
 
 }  // namespace jv

@@ -206,6 +206,214 @@ __global__ void __launch_bounds__(kTX *kTY) stress_phy(GridDev g, WaveDev w, con
     if (MODE != kFwd) w.f[SAU][i] += a * l2m * vx_x + b * l2m * vy_y + c * l2m * vz_z;
 }
 
+// ------------------------------------------------- z-marching variants
+//
+// One thread per (x, y) column of a 32 x 8 tile, marching over a chunk of
+// z planes.  The z-derivatives come from register windows holding planes
+// k-4 .. k+4 of the fields that need them, so every value is loaded once
+// per chunk; x/y neighbours are read through L1.
+
+// window helpers: w[4] is plane k
+__device__ __forceinline__ float win_dp(const float *w, const float *c, int o) {
+    float t = 0.f;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        if (r < o) t += c[r] * (w[4 + r + 1] - w[4 - r]);
+    return t;
+}
+__device__ __forceinline__ float win_dm(const float *w, const float *c, int o) {
+    float t = 0.f;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        if (r < o) t += c[r] * (w[4 + r] - w[4 - r - 1]);
+    return t;
+}
+
+template <int MODE, bool IMG>
+__global__ void __launch_bounds__(kTX *kTY) vel_phy_zm(GridDev g, WaveDev w, const float *__restrict__ rho, float dt,
+                                                      int rec_w, WaveDev rv, ImageDev img, int zc) {
+    const int pi = blockIdx.x * kTX + threadIdx.x;
+    const int pj = blockIdx.y * kTY + threadIdx.y;
+    const int k0 = blockIdx.z * zc;
+    const int k1 = min(k0 + zc, g.pz);
+    if (pi >= g.px || pj >= g.py || k0 >= k1) return;
+    constexpr bool kP = (MODE == kBwd || MODE == kRev);
+    const long long sy = g.sy, sz = g.sz;
+    long long i = g.xoff + (pi + g.m) + sy * (pj + g.m) + sz * (k0 + g.m);
+    const float *sxx = w.f[SXX], *syy = w.f[SYY], *szz = w.f[SZZ];
+    const float *sxy = w.f[SXY], *sxz = w.f[SXZ], *syz = w.f[SYZ], *sau = w.f[SAU];
+    float wzz[9], wxz[9], wyz[9], wau[9];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const long long o = i + (q - 4) * sz;
+        wzz[q] = ld(szz, o);
+        wxz[q] = ld(sxz, o);
+        wyz[q] = ld(syz, o);
+        if (kP) wau[q] = ld(sau, o);
+    }
+    int ox = kPhyHalf, oy = kPhyHalf;
+    if (MODE == kBwd) {
+        ox = rim_order(pi, g.px, rec_w);
+        oy = rim_order(pj, g.py, rec_w);
+    }
+    const float *cx = c_list[ox], *cy = c_list[oy];
+    const float rdx = 1.0f / g.dx;
+    (void)rdx;
+    for (int k = k0; k < k1; k++, i += sz) {
+        const long long o = i + 4 * sz;
+        wzz[8] = ld(szz, o);
+        wxz[8] = ld(sxz, o);
+        wyz[8] = ld(syz, o);
+        if (kP) wau[8] = ld(sau, o);
+        int oz = kPhyHalf;
+        if (MODE == kBwd) oz = rim_order(k, g.pz, rec_w);
+        const float *cz = c_list[oz];
+        float sxx_x, syx_x, szx_x, sxy_y, syy_y, szy_y, sau_x = 0.f, sau_y = 0.f;
+        if (MODE == kBwd) {
+            sxx_x = dpv(sxx, i, 1, cx, ox);
+            syx_x = dmv(sxy, i, 1, cx, ox);
+            szx_x = dmv(sxz, i, 1, cx, ox);
+            sxy_y = dmv(sxy, i, sy, cy, oy);
+            syy_y = dpv(syy, i, sy, cy, oy);
+            szy_y = dmv(syz, i, sy, cy, oy);
+            sau_x = dpv(sau, i, 1, cx, ox);
+            sau_y = dpv(sau, i, sy, cy, oy);
+        } else {
+            sxx_x = dp<4>(sxx, i, 1, cx);
+            syx_x = dm<4>(sxy, i, 1, cx);
+            szx_x = dm<4>(sxz, i, 1, cx);
+            sxy_y = dm<4>(sxy, i, sy, cy);
+            syy_y = dp<4>(syy, i, sy, cy);
+            szy_y = dm<4>(syz, i, sy, cy);
+            if (kP) {
+                sau_x = dp<4>(sau, i, 1, cx);
+                sau_y = dp<4>(sau, i, sy, cy);
+            }
+        }
+        const float sxz_z = win_dm(wxz, cz, oz);
+        const float syz_z = win_dm(wyz, cz, oz);
+        const float szz_z = win_dp(wzz, cz, oz);
+        const float sau_z = kP ? win_dp(wau, cz, oz) : 0.f;
+        const float dtr = dt / ld(rho, i);
+        const float a = dtr / g.dx, b = dtr / g.dy, c = dtr / g.dz;
+        const float vx = w.f[VX][i] + (a * sxx_x + b * sxy_y + c * sxz_z);
+        const float vy = w.f[VY][i] + (a * syx_x + b * syy_y + c * syz_z);
+        const float vz = w.f[VZ][i] + (a * szx_x + b * szy_y + c * szz_z);
+        w.f[VX][i] = vx;
+        w.f[VY][i] = vy;
+        w.f[VZ][i] = vz;
+        if (kP) {
+            const float px = w.f[VXP][i] + a * sau_x;
+            const float py = w.f[VYP][i] + b * sau_y;
+            const float pz = w.f[VZP][i] + c * sau_z;
+            w.f[VXP][i] = px;
+            w.f[VYP][i] = py;
+            w.f[VZP][i] = pz;
+            if (IMG) {
+                const float rpx = ld(rv.f[VXP], i), rpy = ld(rv.f[VYP], i), rpz = ld(rv.f[VZP], i);
+                const float rsx = ld(rv.f[VX], i) - rpx, rsy = ld(rv.f[VY], i) - rpy, rsz = ld(rv.f[VZ], i) - rpz;
+                const float ssx = vx - px, ssy = vy - py, ssz = vz - pz;
+                const long long q = pi + (long long)g.px * (pj + (long long)g.py * k);
+                img.ip[q] += (double)(px * px + py * py + pz * pz);
+                img.pp[q] += (double)(px * rpx + py * rpy + pz * rpz);
+                img.ps[q] += (double)(px * rsx + py * rsy + pz * rsz);
+                img.sp[q] += (double)(ssx * rpx + ssy * rpy + ssz * rpz);
+                img.ss[q] += (double)(ssx * rsx + ssy * rsy + ssz * rsz);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            wzz[q] = wzz[q + 1];
+            wxz[q] = wxz[q + 1];
+            wyz[q] = wyz[q + 1];
+            if (kP) wau[q] = wau[q + 1];
+        }
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kTX *kTY) stress_phy_zm(GridDev g, WaveDev w, const float *__restrict__ lam,
+                                                         const float *__restrict__ mu, float dt, int rec_w,
+                                                         const float *__restrict__ wavelet,
+                                                         const StepState *__restrict__ st, int zc) {
+    const int pi = blockIdx.x * kTX + threadIdx.x;
+    const int pj = blockIdx.y * kTY + threadIdx.y;
+    const int k0 = blockIdx.z * zc;
+    const int k1 = min(k0 + zc, g.pz);
+    if (pi >= g.px || pj >= g.py || k0 >= k1) return;
+    const long long sy = g.sy, sz = g.sz;
+    long long i = g.xoff + (pi + g.m) + sy * (pj + g.m) + sz * (k0 + g.m);
+    const float *vxf = w.f[VX], *vyf = w.f[VY], *vzf = w.f[VZ];
+    float wx[9], wy[9], wz[9];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const long long o = i + (q - 4) * sz;
+        wx[q] = ld(vxf, o);
+        wy[q] = ld(vyf, o);
+        wz[q] = ld(vzf, o);
+    }
+    int ox = kPhyHalf, oy = kPhyHalf;
+    if (MODE == kBwd) {
+        ox = rim_order(pi, g.px, rec_w);
+        oy = rim_order(pj, g.py, rec_w);
+    }
+    const float *cx = c_list[ox], *cy = c_list[oy];
+    const long long src = (MODE != kRev) ? st->src : -1;
+    const float a = dt / g.dx, b = dt / g.dy, c = dt / g.dz;
+    for (int k = k0; k < k1; k++, i += sz) {
+        const long long o = i + 4 * sz;
+        wx[8] = ld(vxf, o);
+        wy[8] = ld(vyf, o);
+        wz[8] = ld(vzf, o);
+        int oz = kPhyHalf;
+        if (MODE == kBwd) oz = rim_order(k, g.pz, rec_w);
+        const float *cz = c_list[oz];
+        float vx_x, vy_x, vz_x, vx_y, vy_y, vz_y;
+        if (MODE == kBwd) {
+            vx_x = dmv(vxf, i, 1, cx, ox);
+            vy_x = dpv(vyf, i, 1, cx, ox);
+            vz_x = dpv(vzf, i, 1, cx, ox);
+            vx_y = dpv(vxf, i, sy, cy, oy);
+            vy_y = dmv(vyf, i, sy, cy, oy);
+            vz_y = dpv(vzf, i, sy, cy, oy);
+        } else {
+            vx_x = dm<4>(vxf, i, 1, cx);
+            vy_x = dp<4>(vyf, i, 1, cx);
+            vz_x = dp<4>(vzf, i, 1, cx);
+            vx_y = dp<4>(vxf, i, sy, cy);
+            vy_y = dm<4>(vyf, i, sy, cy);
+            vz_y = dp<4>(vzf, i, sy, cy);
+        }
+        const float vx_z = win_dp(wx, cz, oz);
+        const float vy_z = win_dp(wy, cz, oz);
+        const float vz_z = win_dm(wz, cz, oz);
+        const float l = ld(lam, i), m = ld(mu, i);
+        const float l2m = l + 2.0f * m;
+        float sxx = w.f[SXX][i], syy = w.f[SYY][i], szz = w.f[SZZ][i];
+        if (MODE != kRev && i == src) {
+            const float s = wavelet[st->it];
+            if (MODE == kBwd) {
+                sxx -= s; syy -= s; szz -= s;
+            } else {
+                sxx += s; syy += s; szz += s;
+            }
+        }
+        w.f[SXX][i] = sxx + (a * l2m * vx_x + b * l * vy_y + c * l * vz_z);
+        w.f[SYY][i] = syy + (a * l * vx_x + b * l2m * vy_y + c * l * vz_z);
+        w.f[SZZ][i] = szz + (a * l * vx_x + b * l * vy_y + c * l2m * vz_z);
+        w.f[SXY][i] += a * m * vy_x + b * m * vx_y;
+        w.f[SXZ][i] += a * m * vz_x + c * m * vx_z;
+        w.f[SYZ][i] += b * m * vz_y + c * m * vy_z;
+        if (MODE != kFwd) w.f[SAU][i] += a * l2m * vx_x + b * l2m * vy_y + c * l2m * vz_z;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            wx[q] = wx[q + 1];
+            wy[q] = wy[q + 1];
+            wz[q] = wz[q + 1];
+        }
+    }
+}
+
 // ---------------------------------------------------------------- CPML
 
 // Damping coefficients of one axis at extended index c
@@ -298,7 +506,7 @@ __global__ void __launch_bounds__(256) vel_pml(GridDev g, CpmlDev P, WaveDev w, 
     w.f[VZ][i] += dtr * (szx_x + szy_y + szz_z);
 }
 
-template <bool SAU>
+template <bool WITH_SAU>
 __global__ void __launch_bounds__(256) stress_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ lam,
                                                   const float *__restrict__ mu, const float *__restrict__ vpm) {
     const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -347,7 +555,7 @@ __global__ void __launch_bounds__(256) stress_pml(GridDev g, CpmlDev P, WaveDev 
     w.f[SXX][i] += dt * (l2m * vx_x + l * vy_y + l * vz_z);
     w.f[SYY][i] += dt * (l * vx_x + l2m * vy_y + l * vz_z);
     w.f[SZZ][i] += dt * (l * vx_x + l * vy_y + l2m * vz_z);
-    if (SAU) w.f[SAU][i] += dt * (l2m * vx_x + l2m * vy_y + l2m * vz_z);
+    if (WITH_SAU) w.f[SAU][i] += dt * (l2m * vx_x + l2m * vy_y + l2m * vz_z);
     w.f[SXY][i] += dt * m * (vy_x + vx_y);
     w.f[SXZ][i] += dt * m * (vz_x + vx_z);
     w.f[SYZ][i] += dt * m * (vz_y + vy_z);
@@ -411,6 +619,19 @@ __global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, const SegDev *
 }
 
 __global__ void step_advance(StepState *st, int delta) { st->it += delta; }
+
+__global__ void count_nonfinite_f(const float *p, size_t n, unsigned long long *out) {
+    unsigned long long c = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        c += !isfinite(p[i]);
+    if (c) atomicAdd(out, c);
+}
+__global__ void count_nonfinite_d(const double *p, size_t n, unsigned long long *out) {
+    unsigned long long c = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        c += !isfinite(p[i]);
+    if (c) atomicAdd(out, c);
+}
 
 // ---------------------------------------------------------- model prep
 
@@ -494,11 +715,26 @@ int k_zero_range(float *p, size_t n, void *stream) {
 }
 
 int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w, const WaveDev *rev,
-              const ImageDev *img, void *stream) {
-    dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
+              const ImageDev *img, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     WaveDev rv = rev ? *rev : WaveDev{};
     ImageDev im = img ? *img : ImageDev{};
+    if (kc.variant == 1) {
+        const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
+        dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, (g.pz + zc - 1) / zc);
+        switch (mode) {
+        case kFwd: vel_phy_zm<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc); break;
+        case kRtmFwd: vel_phy_zm<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc); break;
+        case kRev: vel_phy_zm<kRev, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc); break;
+        case kBwd:
+            if (img && rev) vel_phy_zm<kBwd, true><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc);
+            else vel_phy_zm<kBwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc);
+            break;
+        default: return (int)cudaErrorInvalidValue;
+        }
+        return cerr();
+    }
+    dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
     switch (mode) {
     case kFwd: vel_phy<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
     case kRtmFwd: vel_phy<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
@@ -513,9 +749,21 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 }
 
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt, int rec_w,
-                 const float *wavelet, const StepState *st, void *stream) {
-    dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
+                 const float *wavelet, const StepState *st, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
+    if (kc.variant == 1) {
+        const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
+        dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, (g.pz + zc - 1) / zc);
+        switch (mode) {
+        case kFwd: stress_phy_zm<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
+        case kRtmFwd: stress_phy_zm<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
+        case kBwd: stress_phy_zm<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
+        case kRev: stress_phy_zm<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
+        default: return (int)cudaErrorInvalidValue;
+        }
+        return cerr();
+    }
+    dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
     switch (mode) {
     case kFwd: stress_phy<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
     case kRtmFwd: stress_phy<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
@@ -564,6 +812,13 @@ int k_vowr(const GridDev &g, const WaveDev &w, const SegDev *segs, int nseg, lon
 
 int k_step_advance(StepState *st, int delta, void *stream) {
     step_advance<<<1, 1, 0, (cudaStream_t)stream>>>(st, delta);
+    return cerr();
+}
+
+int k_count_nonfinite(const void *p, size_t n, int is_double, unsigned long long *out, void *stream) {
+    if (n == 0) return 0;
+    if (is_double) count_nonfinite_d<<<148 * 4, 256, 0, (cudaStream_t)stream>>>((const double *)p, n, out);
+    else count_nonfinite_f<<<148 * 4, 256, 0, (cudaStream_t)stream>>>((const float *)p, n, out);
     return cerr();
 }
 
