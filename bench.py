@@ -250,6 +250,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--ref-sample-steps", type=int, default=40)
+    ap.add_argument("--variant", type=int, default=None, help="interior kernel variant (default: library default)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -270,7 +271,8 @@ def main():
 
     jv = importlib.import_module("domain-decomposition-release_b200")
     s = survey(args, jv.synth)
-    ctx = jv.Context.from_survey(s, device=local)
+    kopts = {} if args.variant is None else {"kernel_variant": args.variant}
+    ctx = jv.Context.from_survey(s, device=local, **kopts)
     info = ctx.info()
     nrec, nt = info.n_recv, info.nt
     obs = torch.empty((3, nrec, nt), dtype=torch.float32, device=f"cuda:{local}")

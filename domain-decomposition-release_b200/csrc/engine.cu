@@ -8,6 +8,7 @@
 //  RTM = .../elastic_1_rtm3d_model_mpi, relative to the reference root).
 #include "engine.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -178,12 +179,14 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     g_.sz = g_.sy * g_.ny;
     g_.dx = grid_.dx; g_.dy = grid_.dy; g_.dz = grid_.dz;
     field_elems_ = (size_t)round_up(g_.sz * g_.nz + 64, 64);
+    if (field_elems_ >= (size_t)1 << 31) return bad(JV_EINVAL, "gridext too large for 32-bit element offsets");
 
     // model
     void *p;
     JV_TRY(alloc(&p, 4 * field_elems_ * sizeof(float)));
     float *mb = (float *)p;
     vp_ = mb; rho_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
+    JV_CU(cudaMemsetAsync(mb, 0, 4 * field_elems_ * sizeof(float), stream_));
     const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
     float *tmp = nullptr;
     JV_CU(cudaMalloc(&tmp, 3 * nphy * sizeof(float)));
@@ -199,45 +202,99 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_TRY(alloc(&p, kNumFld * field_elems_ * sizeof(float)));
     for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + f * field_elems_;
 
-    // CPML slabs for one wavefield
-    auto make_cpml = [&](CpmlDev &c) -> Status {
+    // CPML geometry: six slabs covering gridext outside gridphy and outside
+    // the 2-cell outer rim (FD/fdtd3d_0_base_module/fdtd3d_base_6_pml_meat.hpp:29-94),
+    // split into x segments (one warp each); rows and axis tables are shared
+    // by both wavefields, the memory-variable arenas are per wavefield
+    {
         const int NX = g_.nx, NY = g_.ny, NZ = g_.nz;
-        int bx[6][6] = {
+        const int bx[6][6] = {
             {2, NX - 2, 2, NY - 2, 2, m},           {2, NX - 2, 2, NY - 2, NZ - m, NZ - 2},
             {2, NX - 2, 2, m, m, NZ - m},           {2, NX - 2, NY - m, NY - 2, m, NZ - m},
             {2, m, m, NY - m, m, NZ - m},           {NX - m, NX - 2, m, NY - m, m, NZ - m},
         };
-        int na[6] = {3, 3, 2, 2, 1, 1};
-        long long first = 0, psi_total = 0;
-        for (int s = 0; s < 6; s++) {
-            SlabDev &S = c.s[s];
-            S.x0 = bx[s][0]; S.x1 = bx[s][1]; S.y0 = bx[s][2]; S.y1 = bx[s][3]; S.z0 = bx[s][4]; S.z1 = bx[s][5];
-            S.naxes = na[s];
-            S.ncell = (long long)(S.x1 - S.x0) * (S.y1 - S.y0) * (S.z1 - S.z0);
-            if (S.ncell < 0) S.ncell = 0;
-            S.first = first;
-            first += S.ncell;
-            psi_total += 6LL * S.naxes * S.ncell;
-        }
-        c.total = first;
-        void *q;
-        JV_TRY(alloc(&q, (size_t)psi_total * sizeof(float)));
+        const int na[6] = {3, 3, 2, 2, 1, 1};
         long long off = 0;
-        for (int s = 0; s < 6; s++) {
-            c.s[s].psi = (float *)q + off;
-            off += 6LL * c.s[s].naxes * c.s[s].ncell;
+        std::vector<PmlRow> rows;
+        for (int q = 0; q < 6; q++) {
+            SlabDev S{};
+            S.x0 = bx[q][0]; S.x1 = bx[q][1]; S.y0 = bx[q][2]; S.y1 = bx[q][3]; S.z0 = bx[q][4]; S.z1 = bx[q][5];
+            S.naxes = na[q];
+            if (S.x1 <= S.x0 || S.y1 <= S.y0 || S.z1 <= S.z0) continue;
+            S.ncell = (long long)(S.x1 - S.x0) * (S.y1 - S.y0) * (S.z1 - S.z0);
+            S.psi_off = off;
+            off += 6LL * S.naxes * S.ncell;
+            slabs_.push_back(S);
+            for (int z = S.z0; z < S.z1; z++)
+                for (int y = S.y0; y < S.y1; y++) {
+                    PmlRow r{};
+                    r.x0 = S.x0; r.len = S.x1 - S.x0; r.y = y; r.z = z;
+                    r.naxes = S.naxes;
+                    r.ncell = S.ncell;
+                    r.psi_off = S.psi_off + ((long long)(z - S.z0) * (S.y1 - S.y0) + (y - S.y0)) * (S.x1 - S.x0);
+                    rows.push_back(r);
+                }
         }
-        c.fm = fm_;
-        c.dt = dt_;
-        c.l10x7 = std::log10(1.0f / 0.001f) * 7.0f;
-        c.N = (float)(m - kPmlHalf);
-        c.twoNdx = 2.0f * c.N * grid_.dx;
-        c.twoNdy = 2.0f * c.N * grid_.dy;
-        c.twoNdz = 2.0f * c.N * grid_.dz;
-        c.alpha_max = (float)(3.14159265358979323846 * (double)fm_);
-        return Status{};
-    };
-    JV_TRY(make_cpml(cpF_));
+        // long rows (z- and y-slabs, full x extent) first, then the x-slab
+        // rows; within each class neighbouring rows run together
+        const int longlen = NX - 4;
+        std::sort(rows.begin(), rows.end(), [longlen](const PmlRow &u, const PmlRow &v) {
+            const bool lu = u.len == longlen, lv = v.len == longlen;
+            if (lu != lv) return lu;
+            if (u.z != v.z) return u.z < v.z;
+            if (u.y != v.y) return u.y < v.y;
+            return u.x0 < v.x0;
+        });
+        nlong_ = 0;
+        int shortmax = 1;
+        for (const PmlRow &r : rows) {
+            if (r.len == longlen) nlong_++;
+            else shortmax = std::max(shortmax, r.len);
+        }
+        cpl_ = (longlen + 31) / 32;
+        cps_ = (shortmax + 31) / 32;
+        psi_total_ = off;
+        nrows_ = (int)rows.size();
+        if (nrows_ > 0) {
+            JV_TRY(alloc(&p, rows.size() * sizeof(PmlRow)));
+            rows_d_ = (PmlRow *)p;
+            JV_CU(cudaMemcpy(rows_d_, rows.data(), rows.size() * sizeof(PmlRow), cudaMemcpyHostToDevice));
+        }
+        // per-axis damping factors: d = vp * K, K = log10(1/R) 7 (s/N)^2 / (2 N delta)
+        // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620)
+        const double N = (double)(m - kPmlHalf);
+        const double l10x7 = (double)(std::log10(1.0f / 0.001f) * 7.0f);
+        const float alpha_max = (float)(3.14159265358979323846 * (double)fm_);
+        const int nax[3] = {NX, NY, NZ};
+        const float del[3] = {grid_.dx, grid_.dy, grid_.dz};
+        for (int a = 0; a < 3; a++) {
+            const int n = nax[a];
+            std::vector<float4> t(n, make_float4(0.f, 0.f, 0.f, 0.f));
+            for (int c = 0; c < n; c++) {
+                double sI, sH;
+                if (c >= kPmlHalf && c < m) {
+                    sI = m - c;
+                    sH = m - c - 0.5;
+                } else if (c >= n - m && c < n - kPmlHalf) {
+                    sH = c - (n - m - 1);
+                    sI = sH - 0.5;
+                } else {
+                    continue;
+                }
+                const double k0 = l10x7 / (2.0 * N * (double)del[a]);
+                const float qI = (float)sI / (float)N, qH = (float)sH / (float)N;
+                t[c].x = (float)(k0 * (double)qI * (double)qI);
+                t[c].y = (float)(k0 * (double)qH * (double)qH);
+                t[c].z = std::max(alpha_max * (1.0f - qI), 0.0f);
+                t[c].w = std::max(alpha_max * (1.0f - qH), 0.0f);
+            }
+            JV_TRY(alloc(&p, n * sizeof(float4)));
+            axis_d_[a] = (float4 *)p;
+            JV_CU(cudaMemcpy(axis_d_[a], t.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+        }
+        JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
+        cpF_ = make_cpml((float *)p);
+    }
 
     // wavelet and step state
     std::vector<float> w(nt_);
@@ -368,10 +425,21 @@ Status Engine::zero_wave(const WaveDev &w, int nfld) {
     return Status{};
 }
 
+CpmlDev Engine::make_cpml(float *psi) const {
+    CpmlDev c{};
+    c.rows = rows_d_;
+    c.nrows = nrows_;
+    c.nlong = nlong_;
+    c.cpl = cpl_;
+    c.cps = cps_;
+    c.dt = dt_;
+    for (int a = 0; a < 3; a++) c.ax[a] = axis_d_[a];
+    c.psi = psi;
+    return c;
+}
+
 Status Engine::zero_psi(const CpmlDev &c) {
-    long long n = 0;
-    for (int s = 0; s < 6; s++) n += 6LL * c.s[s].naxes * c.s[s].ncell;
-    if (n > 0) JV_CU(cudaMemsetAsync(c.s[0].psi, 0, (size_t)n * sizeof(float), stream_));
+    if (psi_total_ > 0) JV_CU(cudaMemsetAsync(c.psi, 0, (size_t)psi_total_ * sizeof(float), stream_));
     return Status{};
 }
 
@@ -601,20 +669,8 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         void *p;
         JV_TRY(alloc(&p, kNumFld * field_elems_ * sizeof(float)));
         for (int f = 0; f < kNumFld; f++) R_.f[f] = (float *)p + f * field_elems_;
-        JV_TRY([&]() -> Status {
-            CpmlDev c = cpF_;
-            long long n = 0;
-            for (int s = 0; s < 6; s++) n += 6LL * c.s[s].naxes * c.s[s].ncell;
-            void *q;
-            JV_TRY(alloc(&q, (size_t)n * sizeof(float)));
-            long long off = 0;
-            for (int s = 0; s < 6; s++) {
-                c.s[s].psi = (float *)q + off;
-                off += 6LL * c.s[s].naxes * c.s[s].ncell;
-            }
-            cpR_ = c;
-            return Status{};
-        }());
+        JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
+        cpR_ = make_cpml((float *)p);
     }
     if (!store_ && per_step_ > 0 && nslot_ > 0) {
         size_t bytes = (size_t)per_step_ * nslot_ * sizeof(float);

@@ -37,25 +37,34 @@ struct WaveDev {
     float *f[kNumFld];
 };
 
-// One CPML slab: cells [x0,x1) x [y0,y1) x [z0,z1) of gridext, memory
-// variables at psi + q * ncell + local index (q = 3*axis + t for the
-// velocity update, 3*naxes + 3*axis + t for the stress update).
+// One CPML slab: cells [x0,x1) x [y0,y1) x [z0,z1) of gridext.  Its
+// memory variables are 6*naxes arrays of ncell floats in slab-local
+// x-fastest order, starting at psi_off in the wavefield's CPML arena:
+// q = 3*axis + t for the velocity update, 3*naxes + 3*axis + t for the
+// stress update (axis 0 = x, 1 = y, 2 = z).
 struct SlabDev {
     int x0, x1, y0, y1, z0, z1;
     int naxes;          // 3 (top/bottom), 2 (front/back), 1 (right/left)
     long long ncell;
-    long long first;    // first global cell id of this slab
-    float *psi;
+    long long psi_off;
+};
+
+// One contiguous x segment of one slab: the unit of work of one warp.
+struct PmlRow {
+    int x0, len, y, z;
+    int naxes, pad;
+    long long ncell;    // cells of the slab (stride between memory arrays)
+    long long psi_off;  // offset of the segment's first cell in the arena
 };
 
 struct CpmlDev {
-    SlabDev s[6];
-    long long total;    // cells over all slabs
-    float fm, dt;       // dominant frequency, |time step|
-    float l10x7;        // log10(1/R) * DAMP_COEF, R = 0.001, DAMP_COEF = 7
-    float twoNdx, twoNdy, twoNdz;  // 2 N delta per axis, N = pml - 2
-    float N;            // pml - 2
-    float alpha_max;    // pi * fm
+    const PmlRow *rows;   // long rows (the z- and y-slabs) first, then the x-slab rows
+    int nrows;
+    int nlong;            // rows [0, nlong) have cpl 32-cell chunks, the rest cps
+    int cpl, cps;
+    float dt;                 // |time step|
+    const float4 *ax[3];      // per axis, per extended index: {K, K_half, alpha, alpha_half}, K = 0 outside
+    float *psi;               // this wavefield's memory-variable arena
 };
 
 struct ImageDev {
@@ -82,7 +91,7 @@ struct StepState {
 // interior-kernel choice: variant 0 = one z plane per block, 1 = z-marching
 // over chunks of zchunk planes (0: the whole column)
 struct KCfg {
-    int variant = 1;
+    int variant = 2;
     int zchunk = 0;
 };
 

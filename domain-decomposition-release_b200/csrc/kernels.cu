@@ -414,42 +414,338 @@ __global__ void __launch_bounds__(kTX *kTY) stress_phy_zm(GridDev g, WaveDev w, 
     }
 }
 
-// ---------------------------------------------------------------- CPML
+// --------------------------------------------- x-vectorised variants
+//
+// Each thread updates four consecutive x cells (one 16-byte group; the
+// first gridphy column is 128-byte aligned, so groups and their +-4 halo
+// groups are float4-aligned).  x-derivatives come from a 12-value window
+// (three float4 loads), y/z-derivatives from float4 loads of the stencil
+// rows/planes, with 32-bit element offsets.  Partial groups at the +x end of
+// gridphy compute all four lanes but store only the cells inside gridphy.
 
-// Damping coefficients of one axis at extended index c
-// (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620):
-// low side s = m - c (integer nodes) / m - c - 0.5 (half nodes); high side
-// s = c-(n-m-1) - 0.5 / c-(n-m-1); d = temp (s/N)^2, alpha = pi fm (1 - s/N),
-// b = exp(-(d+alpha) dt), a = d (b-1) / (d+alpha).
-__device__ __forceinline__ bool cpml_ab(int c, int n, int m, float vp, const CpmlDev &P, float twoNd, float &A,
-                                        float &B, float &Ah, float &Bh) {
-    float s, sh;
-    if (c >= kPmlHalf && c < m) {
-        s = (float)(m - c);
-        sh = s - 0.5f;
-    } else if (c >= n - m && c < n - kPmlHalf) {
-        sh = (float)(c - (n - m - 1));
-        s = sh - 0.5f;
-    } else {
-        return false;
+constexpr int kGX = 32, kGY = 8;
+
+__device__ __forceinline__ float4 ld4(const float *__restrict__ f, int i) {
+    return __ldg(reinterpret_cast<const float4 *>(f + i));
+}
+__device__ __forceinline__ float4 ldw4(const float *f, int i) { return *reinterpret_cast<const float4 *>(f + i); }
+__device__ __forceinline__ void f4a(float *a, float4 v) { a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w; }
+
+// window w[0..11] = f[i0-4 .. i0+7]
+__device__ __forceinline__ void xwin(const float *__restrict__ f, int i0, float *w) {
+    f4a(w, ld4(f, i0 - 4));
+    f4a(w + 4, ld4(f, i0));
+    f4a(w + 8, ld4(f, i0 + 4));
+}
+// x-derivatives of the 4 cells from the window, coefficient rows cc[c]
+__device__ __forceinline__ void xdp(const float *w, const float *const *cc, float *out) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float t = 0.f;
+#pragma unroll
+        for (int r = 0; r < 4; r++) t += cc[c][r] * (w[4 + c + r + 1] - w[4 + c - r]);
+        out[c] = t;
     }
-    const float temp = P.l10x7 * vp / twoNd;
-    const float q = s / P.N, qh = sh / P.N;
-    const float d = temp * (q * q), dh = temp * (qh * qh);
-    const float al = fmaxf(P.alpha_max * (1.0f - q), 0.f), alh = fmaxf(P.alpha_max * (1.0f - qh), 0.f);
-    B = expf(-(d + al) * P.dt);
-    Bh = expf(-(dh + alh) * P.dt);
-    A = d * (B - 1.0f) / (d + al);
-    Ah = dh * (Bh - 1.0f) / (dh + alh);
-    return true;
+}
+__device__ __forceinline__ void xdm(const float *w, const float *const *cc, float *out) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float t = 0.f;
+#pragma unroll
+        for (int r = 0; r < 4; r++) t += cc[c][r] * (w[4 + c + r] - w[4 + c - r - 1]);
+        out[c] = t;
+    }
+}
+// y or z derivatives of the 4 cells (stride s), one coefficient row
+__device__ __forceinline__ void sdp(const float *__restrict__ f, int i0, int s, const float *cf, float *out) {
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const float4 a = ld4(f, i0 + (r + 1) * s), b = ld4(f, i0 - r * s);
+        t[0] += cf[r] * (a.x - b.x);
+        t[1] += cf[r] * (a.y - b.y);
+        t[2] += cf[r] * (a.z - b.z);
+        t[3] += cf[r] * (a.w - b.w);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) out[c] = t[c];
+}
+__device__ __forceinline__ void sdm(const float *__restrict__ f, int i0, int s, const float *cf, float *out) {
+    float t[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const float4 a = ld4(f, i0 + r * s), b = ld4(f, i0 - (r + 1) * s);
+        t[0] += cf[r] * (a.x - b.x);
+        t[1] += cf[r] * (a.y - b.y);
+        t[2] += cf[r] * (a.z - b.z);
+        t[3] += cf[r] * (a.w - b.w);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) out[c] = t[c];
 }
 
-__device__ __forceinline__ SlabDev pick_slab(const CpmlDev &P, long long gid) {
-    SlabDev S = P.s[0];
+// coefficient rows: full 8th order, or the rtm_backward rim orders
+// (rows of c_list are zero past their order, so a 4-term sum is exact)
+// (outside the rtm_backward rim every row is the constant c_list[4], which
+// the compiler folds into constant-bank operands)
+template <int MODE>
+__device__ __forceinline__ void xcoefs(int pi0, int px, int rw, const float **cc) {
 #pragma unroll
-    for (int q = 1; q < 6; q++)
-        if (gid >= P.s[q].first) S = P.s[q];
-    return S;
+    for (int c = 0; c < 4; c++) cc[c] = c_list[(MODE == kBwd) ? rim_order(pi0 + c, px, rw) : kPhyHalf];
+}
+template <int MODE>
+__device__ __forceinline__ const float *scoef(int p, int np, int rw) {
+    return c_list[(MODE == kBwd) ? rim_order(p, np, rw) : kPhyHalf];
+}
+
+__device__ __forceinline__ void st4(float *f, int i0, const float *v, int nvalid) {
+    if (nvalid >= 4) {
+        *reinterpret_cast<float4 *>(f + i0) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (c < nvalid) f[i0 + c] = v[c];
+    }
+}
+
+template <int MODE, bool IMG>
+__global__ void __launch_bounds__(kGX *kGY, 3) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ rho,
+                                                         float dt, int rec_w, WaveDev rv, ImageDev img) {
+    const int pi0 = (blockIdx.x * kGX + threadIdx.x) * 4;
+    const int pj = blockIdx.y * kGY + threadIdx.y;
+    const int pk = blockIdx.z;
+    if (pi0 >= g.px || pj >= g.py) return;
+    constexpr bool kP = (MODE == kBwd || MODE == kRev);
+    const int nvalid = min(4, g.px - pi0);
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const int i0 = (int)g.xoff + (pi0 + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
+    const float *cx[4];
+    xcoefs<MODE>(pi0, g.px, rec_w, cx);
+    const float *cy = scoef<MODE>(pj, g.py, rec_w);
+    const float *cz = scoef<MODE>(pk, g.pz, rec_w);
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    float Dx[4], Dy[4], Dz[4], t[4], win[12];
+    // vx: Dp_x sxx + Dm_y sxy + Dm_z sxz
+    xwin(w.f[SXX], i0, win);
+    xdp(win, cx, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dx[c] = t[c] * rdx;
+    sdm(w.f[SXY], i0, sy, cy, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dx[c] += t[c] * rdy;
+    sdm(w.f[SXZ], i0, sz, cz, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dx[c] += t[c] * rdz;
+    // vy: Dm_x sxy + Dp_y syy + Dm_z syz
+    xwin(w.f[SXY], i0, win);
+    xdm(win, cx, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dy[c] = t[c] * rdx;
+    sdp(w.f[SYY], i0, sy, cy, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dy[c] += t[c] * rdy;
+    sdm(w.f[SYZ], i0, sz, cz, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dy[c] += t[c] * rdz;
+    // vz: Dm_x sxz + Dm_y syz + Dp_z szz
+    xwin(w.f[SXZ], i0, win);
+    xdm(win, cx, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dz[c] = t[c] * rdx;
+    sdm(w.f[SYZ], i0, sy, cy, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dz[c] += t[c] * rdy;
+    sdp(w.f[SZZ], i0, sz, cz, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Dz[c] += t[c] * rdz;
+
+    float dtr[4];
+    {
+        const float4 r4 = ld4(rho, i0);
+        dtr[0] = dt / r4.x; dtr[1] = dt / r4.y; dtr[2] = dt / r4.z; dtr[3] = dt / r4.w;
+    }
+    float vx[4], vy[4], vz[4];
+    f4a(vx, ldw4(w.f[VX], i0));
+    f4a(vy, ldw4(w.f[VY], i0));
+    f4a(vz, ldw4(w.f[VZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        vx[c] += dtr[c] * Dx[c];
+        vy[c] += dtr[c] * Dy[c];
+        vz[c] += dtr[c] * Dz[c];
+    }
+    st4(w.f[VX], i0, vx, nvalid);
+    st4(w.f[VY], i0, vy, nvalid);
+    st4(w.f[VZ], i0, vz, nvalid);
+    if (kP) {
+        // P-wave velocity from the pressure-like field sau (Dp on every axis)
+        float px[4], py[4], pz[4];
+        xwin(w.f[SAU], i0, win);
+        xdp(win, cx, t);
+        f4a(px, ldw4(w.f[VXP], i0));
+#pragma unroll
+        for (int c = 0; c < 4; c++) px[c] += dtr[c] * (t[c] * rdx);
+        sdp(w.f[SAU], i0, sy, cy, t);
+        f4a(py, ldw4(w.f[VYP], i0));
+#pragma unroll
+        for (int c = 0; c < 4; c++) py[c] += dtr[c] * (t[c] * rdy);
+        sdp(w.f[SAU], i0, sz, cz, t);
+        f4a(pz, ldw4(w.f[VZP], i0));
+#pragma unroll
+        for (int c = 0; c < 4; c++) pz[c] += dtr[c] * (t[c] * rdz);
+        st4(w.f[VXP], i0, px, nvalid);
+        st4(w.f[VYP], i0, py, nvalid);
+        st4(w.f[VZP], i0, pz, nvalid);
+        if (IMG) {
+            float rvx[4], rvy[4], rvz[4], rpx[4], rpy[4], rpz[4];
+            f4a(rvx, ld4(rv.f[VX], i0));
+            f4a(rvy, ld4(rv.f[VY], i0));
+            f4a(rvz, ld4(rv.f[VZ], i0));
+            f4a(rpx, ld4(rv.f[VXP], i0));
+            f4a(rpy, ld4(rv.f[VYP], i0));
+            f4a(rpz, ld4(rv.f[VZP], i0));
+            const long long o0 = pi0 + (long long)g.px * (pj + (long long)g.py * pk);
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (c >= nvalid) break;
+                const float rsx = rvx[c] - rpx[c], rsy = rvy[c] - rpy[c], rsz = rvz[c] - rpz[c];
+                const float ssx = vx[c] - px[c], ssy = vy[c] - py[c], ssz = vz[c] - pz[c];
+                const long long o = o0 + c;
+                img.ip[o] += (double)(px[c] * px[c] + py[c] * py[c] + pz[c] * pz[c]);
+                img.pp[o] += (double)(px[c] * rpx[c] + py[c] * rpy[c] + pz[c] * rpz[c]);
+                img.ps[o] += (double)(px[c] * rsx + py[c] * rsy + pz[c] * rsz);
+                img.sp[o] += (double)(ssx * rpx[c] + ssy * rpy[c] + ssz * rpz[c]);
+                img.ss[o] += (double)(ssx * rsx + ssy * rsy + ssz * rsz);
+            }
+        }
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kGX *kGY, 3) stress_phy_v4(GridDev g, WaveDev w, const float *__restrict__ lam,
+                                                            const float *__restrict__ mu, float dt, int rec_w,
+                                                            const float *__restrict__ wavelet,
+                                                            const StepState *__restrict__ st) {
+    const int pi0 = (blockIdx.x * kGX + threadIdx.x) * 4;
+    const int pj = blockIdx.y * kGY + threadIdx.y;
+    const int pk = blockIdx.z;
+    if (pi0 >= g.px || pj >= g.py) return;
+    const int nvalid = min(4, g.px - pi0);
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const int i0 = (int)g.xoff + (pi0 + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
+    const float *cx[4];
+    xcoefs<MODE>(pi0, g.px, rec_w, cx);
+    const float *cy = scoef<MODE>(pj, g.py, rec_w);
+    const float *cz = scoef<MODE>(pk, g.pz, rec_w);
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    // normal derivatives Nx = d vx/dx, ...; shear sums Sxy = d vy/dx + d vx/dy, ...
+    float Nx[4], Ny[4], Nz[4], Sxy[4], Sxz[4], Syz[4], t[4], win[12];
+    xwin(w.f[VX], i0, win);
+    xdm(win, cx, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Nx[c] = t[c] * rdx;
+    sdp(w.f[VX], i0, sy, cy, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Sxy[c] = t[c] * rdy;
+    sdp(w.f[VX], i0, sz, cz, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Sxz[c] = t[c] * rdz;
+    xwin(w.f[VY], i0, win);
+    xdp(win, cx, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Sxy[c] += t[c] * rdx;
+    sdm(w.f[VY], i0, sy, cy, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Ny[c] = t[c] * rdy;
+    sdp(w.f[VY], i0, sz, cz, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Syz[c] = t[c] * rdz;
+    xwin(w.f[VZ], i0, win);
+    xdp(win, cx, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Sxz[c] += t[c] * rdx;
+    sdp(w.f[VZ], i0, sy, cy, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Syz[c] += t[c] * rdy;
+    sdm(w.f[VZ], i0, sz, cz, t);
+#pragma unroll
+    for (int c = 0; c < 4; c++) Nz[c] = t[c] * rdz;
+
+    float l[4], m[4], sxx[4], syy[4], szz[4];
+    f4a(l, ld4(lam, i0));
+    f4a(m, ld4(mu, i0));
+    f4a(sxx, ldw4(w.f[SXX], i0));
+    f4a(syy, ldw4(w.f[SYY], i0));
+    f4a(szz, ldw4(w.f[SZZ], i0));
+    if (MODE != kRev) {
+        // explosive source, applied before the stress update of step it
+        // (FD/fdtd3d_2_phy_mpi_module/fdtd3d_phy_mpi_3_stress_kernel.hpp:1308-1364)
+        const long long src = st->src;
+        const long long d = src - (long long)i0;
+        if (d >= 0 && d < nvalid) {
+            const float sv = (MODE == kBwd) ? -wavelet[st->it] : wavelet[st->it];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c == (int)d) {
+                    sxx[c] += sv;
+                    syy[c] += sv;
+                    szz[c] += sv;
+                }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const float l2m = l[c] + 2.0f * m[c];
+        sxx[c] += dt * (l2m * Nx[c] + l[c] * Ny[c] + l[c] * Nz[c]);
+        syy[c] += dt * (l[c] * Nx[c] + l2m * Ny[c] + l[c] * Nz[c]);
+        szz[c] += dt * (l[c] * Nx[c] + l[c] * Ny[c] + l2m * Nz[c]);
+    }
+    st4(w.f[SXX], i0, sxx, nvalid);
+    st4(w.f[SYY], i0, syy, nvalid);
+    st4(w.f[SZZ], i0, szz, nvalid);
+    float a[4];
+    f4a(a, ldw4(w.f[SXY], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * m[c] * Sxy[c];
+    st4(w.f[SXY], i0, a, nvalid);
+    f4a(a, ldw4(w.f[SXZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * m[c] * Sxz[c];
+    st4(w.f[SXZ], i0, a, nvalid);
+    f4a(a, ldw4(w.f[SYZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * m[c] * Syz[c];
+    st4(w.f[SYZ], i0, a, nvalid);
+    if (MODE != kFwd) {
+        f4a(a, ldw4(w.f[SAU], i0));
+#pragma unroll
+        for (int c = 0; c < 4; c++) a[c] += dt * (l[c] + 2.0f * m[c]) * (Nx[c] + Ny[c] + Nz[c]);
+        st4(w.f[SAU], i0, a, nvalid);
+    }
+}
+
+// ---------------------------------------------------------------- CPML
+
+// Damping coefficients of one absorbing axis at one cell
+// (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620):
+// d = temp (s/N)^2 with temp = log10(1/R) 7 vp / (2 N delta), alpha =
+// pi fm (1 - s/N), b = exp(-(d+alpha) dt), a = d (b-1) / (d+alpha).  The
+// axis table t holds the vp-independent factors of the integer and half
+// node, {K, K_half, alpha, alpha_half} with d = vp K.
+__device__ __forceinline__ void cpml_coef(float vp, float4 t, float dt, float &A, float &B, float &Ah, float &Bh) {
+    const float d = vp * t.x, dh = vp * t.y;
+    B = expf(-(d + t.z) * dt);
+    Bh = expf(-(dh + t.w) * dt);
+    A = d * (B - 1.0f) / (d + t.z);
+    Ah = dh * (Bh - 1.0f) / (dh + t.w);
+}
+
+// 4th-order staggered differences with 32-bit element offsets
+__device__ __forceinline__ float dp2(const float *__restrict__ f, int i, int s, float c0, float c1) {
+    return c0 * (__ldg(f + i + s) - __ldg(f + i)) + c1 * (__ldg(f + i + 2 * s) - __ldg(f + i - s));
+}
+__device__ __forceinline__ float dm2(const float *__restrict__ f, int i, int s, float c0, float c1) {
+    return c0 * (__ldg(f + i) - __ldg(f + i - s)) + c1 * (__ldg(f + i + s) - __ldg(f + i - 2 * s));
 }
 
 __device__ __forceinline__ float psi_step(float *p, float b, float a, float d) {
@@ -458,107 +754,141 @@ __device__ __forceinline__ float psi_step(float *p, float b, float a, float d) {
     return v;
 }
 
+// Warp -> (row, 32-cell chunk): rows [0, nlong) have cpl chunks each, the
+// remaining rows cps chunks each; one cell per thread.
+__device__ __forceinline__ bool pml_locate(const CpmlDev &P, int &row, int &dx) {
+    const int wid = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const int nl = P.nlong * P.cpl;
+    int chunk;
+    if (wid < nl) {
+        row = wid / P.cpl;
+        chunk = wid - row * P.cpl;
+    } else {
+        const int w2 = wid - nl;
+        const int r2 = w2 / P.cps;
+        row = P.nlong + r2;
+        chunk = w2 - r2 * P.cps;
+        if (row >= P.nrows) return false;
+    }
+    dx = chunk * 32 + lane;
+    return dx < P.rows[row].len;
+}
+
+// One cell per thread: a warp covers 32 cells of one row segment (PmlRow).  A memory
+// variable is read and written only on the axes on which the cell lies in
+// that axis' absorbing range (elsewhere a = 0, b = 1 keep it at zero).
 __global__ void __launch_bounds__(256) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
                                                const float *__restrict__ vpm) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= P.total) return;
-    const SlabDev S = pick_slab(P, gid);
-    const long long loc = gid - S.first;
-    const int wx = S.x1 - S.x0, wy = S.y1 - S.y0;
-    const int x = S.x0 + (int)(loc % wx);
-    const long long t = loc / wx;
-    const int y = S.y0 + (int)(t % wy);
-    const int z = S.z0 + (int)(t / wy);
-    const long long sy = g.sy, sz = g.sz;
-    const long long i = g.xoff + x + sy * y + sz * z;
-    const float *c = c_dc2;
-    float sxx_x = dp<2>(w.f[SXX], i, 1, c) / g.dx;
-    float syx_x = dm<2>(w.f[SXY], i, 1, c) / g.dx;
-    float szx_x = dm<2>(w.f[SXZ], i, 1, c) / g.dx;
-    float sxy_y = dm<2>(w.f[SXY], i, sy, c) / g.dy;
-    float syy_y = dp<2>(w.f[SYY], i, sy, c) / g.dy;
-    float szy_y = dm<2>(w.f[SYZ], i, sy, c) / g.dy;
-    float sxz_z = dm<2>(w.f[SXZ], i, sz, c) / g.dz;
-    float syz_z = dm<2>(w.f[SYZ], i, sz, c) / g.dz;
-    float szz_z = dp<2>(w.f[SZZ], i, sz, c) / g.dz;
-    const float vp = ld(vpm, i);
-    float *psi = S.psi + loc;
-    const long long n = S.ncell;
-    float A, B, Ah, Bh;
-    if (cpml_ab(x, g.nx, g.m, vp, P, P.twoNdx, A, B, Ah, Bh)) {
-        sxx_x += psi_step(psi + 0 * n, Bh, Ah, sxx_x);
-        syx_x += psi_step(psi + 1 * n, B, A, syx_x);
-        szx_x += psi_step(psi + 2 * n, B, A, szx_x);
+    int row, dx;
+    if (!pml_locate(P, row, dx)) return;
+    const PmlRow R = P.rows[row];
+    const float4 ty = P.ax[1][R.y], tz = P.ax[2][R.z];
+    const bool ya = ty.x > 0.f, za = tz.x > 0.f;
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const int base = (int)g.xoff + sy * R.y + sz * R.z;
+    const float c0 = c_dc2[0], c1 = c_dc2[1];
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    const int n = (int)R.ncell;
+    {
+        const int x = R.x0 + dx;
+        const int i = base + x;
+        float sxx_x = dp2(w.f[SXX], i, 1, c0, c1) * rdx;
+        float syx_x = dm2(w.f[SXY], i, 1, c0, c1) * rdx;
+        float szx_x = dm2(w.f[SXZ], i, 1, c0, c1) * rdx;
+        float sxy_y = dm2(w.f[SXY], i, sy, c0, c1) * rdy;
+        float syy_y = dp2(w.f[SYY], i, sy, c0, c1) * rdy;
+        float szy_y = dm2(w.f[SYZ], i, sy, c0, c1) * rdy;
+        float sxz_z = dm2(w.f[SXZ], i, sz, c0, c1) * rdz;
+        float syz_z = dm2(w.f[SYZ], i, sz, c0, c1) * rdz;
+        float szz_z = dp2(w.f[SZZ], i, sz, c0, c1) * rdz;
+        const float vp = __ldg(vpm + i);
+        const float4 tx = P.ax[0][x];
+        float *psi = P.psi + R.psi_off + dx;
+        float A, B, Ah, Bh;
+        if (tx.x > 0.f) {
+            cpml_coef(vp, tx, P.dt, A, B, Ah, Bh);
+            sxx_x += psi_step(psi + 0 * n, Bh, Ah, sxx_x);
+            syx_x += psi_step(psi + 1 * n, B, A, syx_x);
+            szx_x += psi_step(psi + 2 * n, B, A, szx_x);
+        }
+        if (ya) {
+            cpml_coef(vp, ty, P.dt, A, B, Ah, Bh);
+            sxy_y += psi_step(psi + 3 * n, B, A, sxy_y);
+            syy_y += psi_step(psi + 4 * n, Bh, Ah, syy_y);
+            szy_y += psi_step(psi + 5 * n, B, A, szy_y);
+        }
+        if (za) {
+            cpml_coef(vp, tz, P.dt, A, B, Ah, Bh);
+            sxz_z += psi_step(psi + 6 * n, B, A, sxz_z);
+            syz_z += psi_step(psi + 7 * n, B, A, syz_z);
+            szz_z += psi_step(psi + 8 * n, Bh, Ah, szz_z);
+        }
+        const float dtr = P.dt / __ldg(rho + i);
+        w.f[VX][i] += dtr * (sxx_x + sxy_y + sxz_z);
+        w.f[VY][i] += dtr * (syx_x + syy_y + syz_z);
+        w.f[VZ][i] += dtr * (szx_x + szy_y + szz_z);
     }
-    if (cpml_ab(y, g.ny, g.m, vp, P, P.twoNdy, A, B, Ah, Bh)) {
-        sxy_y += psi_step(psi + 3 * n, B, A, sxy_y);
-        syy_y += psi_step(psi + 4 * n, Bh, Ah, syy_y);
-        szy_y += psi_step(psi + 5 * n, B, A, szy_y);
-    }
-    if (cpml_ab(z, g.nz, g.m, vp, P, P.twoNdz, A, B, Ah, Bh)) {
-        sxz_z += psi_step(psi + 6 * n, B, A, sxz_z);
-        syz_z += psi_step(psi + 7 * n, B, A, syz_z);
-        szz_z += psi_step(psi + 8 * n, Bh, Ah, szz_z);
-    }
-    const float dtr = P.dt / ld(rho, i);
-    w.f[VX][i] += dtr * (sxx_x + sxy_y + sxz_z);
-    w.f[VY][i] += dtr * (syx_x + syy_y + syz_z);
-    w.f[VZ][i] += dtr * (szx_x + szy_y + szz_z);
 }
 
 template <bool WITH_SAU>
 __global__ void __launch_bounds__(256) stress_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ lam,
                                                   const float *__restrict__ mu, const float *__restrict__ vpm) {
-    const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (gid >= P.total) return;
-    const SlabDev S = pick_slab(P, gid);
-    const long long loc = gid - S.first;
-    const int wx = S.x1 - S.x0, wy = S.y1 - S.y0;
-    const int x = S.x0 + (int)(loc % wx);
-    const long long t = loc / wx;
-    const int y = S.y0 + (int)(t % wy);
-    const int z = S.z0 + (int)(t / wy);
-    const long long sy = g.sy, sz = g.sz;
-    const long long i = g.xoff + x + sy * y + sz * z;
-    const float *c = c_dc2;
-    float vx_x = dm<2>(w.f[VX], i, 1, c) / g.dx;
-    float vy_x = dp<2>(w.f[VY], i, 1, c) / g.dx;
-    float vz_x = dp<2>(w.f[VZ], i, 1, c) / g.dx;
-    float vx_y = dp<2>(w.f[VX], i, sy, c) / g.dy;
-    float vy_y = dm<2>(w.f[VY], i, sy, c) / g.dy;
-    float vz_y = dp<2>(w.f[VZ], i, sy, c) / g.dy;
-    float vx_z = dp<2>(w.f[VX], i, sz, c) / g.dz;
-    float vy_z = dp<2>(w.f[VY], i, sz, c) / g.dz;
-    float vz_z = dm<2>(w.f[VZ], i, sz, c) / g.dz;
-    const float vp = ld(vpm, i);
-    float *psi = S.psi + loc + 3 * S.naxes * S.ncell;
-    const long long n = S.ncell;
-    float A, B, Ah, Bh;
-    if (cpml_ab(x, g.nx, g.m, vp, P, P.twoNdx, A, B, Ah, Bh)) {
-        vx_x += psi_step(psi + 0 * n, B, A, vx_x);
-        vy_x += psi_step(psi + 1 * n, Bh, Ah, vy_x);
-        vz_x += psi_step(psi + 2 * n, Bh, Ah, vz_x);
+    int row, dx;
+    if (!pml_locate(P, row, dx)) return;
+    const PmlRow R = P.rows[row];
+    const float4 ty = P.ax[1][R.y], tz = P.ax[2][R.z];
+    const bool ya = ty.x > 0.f, za = tz.x > 0.f;
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const int base = (int)g.xoff + sy * R.y + sz * R.z;
+    const float c0 = c_dc2[0], c1 = c_dc2[1];
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    const int n = (int)R.ncell;
+    {
+        const int x = R.x0 + dx;
+        const int i = base + x;
+        float vx_x = dm2(w.f[VX], i, 1, c0, c1) * rdx;
+        float vy_x = dp2(w.f[VY], i, 1, c0, c1) * rdx;
+        float vz_x = dp2(w.f[VZ], i, 1, c0, c1) * rdx;
+        float vx_y = dp2(w.f[VX], i, sy, c0, c1) * rdy;
+        float vy_y = dm2(w.f[VY], i, sy, c0, c1) * rdy;
+        float vz_y = dp2(w.f[VZ], i, sy, c0, c1) * rdy;
+        float vx_z = dp2(w.f[VX], i, sz, c0, c1) * rdz;
+        float vy_z = dp2(w.f[VY], i, sz, c0, c1) * rdz;
+        float vz_z = dm2(w.f[VZ], i, sz, c0, c1) * rdz;
+        const float vp = __ldg(vpm + i);
+        const float4 tx = P.ax[0][x];
+        float *psi = P.psi + R.psi_off + 3LL * R.naxes * n + dx;
+        float A, B, Ah, Bh;
+        if (tx.x > 0.f) {
+            cpml_coef(vp, tx, P.dt, A, B, Ah, Bh);
+            vx_x += psi_step(psi + 0 * n, B, A, vx_x);
+            vy_x += psi_step(psi + 1 * n, Bh, Ah, vy_x);
+            vz_x += psi_step(psi + 2 * n, Bh, Ah, vz_x);
+        }
+        if (ya) {
+            cpml_coef(vp, ty, P.dt, A, B, Ah, Bh);
+            vy_y += psi_step(psi + 3 * n, B, A, vy_y);
+            vx_y += psi_step(psi + 4 * n, Bh, Ah, vx_y);
+            vz_y += psi_step(psi + 5 * n, Bh, Ah, vz_y);
+        }
+        if (za) {
+            cpml_coef(vp, tz, P.dt, A, B, Ah, Bh);
+            vz_z += psi_step(psi + 6 * n, B, A, vz_z);
+            vx_z += psi_step(psi + 7 * n, Bh, Ah, vx_z);
+            vy_z += psi_step(psi + 8 * n, Bh, Ah, vy_z);
+        }
+        const float l = __ldg(lam + i), m = __ldg(mu + i);
+        const float l2m = l + 2.0f * m;
+        const float dt = P.dt;
+        w.f[SXX][i] += dt * (l2m * vx_x + l * vy_y + l * vz_z);
+        w.f[SYY][i] += dt * (l * vx_x + l2m * vy_y + l * vz_z);
+        w.f[SZZ][i] += dt * (l * vx_x + l * vy_y + l2m * vz_z);
+        if (WITH_SAU) w.f[SAU][i] += dt * (l2m * vx_x + l2m * vy_y + l2m * vz_z);
+        w.f[SXY][i] += dt * m * (vy_x + vx_y);
+        w.f[SXZ][i] += dt * m * (vz_x + vx_z);
+        w.f[SYZ][i] += dt * m * (vz_y + vy_z);
     }
-    if (cpml_ab(y, g.ny, g.m, vp, P, P.twoNdy, A, B, Ah, Bh)) {
-        vy_y += psi_step(psi + 3 * n, B, A, vy_y);
-        vx_y += psi_step(psi + 4 * n, Bh, Ah, vx_y);
-        vz_y += psi_step(psi + 5 * n, Bh, Ah, vz_y);
-    }
-    if (cpml_ab(z, g.nz, g.m, vp, P, P.twoNdz, A, B, Ah, Bh)) {
-        vz_z += psi_step(psi + 6 * n, B, A, vz_z);
-        vx_z += psi_step(psi + 7 * n, Bh, Ah, vx_z);
-        vy_z += psi_step(psi + 8 * n, Bh, Ah, vy_z);
-    }
-    const float l = ld(lam, i), m = ld(mu, i);
-    const float l2m = l + 2.0f * m;
-    const float dt = P.dt;
-    w.f[SXX][i] += dt * (l2m * vx_x + l * vy_y + l * vz_z);
-    w.f[SYY][i] += dt * (l * vx_x + l2m * vy_y + l * vz_z);
-    w.f[SZZ][i] += dt * (l * vx_x + l * vy_y + l2m * vz_z);
-    if (WITH_SAU) w.f[SAU][i] += dt * (l2m * vx_x + l2m * vy_y + l2m * vz_z);
-    w.f[SXY][i] += dt * m * (vy_x + vx_y);
-    w.f[SXZ][i] += dt * m * (vz_x + vx_z);
-    w.f[SYZ][i] += dt * m * (vz_y + vy_z);
 }
 
 // ------------------------------------------------------------ receivers
@@ -719,6 +1049,20 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
     cudaStream_t s = (cudaStream_t)stream;
     WaveDev rv = rev ? *rev : WaveDev{};
     ImageDev im = img ? *img : ImageDev{};
+    if (kc.variant == 2) {
+        dim3 b(kGX, kGY), gr((g.px + 4 * kGX - 1) / (4 * kGX), (g.py + kGY - 1) / kGY, g.pz);
+        switch (mode) {
+        case kFwd: vel_phy_v4<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+        case kRtmFwd: vel_phy_v4<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+        case kRev: vel_phy_v4<kRev, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+        case kBwd:
+            if (img && rev) vel_phy_v4<kBwd, true><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+            else vel_phy_v4<kBwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+            break;
+        default: return (int)cudaErrorInvalidValue;
+        }
+        return cerr();
+    }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
         dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, (g.pz + zc - 1) / zc);
@@ -751,6 +1095,17 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt, int rec_w,
                  const float *wavelet, const StepState *st, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
+    if (kc.variant == 2) {
+        dim3 b(kGX, kGY), gr((g.px + 4 * kGX - 1) / (4 * kGX), (g.py + kGY - 1) / kGY, g.pz);
+        switch (mode) {
+        case kFwd: stress_phy_v4<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+        case kRtmFwd: stress_phy_v4<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+        case kBwd: stress_phy_v4<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+        case kRev: stress_phy_v4<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+        default: return (int)cudaErrorInvalidValue;
+        }
+        return cerr();
+    }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
         dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, (g.pz + zc - 1) / zc);
@@ -775,18 +1130,19 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
 }
 
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp, void *stream) {
-    if (c.total <= 0) return 0;
-    const long long blocks = (c.total + 255) / 256;
-    vel_pml<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, rho, vp);
+    if (c.nrows <= 0) return 0;
+    const long long warps = (long long)c.nlong * c.cpl + (long long)(c.nrows - c.nlong) * c.cps;
+    vel_pml<<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(g, c, w, rho, vp);
     return cerr();
 }
 
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
                  const float *vp, int with_sau, void *stream) {
-    if (c.total <= 0) return 0;
-    const long long blocks = (c.total + 255) / 256;
-    if (with_sau) stress_pml<true><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
-    else stress_pml<false><<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
+    if (c.nrows <= 0) return 0;
+    const long long warps = (long long)c.nlong * c.cpl + (long long)(c.nrows - c.nlong) * c.cps;
+    const unsigned blocks = (unsigned)((warps + 7) / 8);
+    if (with_sau) stress_pml<true><<<blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
+    else stress_pml<false><<<blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
     return cerr();
 }
 

@@ -75,7 +75,7 @@ typedef struct jv_options {
     int use_graphs;     /* capture the time loop in CUDA graphs (default on)     */
     int graph_steps;    /* time steps per captured graph (0 -> library default)  */
     size_t store_budget;/* max bytes of HBM for the boundary store (0 -> auto)   */
-    int kernel_variant; /* interior kernels: 0 one plane per block, 1 z-marching */
+    int kernel_variant; /* interior kernels: 0 one plane per block, 1 z-marching, 2 x-vectorised (default) */
     int zchunk;         /* z planes per block for variant 1 (0 -> auto)          */
 } jv_options;
 

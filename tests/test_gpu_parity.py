@@ -33,12 +33,16 @@ SMALL = [
 ]
 
 
+VARIANTS = [0, 1, 2]  # interior kernels: one plane per block, z-marching, x-vectorised
+
+
 @pytest.mark.parametrize("kw", SMALL)
 @pytest.mark.parametrize("graphs", [1, 0])
-def test_forward_vs_oracle(oracle, synth, kw, graphs):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_forward_vs_oracle(oracle, synth, kw, graphs, variant):
     s = synth.small_case(**kw)
     ref = oracle.forward(_problem(oracle, s))
-    with jv.Context.from_survey(s, use_graphs=graphs, graph_steps=7) as ctx:
+    with jv.Context.from_survey(s, use_graphs=graphs, graph_steps=7, kernel_variant=variant, zchunk=5) as ctx:
         tr = ctx.forward(0)
     assert tr[0].shape == ref[0].shape
     for a, b in zip(tr, ref):
@@ -71,14 +75,15 @@ def test_pins_vs_reference(synth, name):
 
 
 @pytest.mark.parametrize("w", [1, 2, 3, 4])
-def test_rtm_vs_oracle(oracle, synth, w):
-    s = synth.small_case(n=(22, 18, 20), pml=6, nt=140, seed=21, rec_width=w, anomaly=(0.1, 3.0),
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_rtm_vs_oracle(oracle, synth, w, variant):
+    s = synth.small_case(n=(22, 18, 21), pml=6, nt=140, seed=21, rec_width=w, anomaly=(0.1, 3.0),
                          shot_idx=[(11, 9, 3)])
     p = _problem(oracle, s, w)
     obs = oracle.forward(p)
     ref = oracle.rtm_shot(p, obs)
     obs32 = [o.astype(np.float32) for o in obs]
-    with jv.Context.from_survey(s) as ctx:
+    with jv.Context.from_survey(s, kernel_variant=variant, zchunk=6) as ctx:
         ctx.rtm_shot(0, obs32)
         raw = ctx.images()
         comp, lap = ctx.finalize()
