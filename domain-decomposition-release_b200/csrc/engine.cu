@@ -61,6 +61,12 @@ void ricker(int nt, float fm, float dt, float *w) {
 
 static long long round_up(long long v, long long a) { return (v + a - 1) / a * a; }
 
+// Every pitched field arena starts with kGuard zero floats, so the 16-byte
+// x groups of the CPML slabs may read a few cells before gridext (x >= -5)
+// without leaving the allocation; each field also ends with >= 128 floats
+// of slack for reads past the last row.
+constexpr size_t kGuard = 32;
+
 Status Engine::cu(cudaError_t e, const char *what) const {
     Status s;
     if (e != cudaSuccess) {
@@ -178,15 +184,15 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     g_.sy = round_up(g_.xoff + g_.nx, 32);
     g_.sz = g_.sy * g_.ny;
     g_.dx = grid_.dx; g_.dy = grid_.dy; g_.dz = grid_.dz;
-    field_elems_ = (size_t)round_up(g_.sz * g_.nz + 64, 64);
+    field_elems_ = (size_t)round_up(g_.sz * g_.nz + 128, 64);
     if (field_elems_ >= (size_t)1 << 31) return bad(JV_EINVAL, "gridext too large for 32-bit element offsets");
 
     // model
     void *p;
-    JV_TRY(alloc(&p, 4 * field_elems_ * sizeof(float)));
-    float *mb = (float *)p;
+    JV_TRY(alloc(&p, (4 * field_elems_ + kGuard) * sizeof(float)));
+    JV_CU(cudaMemsetAsync(p, 0, (4 * field_elems_ + kGuard) * sizeof(float), stream_));
+    float *mb = (float *)p + kGuard;
     vp_ = mb; rho_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
-    JV_CU(cudaMemsetAsync(mb, 0, 4 * field_elems_ * sizeof(float), stream_));
     const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
     float *tmp = nullptr;
     JV_CU(cudaMalloc(&tmp, 3 * nphy * sizeof(float)));
@@ -199,13 +205,15 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_CU(e1); JV_CU(e2); JV_CU(e3); JV_K(ek); JV_CU(e4);
 
     // forward/backward wavefield (13 components, one arena)
-    JV_TRY(alloc(&p, kNumFld * field_elems_ * sizeof(float)));
-    for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + f * field_elems_;
+    JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
+    JV_CU(cudaMemsetAsync(p, 0, kGuard * sizeof(float), stream_));
+    for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + kGuard + f * field_elems_;
 
     // CPML geometry: six slabs covering gridext outside gridphy and outside
     // the 2-cell outer rim (FD/fdtd3d_0_base_module/fdtd3d_base_6_pml_meat.hpp:29-94),
-    // split into x segments (one warp each); rows and axis tables are shared
-    // by both wavefields, the memory-variable arenas are per wavefield
+    // processed in 16-byte aligned 4-cell x groups; the slab table and axis
+    // tables are shared by both wavefields, the memory-variable arenas are
+    // per wavefield
     {
         const int NX = g_.nx, NY = g_.ny, NZ = g_.nz;
         const int bx[6][6] = {
@@ -215,51 +223,34 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         };
         const int na[6] = {3, 3, 2, 2, 1, 1};
         long long off = 0;
-        std::vector<PmlRow> rows;
+        int blocks = 0;
+        cpml_proto_ = CpmlDev{};
         for (int q = 0; q < 6; q++) {
-            SlabDev S{};
+            PmlSlab S{};
             S.x0 = bx[q][0]; S.x1 = bx[q][1]; S.y0 = bx[q][2]; S.y1 = bx[q][3]; S.z0 = bx[q][4]; S.z1 = bx[q][5];
             S.naxes = na[q];
             if (S.x1 <= S.x0 || S.y1 <= S.y0 || S.z1 <= S.z0) continue;
-            S.ncell = (long long)(S.x1 - S.x0) * (S.y1 - S.y0) * (S.z1 - S.z0);
+            S.gstart = S.x0 - (int)((g_.xoff + S.x0) & 3);
+            S.ngroups = (S.x1 - S.gstart + 3) / 4;
+            S.pitch = 4 * S.ngroups;
+            S.gx = 1;
+            S.lgx = 0;
+            while (S.gx < S.ngroups && S.gx < 32) {
+                S.gx *= 2;
+                S.lgx++;
+            }
+            S.gy = 256 / S.gx;
+            S.bx = (S.ngroups + S.gx - 1) / S.gx;
+            S.by = (S.y1 - S.y0 + S.gy - 1) / S.gy;
+            S.first_block = blocks;
+            blocks += S.bx * S.by * (S.z1 - S.z0);
+            S.stride = (long long)S.pitch * (S.y1 - S.y0) * (S.z1 - S.z0);
             S.psi_off = off;
-            off += 6LL * S.naxes * S.ncell;
-            slabs_.push_back(S);
-            for (int z = S.z0; z < S.z1; z++)
-                for (int y = S.y0; y < S.y1; y++) {
-                    PmlRow r{};
-                    r.x0 = S.x0; r.len = S.x1 - S.x0; r.y = y; r.z = z;
-                    r.naxes = S.naxes;
-                    r.ncell = S.ncell;
-                    r.psi_off = S.psi_off + ((long long)(z - S.z0) * (S.y1 - S.y0) + (y - S.y0)) * (S.x1 - S.x0);
-                    rows.push_back(r);
-                }
+            off += 6LL * S.naxes * S.stride;
+            cpml_proto_.s[cpml_proto_.nslab++] = S;
         }
-        // long rows (z- and y-slabs, full x extent) first, then the x-slab
-        // rows; within each class neighbouring rows run together
-        const int longlen = NX - 4;
-        std::sort(rows.begin(), rows.end(), [longlen](const PmlRow &u, const PmlRow &v) {
-            const bool lu = u.len == longlen, lv = v.len == longlen;
-            if (lu != lv) return lu;
-            if (u.z != v.z) return u.z < v.z;
-            if (u.y != v.y) return u.y < v.y;
-            return u.x0 < v.x0;
-        });
-        nlong_ = 0;
-        int shortmax = 1;
-        for (const PmlRow &r : rows) {
-            if (r.len == longlen) nlong_++;
-            else shortmax = std::max(shortmax, r.len);
-        }
-        cpl_ = (longlen + 31) / 32;
-        cps_ = (shortmax + 31) / 32;
+        cpml_proto_.nblocks = blocks;
         psi_total_ = off;
-        nrows_ = (int)rows.size();
-        if (nrows_ > 0) {
-            JV_TRY(alloc(&p, rows.size() * sizeof(PmlRow)));
-            rows_d_ = (PmlRow *)p;
-            JV_CU(cudaMemcpy(rows_d_, rows.data(), rows.size() * sizeof(PmlRow), cudaMemcpyHostToDevice));
-        }
         // per-axis damping factors: d = vp * K, K = log10(1/R) 7 (s/N)^2 / (2 N delta)
         // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620)
         const double N = (double)(m - kPmlHalf);
@@ -309,7 +300,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_TRY(alloc(&p, 5 * nphy * sizeof(double)));
     double *ib = (double *)p;
     img_.ip = ib; img_.pp = ib + nphy; img_.ps = ib + 2 * nphy; img_.sp = ib + 3 * nphy; img_.ss = ib + 4 * nphy;
-    JV_CU(cudaMemset(ib, 0, 5 * nphy * sizeof(double)));
+    JV_CU(cudaMemsetAsync(ib, 0, 5 * nphy * sizeof(double), stream_));
 
     // VOWR face boxes (FD/fdtd3d_0_base_module/fdtd3d_base_5_wave_recon_meat.hpp:19-30;
     // face frames .jarvis_0_meta/.jarvis_3_operator/jarvis_1_mpicu_halo_store_operator_meat.hpp:129-134)
@@ -355,6 +346,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         }
         nslot_ = nt_ > 1 ? nt_ - 1 : 0;
     }
+    JV_CU(cudaStreamSynchronize(stream_));
     return Status{};
 }
 
@@ -426,12 +418,7 @@ Status Engine::zero_wave(const WaveDev &w, int nfld) {
 }
 
 CpmlDev Engine::make_cpml(float *psi) const {
-    CpmlDev c{};
-    c.rows = rows_d_;
-    c.nrows = nrows_;
-    c.nlong = nlong_;
-    c.cpl = cpl_;
-    c.cps = cps_;
+    CpmlDev c = cpml_proto_;
     c.dt = dt_;
     for (int a = 0; a < 3; a++) c.ax[a] = axis_d_[a];
     c.psi = psi;
@@ -667,8 +654,9 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
     // lazily allocate the receiver wavefield and the boundary store
     if (!R_.f[0]) {
         void *p;
-        JV_TRY(alloc(&p, kNumFld * field_elems_ * sizeof(float)));
-        for (int f = 0; f < kNumFld; f++) R_.f[f] = (float *)p + f * field_elems_;
+        JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
+        JV_CU(cudaMemsetAsync(p, 0, kGuard * sizeof(float), stream_));
+        for (int f = 0; f < kNumFld; f++) R_.f[f] = (float *)p + kGuard + f * field_elems_;
         JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
         cpR_ = make_cpml((float *)p);
     }

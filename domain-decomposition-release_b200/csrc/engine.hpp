@@ -91,10 +91,8 @@ class Engine {
     float *vp_ = nullptr, *rho_ = nullptr, *lam_ = nullptr, *mu_ = nullptr;
     WaveDev F_{}, R_{};
     CpmlDev cpF_{}, cpR_{};
-    std::vector<SlabDev> slabs_;
+    CpmlDev cpml_proto_{};     // slab table shared by both wavefields
     long long psi_total_ = 0;  // memory-variable floats per wavefield
-    PmlRow *rows_d_ = nullptr;
-    int nrows_ = 0, nlong_ = 0, cpl_ = 1, cps_ = 1;
     float4 *axis_d_[3] = {nullptr, nullptr, nullptr};
     CpmlDev make_cpml(float *psi) const;
     float *wavelet_ = nullptr;

@@ -37,31 +37,26 @@ struct WaveDev {
     float *f[kNumFld];
 };
 
-// One CPML slab: cells [x0,x1) x [y0,y1) x [z0,z1) of gridext.  Its
-// memory variables are 6*naxes arrays of ncell floats in slab-local
-// x-fastest order, starting at psi_off in the wavefield's CPML arena:
+// One CPML slab: cells [x0,x1) x [y0,y1) x [z0,z1) of gridext, processed
+// in 4-cell x groups starting at the 16-byte aligned cell gstart (cells of
+// a group outside [x0,x1) are masked).  Its memory variables are 6*naxes
+// arrays of `stride` floats: rows of `pitch` = 4*ngroups floats, group g
+// of row (y,z) at psi_off + ((z-z0)*(y1-y0) + (y-y0))*pitch + 4g; array
 // q = 3*axis + t for the velocity update, 3*naxes + 3*axis + t for the
-// stress update (axis 0 = x, 1 = y, 2 = z).
-struct SlabDev {
+// stress update (axis 0 = x, 1 = y, 2 = z).  Launch shape: blocks of
+// 256 threads = gx groups x gy rows (gx = 2^lgx), bx*by blocks per plane.
+struct PmlSlab {
     int x0, x1, y0, y1, z0, z1;
-    int naxes;          // 3 (top/bottom), 2 (front/back), 1 (right/left)
-    long long ncell;
-    long long psi_off;
-};
-
-// One contiguous x segment of one slab: the unit of work of one warp.
-struct PmlRow {
-    int x0, len, y, z;
-    int naxes, pad;
-    long long ncell;    // cells of the slab (stride between memory arrays)
-    long long psi_off;  // offset of the segment's first cell in the arena
+    int gstart, ngroups;
+    int gx, gy, lgx, bx, by;
+    int first_block;
+    int naxes, pitch;
+    long long psi_off, stride;
 };
 
 struct CpmlDev {
-    const PmlRow *rows;   // long rows (the z- and y-slabs) first, then the x-slab rows
-    int nrows;
-    int nlong;            // rows [0, nlong) have cpl 32-cell chunks, the rest cps
-    int cpl, cps;
+    PmlSlab s[6];
+    int nslab, nblocks;
     float dt;                 // |time step|
     const float4 *ax[3];      // per axis, per extended index: {K, K_half, alpha, alpha_half}, K = 0 outside
     float *psi;               // this wavefield's memory-variable arena

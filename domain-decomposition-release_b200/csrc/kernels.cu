@@ -730,165 +730,286 @@ __global__ void __launch_bounds__(kGX *kGY, 3) stress_phy_v4(GridDev g, WaveDev 
 // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620):
 // d = temp (s/N)^2 with temp = log10(1/R) 7 vp / (2 N delta), alpha =
 // pi fm (1 - s/N), b = exp(-(d+alpha) dt), a = d (b-1) / (d+alpha).  The
-// axis table t holds the vp-independent factors of the integer and half
-// node, {K, K_half, alpha, alpha_half} with d = vp K.
+// axis table entry t holds the vp-independent factors of the integer and
+// half node, {K, K_half, alpha, alpha_half} with d = vp K; K = 0 marks an
+// index outside that axis' absorbing range (a = 0, b = 1 there).
 __device__ __forceinline__ void cpml_coef(float vp, float4 t, float dt, float &A, float &B, float &Ah, float &Bh) {
-    const float d = vp * t.x, dh = vp * t.y;
-    B = expf(-(d + t.z) * dt);
-    Bh = expf(-(dh + t.w) * dt);
-    A = d * (B - 1.0f) / (d + t.z);
-    Ah = dh * (Bh - 1.0f) / (dh + t.w);
-}
-
-// 4th-order staggered differences with 32-bit element offsets
-__device__ __forceinline__ float dp2(const float *__restrict__ f, int i, int s, float c0, float c1) {
-    return c0 * (__ldg(f + i + s) - __ldg(f + i)) + c1 * (__ldg(f + i + 2 * s) - __ldg(f + i - s));
-}
-__device__ __forceinline__ float dm2(const float *__restrict__ f, int i, int s, float c0, float c1) {
-    return c0 * (__ldg(f + i) - __ldg(f + i - s)) + c1 * (__ldg(f + i + s) - __ldg(f + i - 2 * s));
-}
-
-__device__ __forceinline__ float psi_step(float *p, float b, float a, float d) {
-    const float v = b * *p + a * d;
-    *p = v;
-    return v;
-}
-
-// Warp -> (row, 32-cell chunk): rows [0, nlong) have cpl chunks each, the
-// remaining rows cps chunks each; one cell per thread.
-__device__ __forceinline__ bool pml_locate(const CpmlDev &P, int &row, int &dx) {
-    const int wid = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    const int nl = P.nlong * P.cpl;
-    int chunk;
-    if (wid < nl) {
-        row = wid / P.cpl;
-        chunk = wid - row * P.cpl;
+    if (t.x > 0.f) {
+        const float d = vp * t.x, dh = vp * t.y;
+        B = expf(-(d + t.z) * dt);
+        Bh = expf(-(dh + t.w) * dt);
+        A = d * (B - 1.0f) / (d + t.z);
+        Ah = dh * (Bh - 1.0f) / (dh + t.w);
     } else {
-        const int w2 = wid - nl;
-        const int r2 = w2 / P.cps;
-        row = P.nlong + r2;
-        chunk = w2 - r2 * P.cps;
-        if (row >= P.nrows) return false;
+        A = 0.f; B = 1.f; Ah = 0.f; Bh = 1.f;
     }
-    dx = chunk * 32 + lane;
-    return dx < P.rows[row].len;
 }
 
-// One cell per thread: a warp covers 32 cells of one row segment (PmlRow).  A memory
-// variable is read and written only on the axes on which the cell lies in
-// that axis' absorbing range (elsewhere a = 0, b = 1 keep it at zero).
-__global__ void __launch_bounds__(256) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
+// 4th-order y/z differences of the 4 cells of a group (stride s)
+__device__ __forceinline__ void sdp2(const float *__restrict__ f, int i0, int s, float c0, float c1, float *out) {
+    const float4 a = ld4(f, i0 + s), b = ld4(f, i0), c = ld4(f, i0 + 2 * s), d = ld4(f, i0 - s);
+    out[0] = c0 * (a.x - b.x) + c1 * (c.x - d.x);
+    out[1] = c0 * (a.y - b.y) + c1 * (c.y - d.y);
+    out[2] = c0 * (a.z - b.z) + c1 * (c.z - d.z);
+    out[3] = c0 * (a.w - b.w) + c1 * (c.w - d.w);
+}
+__device__ __forceinline__ void sdm2(const float *__restrict__ f, int i0, int s, float c0, float c1, float *out) {
+    const float4 a = ld4(f, i0), b = ld4(f, i0 - s), c = ld4(f, i0 + s), d = ld4(f, i0 - 2 * s);
+    out[0] = c0 * (a.x - b.x) + c1 * (c.x - d.x);
+    out[1] = c0 * (a.y - b.y) + c1 * (c.y - d.y);
+    out[2] = c0 * (a.z - b.z) + c1 * (c.z - d.z);
+    out[3] = c0 * (a.w - b.w) + c1 * (c.w - d.w);
+}
+// 4th-order x differences of the 4 cells from the 12-value window
+__device__ __forceinline__ void xdp2(const float *w, float c0, float c1, float *out) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) out[c] = c0 * (w[5 + c] - w[4 + c]) + c1 * (w[6 + c] - w[3 + c]);
+}
+__device__ __forceinline__ void xdm2(const float *w, float c0, float c1, float *out) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) out[c] = c0 * (w[4 + c] - w[3 + c]) + c1 * (w[5 + c] - w[2 + c]);
+}
+
+// b * psi + a * d for the 4 cells of a group (float4 memory variable)
+__device__ __forceinline__ void psi4(float *p, const float *B, const float *A, float *d) {
+    float4 v = *reinterpret_cast<float4 *>(p);
+    v.x = B[0] * v.x + A[0] * d[0];
+    v.y = B[1] * v.y + A[1] * d[1];
+    v.z = B[2] * v.z + A[2] * d[2];
+    v.w = B[3] * v.w + A[3] * d[3];
+    *reinterpret_cast<float4 *>(p) = v;
+    d[0] += v.x;
+    d[1] += v.y;
+    d[2] += v.z;
+    d[3] += v.w;
+}
+
+__device__ __forceinline__ void st4m(float *f, int i0, const float *v, unsigned mask) {
+    if (mask == 0xF) {
+        *reinterpret_cast<float4 *>(f + i0) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (mask & (1u << c)) f[i0 + c] = v[c];
+    }
+}
+
+// Thread -> one 4-cell x group of one row of one slab.  Returns false for
+// threads past the slab's groups or rows.
+struct PmlPos {
+    int xs, y, z;        // first cell of the group
+    unsigned mask;       // cells of the group inside the slab
+    long long psi;       // arena offset of the group's first memory variable
+    long long stride;    // floats between memory arrays of the slab
+    int naxes;
+};
+__device__ __forceinline__ bool pml_pos(const CpmlDev &P, PmlPos &q) {
+    const int b = blockIdx.x;
+    PmlSlab S = P.s[0];
+#pragma unroll
+    for (int k = 1; k < 6; k++)
+        if (k < P.nslab && b >= P.s[k].first_block) S = P.s[k];
+    const int lb = b - S.first_block;
+    const int bxi = lb % S.bx;
+    const int t = lb / S.bx;
+    const int byi = t % S.by;
+    q.z = S.z0 + t / S.by;
+    const int grp = bxi * S.gx + (threadIdx.x & (S.gx - 1));
+    q.y = S.y0 + byi * S.gy + (threadIdx.x >> S.lgx);
+    if (grp >= S.ngroups || q.y >= S.y1) return false;
+    q.xs = S.gstart + 4 * grp;
+    q.mask = 0;
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+        if (q.xs + c >= S.x0 && q.xs + c < S.x1) q.mask |= 1u << c;
+    q.psi = S.psi_off + ((long long)(q.z - S.z0) * (S.y1 - S.y0) + (q.y - S.y0)) * S.pitch + 4 * grp;
+    q.stride = S.stride;
+    q.naxes = S.naxes;
+    return true;
+}
+
+__device__ __forceinline__ void xcoef4(const CpmlDev &P, const PmlPos &q, float vp4[4], float *A, float *B,
+                                       float *Ah, float *Bh, bool &any) {
+    any = false;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (q.mask & (1u << c)) t = P.ax[0][q.xs + c];
+        any |= t.x > 0.f;
+        cpml_coef(vp4[c], t, P.dt, A[c], B[c], Ah[c], Bh[c]);
+    }
+}
+
+// CPML velocity update of the six absorbing slabs: 4th order, memory
+// variables on the absorbing axes (z-slabs x,y,z; y-slabs x,y; x-slabs x)
+// (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_2_kernel_device_{x,y,z}_meat.hpp)
+__global__ void __launch_bounds__(256, 3) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
                                                const float *__restrict__ vpm) {
-    int row, dx;
-    if (!pml_locate(P, row, dx)) return;
-    const PmlRow R = P.rows[row];
-    const float4 ty = P.ax[1][R.y], tz = P.ax[2][R.z];
-    const bool ya = ty.x > 0.f, za = tz.x > 0.f;
+    PmlPos q;
+    if (!pml_pos(P, q)) return;
     const int sy = (int)g.sy, sz = (int)g.sz;
-    const int base = (int)g.xoff + sy * R.y + sz * R.z;
+    const int i0 = (int)g.xoff + q.xs + sy * q.y + sz * q.z;
     const float c0 = c_dc2[0], c1 = c_dc2[1];
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    const int n = (int)R.ncell;
-    {
-        const int x = R.x0 + dx;
-        const int i = base + x;
-        float sxx_x = dp2(w.f[SXX], i, 1, c0, c1) * rdx;
-        float syx_x = dm2(w.f[SXY], i, 1, c0, c1) * rdx;
-        float szx_x = dm2(w.f[SXZ], i, 1, c0, c1) * rdx;
-        float sxy_y = dm2(w.f[SXY], i, sy, c0, c1) * rdy;
-        float syy_y = dp2(w.f[SYY], i, sy, c0, c1) * rdy;
-        float szy_y = dm2(w.f[SYZ], i, sy, c0, c1) * rdy;
-        float sxz_z = dm2(w.f[SXZ], i, sz, c0, c1) * rdz;
-        float syz_z = dm2(w.f[SYZ], i, sz, c0, c1) * rdz;
-        float szz_z = dp2(w.f[SZZ], i, sz, c0, c1) * rdz;
-        const float vp = __ldg(vpm + i);
-        const float4 tx = P.ax[0][x];
-        float *psi = P.psi + R.psi_off + dx;
-        float A, B, Ah, Bh;
-        if (tx.x > 0.f) {
-            cpml_coef(vp, tx, P.dt, A, B, Ah, Bh);
-            sxx_x += psi_step(psi + 0 * n, Bh, Ah, sxx_x);
-            syx_x += psi_step(psi + 1 * n, B, A, syx_x);
-            szx_x += psi_step(psi + 2 * n, B, A, szx_x);
-        }
-        if (ya) {
-            cpml_coef(vp, ty, P.dt, A, B, Ah, Bh);
-            sxy_y += psi_step(psi + 3 * n, B, A, sxy_y);
-            syy_y += psi_step(psi + 4 * n, Bh, Ah, syy_y);
-            szy_y += psi_step(psi + 5 * n, B, A, szy_y);
-        }
-        if (za) {
-            cpml_coef(vp, tz, P.dt, A, B, Ah, Bh);
-            sxz_z += psi_step(psi + 6 * n, B, A, sxz_z);
-            syz_z += psi_step(psi + 7 * n, B, A, syz_z);
-            szz_z += psi_step(psi + 8 * n, Bh, Ah, szz_z);
-        }
-        const float dtr = P.dt / __ldg(rho + i);
-        w.f[VX][i] += dtr * (sxx_x + sxy_y + sxz_z);
-        w.f[VY][i] += dtr * (syx_x + syy_y + syz_z);
-        w.f[VZ][i] += dtr * (szx_x + szy_y + szz_z);
+    float win[12], sxx_x[4], syx_x[4], szx_x[4], sxy_y[4], syy_y[4], szy_y[4], sxz_z[4], syz_z[4], szz_z[4];
+    xwin(w.f[SXX], i0, win);
+    xdp2(win, c0, c1, sxx_x);
+    xwin(w.f[SXY], i0, win);
+    xdm2(win, c0, c1, syx_x);
+    xwin(w.f[SXZ], i0, win);
+    xdm2(win, c0, c1, szx_x);
+    sdm2(w.f[SXY], i0, sy, c0, c1, sxy_y);
+    sdp2(w.f[SYY], i0, sy, c0, c1, syy_y);
+    sdm2(w.f[SYZ], i0, sy, c0, c1, szy_y);
+    sdm2(w.f[SXZ], i0, sz, c0, c1, sxz_z);
+    sdm2(w.f[SYZ], i0, sz, c0, c1, syz_z);
+    sdp2(w.f[SZZ], i0, sz, c0, c1, szz_z);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        sxx_x[c] *= rdx; syx_x[c] *= rdx; szx_x[c] *= rdx;
+        sxy_y[c] *= rdy; syy_y[c] *= rdy; szy_y[c] *= rdy;
+        sxz_z[c] *= rdz; syz_z[c] *= rdz; szz_z[c] *= rdz;
     }
+    float vp4[4];
+    f4a(vp4, ld4(vpm, i0));
+    float *psi = P.psi + q.psi;
+    const long long n = q.stride;
+    float A[4], B[4], Ah[4], Bh[4];
+    bool any;
+    xcoef4(P, q, vp4, A, B, Ah, Bh, any);
+    if (any) {
+        psi4(psi + 0 * n, Bh, Ah, sxx_x);
+        psi4(psi + 1 * n, B, A, syx_x);
+        psi4(psi + 2 * n, B, A, szx_x);
+    }
+    const float4 ty = P.ax[1][q.y], tz = P.ax[2][q.z];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ty.x > 0.f) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) cpml_coef(vp4[c], (q.mask >> c) & 1u ? ty : z4, P.dt, A[c], B[c], Ah[c], Bh[c]);
+        psi4(psi + 3 * n, B, A, sxy_y);
+        psi4(psi + 4 * n, Bh, Ah, syy_y);
+        psi4(psi + 5 * n, B, A, szy_y);
+    }
+    if (tz.x > 0.f) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) cpml_coef(vp4[c], (q.mask >> c) & 1u ? tz : z4, P.dt, A[c], B[c], Ah[c], Bh[c]);
+        psi4(psi + 6 * n, B, A, sxz_z);
+        psi4(psi + 7 * n, B, A, syz_z);
+        psi4(psi + 8 * n, Bh, Ah, szz_z);
+    }
+    float r4[4], v[4];
+    f4a(r4, ld4(rho, i0));
+    float dtr[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) dtr[c] = P.dt / r4[c];
+    f4a(v, ldw4(w.f[VX], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) v[c] += dtr[c] * (sxx_x[c] + sxy_y[c] + sxz_z[c]);
+    st4m(w.f[VX], i0, v, q.mask);
+    f4a(v, ldw4(w.f[VY], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) v[c] += dtr[c] * (syx_x[c] + syy_y[c] + syz_z[c]);
+    st4m(w.f[VY], i0, v, q.mask);
+    f4a(v, ldw4(w.f[VZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) v[c] += dtr[c] * (szx_x[c] + szy_y[c] + szz_z[c]);
+    st4m(w.f[VZ], i0, v, q.mask);
 }
 
 template <bool WITH_SAU>
-__global__ void __launch_bounds__(256) stress_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ lam,
+__global__ void __launch_bounds__(256, 3) stress_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ lam,
                                                   const float *__restrict__ mu, const float *__restrict__ vpm) {
-    int row, dx;
-    if (!pml_locate(P, row, dx)) return;
-    const PmlRow R = P.rows[row];
-    const float4 ty = P.ax[1][R.y], tz = P.ax[2][R.z];
-    const bool ya = ty.x > 0.f, za = tz.x > 0.f;
+    PmlPos q;
+    if (!pml_pos(P, q)) return;
     const int sy = (int)g.sy, sz = (int)g.sz;
-    const int base = (int)g.xoff + sy * R.y + sz * R.z;
+    const int i0 = (int)g.xoff + q.xs + sy * q.y + sz * q.z;
     const float c0 = c_dc2[0], c1 = c_dc2[1];
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    const int n = (int)R.ncell;
-    {
-        const int x = R.x0 + dx;
-        const int i = base + x;
-        float vx_x = dm2(w.f[VX], i, 1, c0, c1) * rdx;
-        float vy_x = dp2(w.f[VY], i, 1, c0, c1) * rdx;
-        float vz_x = dp2(w.f[VZ], i, 1, c0, c1) * rdx;
-        float vx_y = dp2(w.f[VX], i, sy, c0, c1) * rdy;
-        float vy_y = dm2(w.f[VY], i, sy, c0, c1) * rdy;
-        float vz_y = dp2(w.f[VZ], i, sy, c0, c1) * rdy;
-        float vx_z = dp2(w.f[VX], i, sz, c0, c1) * rdz;
-        float vy_z = dp2(w.f[VY], i, sz, c0, c1) * rdz;
-        float vz_z = dm2(w.f[VZ], i, sz, c0, c1) * rdz;
-        const float vp = __ldg(vpm + i);
-        const float4 tx = P.ax[0][x];
-        float *psi = P.psi + R.psi_off + 3LL * R.naxes * n + dx;
-        float A, B, Ah, Bh;
-        if (tx.x > 0.f) {
-            cpml_coef(vp, tx, P.dt, A, B, Ah, Bh);
-            vx_x += psi_step(psi + 0 * n, B, A, vx_x);
-            vy_x += psi_step(psi + 1 * n, Bh, Ah, vy_x);
-            vz_x += psi_step(psi + 2 * n, Bh, Ah, vz_x);
-        }
-        if (ya) {
-            cpml_coef(vp, ty, P.dt, A, B, Ah, Bh);
-            vy_y += psi_step(psi + 3 * n, B, A, vy_y);
-            vx_y += psi_step(psi + 4 * n, Bh, Ah, vx_y);
-            vz_y += psi_step(psi + 5 * n, Bh, Ah, vz_y);
-        }
-        if (za) {
-            cpml_coef(vp, tz, P.dt, A, B, Ah, Bh);
-            vz_z += psi_step(psi + 6 * n, B, A, vz_z);
-            vx_z += psi_step(psi + 7 * n, Bh, Ah, vx_z);
-            vy_z += psi_step(psi + 8 * n, Bh, Ah, vy_z);
-        }
-        const float l = __ldg(lam + i), m = __ldg(mu + i);
-        const float l2m = l + 2.0f * m;
-        const float dt = P.dt;
-        w.f[SXX][i] += dt * (l2m * vx_x + l * vy_y + l * vz_z);
-        w.f[SYY][i] += dt * (l * vx_x + l2m * vy_y + l * vz_z);
-        w.f[SZZ][i] += dt * (l * vx_x + l * vy_y + l2m * vz_z);
-        if (WITH_SAU) w.f[SAU][i] += dt * (l2m * vx_x + l2m * vy_y + l2m * vz_z);
-        w.f[SXY][i] += dt * m * (vy_x + vx_y);
-        w.f[SXZ][i] += dt * m * (vz_x + vx_z);
-        w.f[SYZ][i] += dt * m * (vz_y + vy_z);
+    float win[12], vx_x[4], vy_x[4], vz_x[4], vx_y[4], vy_y[4], vz_y[4], vx_z[4], vy_z[4], vz_z[4];
+    xwin(w.f[VX], i0, win);
+    xdm2(win, c0, c1, vx_x);
+    xwin(w.f[VY], i0, win);
+    xdp2(win, c0, c1, vy_x);
+    xwin(w.f[VZ], i0, win);
+    xdp2(win, c0, c1, vz_x);
+    sdp2(w.f[VX], i0, sy, c0, c1, vx_y);
+    sdm2(w.f[VY], i0, sy, c0, c1, vy_y);
+    sdp2(w.f[VZ], i0, sy, c0, c1, vz_y);
+    sdp2(w.f[VX], i0, sz, c0, c1, vx_z);
+    sdp2(w.f[VY], i0, sz, c0, c1, vy_z);
+    sdm2(w.f[VZ], i0, sz, c0, c1, vz_z);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        vx_x[c] *= rdx; vy_x[c] *= rdx; vz_x[c] *= rdx;
+        vx_y[c] *= rdy; vy_y[c] *= rdy; vz_y[c] *= rdy;
+        vx_z[c] *= rdz; vy_z[c] *= rdz; vz_z[c] *= rdz;
     }
+    float vp4[4];
+    f4a(vp4, ld4(vpm, i0));
+    float *psi = P.psi + q.psi + 3LL * q.naxes * q.stride;
+    const long long n = q.stride;
+    float A[4], B[4], Ah[4], Bh[4];
+    bool any;
+    xcoef4(P, q, vp4, A, B, Ah, Bh, any);
+    if (any) {
+        psi4(psi + 0 * n, B, A, vx_x);
+        psi4(psi + 1 * n, Bh, Ah, vy_x);
+        psi4(psi + 2 * n, Bh, Ah, vz_x);
+    }
+    const float4 ty = P.ax[1][q.y], tz = P.ax[2][q.z];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ty.x > 0.f) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) cpml_coef(vp4[c], (q.mask >> c) & 1u ? ty : z4, P.dt, A[c], B[c], Ah[c], Bh[c]);
+        psi4(psi + 3 * n, B, A, vy_y);
+        psi4(psi + 4 * n, Bh, Ah, vx_y);
+        psi4(psi + 5 * n, Bh, Ah, vz_y);
+    }
+    if (tz.x > 0.f) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) cpml_coef(vp4[c], (q.mask >> c) & 1u ? tz : z4, P.dt, A[c], B[c], Ah[c], Bh[c]);
+        psi4(psi + 6 * n, B, A, vz_z);
+        psi4(psi + 7 * n, Bh, Ah, vx_z);
+        psi4(psi + 8 * n, Bh, Ah, vy_z);
+    }
+    float l[4], m[4], a[4];
+    f4a(l, ld4(lam, i0));
+    f4a(m, ld4(mu, i0));
+    const float dt = P.dt;
+    f4a(a, ldw4(w.f[SXX], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * ((l[c] + 2.0f * m[c]) * vx_x[c] + l[c] * vy_y[c] + l[c] * vz_z[c]);
+    st4m(w.f[SXX], i0, a, q.mask);
+    f4a(a, ldw4(w.f[SYY], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * (l[c] * vx_x[c] + (l[c] + 2.0f * m[c]) * vy_y[c] + l[c] * vz_z[c]);
+    st4m(w.f[SYY], i0, a, q.mask);
+    f4a(a, ldw4(w.f[SZZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * (l[c] * vx_x[c] + l[c] * vy_y[c] + (l[c] + 2.0f * m[c]) * vz_z[c]);
+    st4m(w.f[SZZ], i0, a, q.mask);
+    if (WITH_SAU) {
+        f4a(a, ldw4(w.f[SAU], i0));
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float l2m = l[c] + 2.0f * m[c];
+            a[c] += dt * (l2m * vx_x[c] + l2m * vy_y[c] + l2m * vz_z[c]);
+        }
+        st4m(w.f[SAU], i0, a, q.mask);
+    }
+    f4a(a, ldw4(w.f[SXY], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * m[c] * (vy_x[c] + vx_y[c]);
+    st4m(w.f[SXY], i0, a, q.mask);
+    f4a(a, ldw4(w.f[SXZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * m[c] * (vz_x[c] + vx_z[c]);
+    st4m(w.f[SXZ], i0, a, q.mask);
+    f4a(a, ldw4(w.f[SYZ], i0));
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] += dt * m[c] * (vz_y[c] + vy_z[c]);
+    st4m(w.f[SYZ], i0, a, q.mask);
 }
 
 // ------------------------------------------------------------ receivers
@@ -1130,17 +1251,15 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
 }
 
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp, void *stream) {
-    if (c.nrows <= 0) return 0;
-    const long long warps = (long long)c.nlong * c.cpl + (long long)(c.nrows - c.nlong) * c.cps;
-    vel_pml<<<(unsigned)((warps + 7) / 8), 256, 0, (cudaStream_t)stream>>>(g, c, w, rho, vp);
+    if (c.nblocks <= 0) return 0;
+    vel_pml<<<(unsigned)c.nblocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, rho, vp);
     return cerr();
 }
 
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
                  const float *vp, int with_sau, void *stream) {
-    if (c.nrows <= 0) return 0;
-    const long long warps = (long long)c.nlong * c.cpl + (long long)(c.nrows - c.nlong) * c.cps;
-    const unsigned blocks = (unsigned)((warps + 7) / 8);
+    if (c.nblocks <= 0) return 0;
+    const unsigned blocks = (unsigned)c.nblocks;
     if (with_sau) stress_pml<true><<<blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
     else stress_pml<false><<<blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
     return cerr();
