@@ -40,7 +40,7 @@ EXPORTS = (
     "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_get_info", "jv_forward",
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
     "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
-    "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info",
+    "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info", "jv_forward_noalloc",
 )
 
 
@@ -106,6 +106,8 @@ def lib() -> C.CDLL:
     L.jv_set_profiling.argtypes = [ctxp, C.c_int]
     L.jv_profile_entry.argtypes = [ctxp, C.c_int, C.POINTER(C.c_char_p), dp, C.POINTER(C.c_longlong)]
     L.jv_run_project.argtypes = [ctxp]
+    L.jv_forward_noalloc.argtypes = [C.POINTER(Grid), vp, vp, vp, C.c_float, C.c_float, C.c_int, fp, C.c_int, fp,
+                                     vp, vp, vp, C.POINTER(C.c_int), vp]
     L.jv_last_timing.argtypes = [ctxp, dp]
     L.jv_sync.argtypes = [ctxp]
     L.jv_close.argtypes = [ctxp]

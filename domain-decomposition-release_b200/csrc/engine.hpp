@@ -28,6 +28,9 @@ int ntime(float T, float dt);
 // Ricker wavelet as the reference builds it (seisrecord_meat.hpp:279-285)
 void ricker(int nt, float fm, float dt, float *w);
 
+// message returned by jv_last_error() on the calling thread
+void set_last_error(const std::string &m);
+
 struct Status {
     jv_status code = JV_OK;
     std::string msg;

@@ -26,6 +26,11 @@ jv_status fail(jv_status c, const std::string &m) {
 }
 }  // namespace
 
+namespace jv {
+// lets other translation units of the library report through jv_last_error()
+void set_last_error(const std::string &m) { g_err = m; }
+}  // namespace jv
+
 struct jv_ctx {
     std::unique_ptr<jv::Engine> eng;
     bool from_project = false;

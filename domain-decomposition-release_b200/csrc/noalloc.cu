@@ -1,0 +1,278 @@
+// noalloc.cu -- forward modelling without any device allocation.
+//
+// Who needs this: callers that must not call cudaMalloc/cudaFree at the
+// moment they model a shot.  Examples are a host application whose memory
+// pool (a framework's caching allocator, a reserved arena) already owns all
+// free device memory, so a fresh cudaMalloc would fail; latency-sensitive
+// paths where an allocation or free could block or synchronise the device;
+// and plug-in hosts that forbid a plug-in from owning device memory at all.
+// They pass every input and output; the working memory (wavefield, CPML
+// memory variables, extended model, tables, receiver indices, step state)
+// is carved out of one fixed scratch array compiled into this library.
+//
+// The scratch array lives for as long as the library is loaded, on every
+// GPU that loads it (kNoAllocScratchBytes, 64 MiB).  Every call shares it
+// and finds the previous call's contents in it: each call rewrites the
+// tables and clears the wavefield and memory variables before it starts.
+// Two calls whose GPU work overlaps (two host threads, or two streams on
+// one device) race on the same array and produce garbage; serialise them.
+//
+// Host code cannot use the array's name as a device address (in host code
+// it is a host-side stand-in), so the first call on each device, with that
+// device current, looks the address up with cudaGetSymbolAddress and caches
+// it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "jv/jv.h"
+#include "jv_internal.hpp"
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+void *g_addr[kMaxDevices] = {};
+
+jv_status fail(jv_status c, const std::string &m) {
+    jv::set_last_error(m);
+    return c;
+}
+
+// device address of the scratch array for `dev` (looked up once per device)
+jv_status scratch_address(int dev, unsigned char **out) {
+    if (dev < 0 || dev >= kMaxDevices) return fail(JV_EINVAL, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(JV_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_addr[dev] = p;
+    }
+    *out = (unsigned char *)g_addr[dev];
+    return JV_OK;
+}
+
+// bump allocator over the scratch array (256-byte aligned pieces)
+struct Carver {
+    unsigned char *base;
+    size_t used = 0, cap;
+    template <class T>
+    T *take(size_t count) {
+        size_t off = (used + 255) & ~size_t(255);
+        size_t bytes = count * sizeof(T);
+        if (off + bytes > cap) return nullptr;
+        used = off + bytes;
+        return reinterpret_cast<T *>(base + off);
+    }
+};
+
+long long rup(long long v, long long a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, const float *d_vs, const float *d_rho,
+                                        float dt, float fm, int nt, const float *src_xyz, int n_recv,
+                                        const float *recv_xyz, float *d_vx, float *d_vy, float *d_vz,
+                                        int *n_kept, void *stream) {
+    using namespace jv;
+    if (!grid || !d_vp || !d_vs || !d_rho || !src_xyz || (n_recv > 0 && !recv_xyz) || !n_kept)
+        return fail(JV_EINVAL, "jv_forward_noalloc: NULL argument");
+    if (grid->nx < 8 || grid->ny < 8 || grid->nz < 8) return fail(JV_EINVAL, "gridphy must have >= 8 cells per axis");
+    if (grid->pml < kPhyHalf) return fail(JV_EINVAL, "pml_num must be >= 4");
+    if (!(grid->dx > 0) || !(grid->dy > 0) || !(grid->dz > 0) || !(dt > 0) || !(fm > 0) || nt < 1)
+        return fail(JV_EINVAL, "spacing, dt, fm must be > 0 and nt >= 1");
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(JV_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+
+    // layout: the same pitched gridext layout as the context path
+    const int m = grid->pml;
+    GridDev g{};
+    g.m = m;
+    g.px = grid->nx; g.py = grid->ny; g.pz = grid->nz;
+    g.nx = g.px + 2 * m; g.ny = g.py + 2 * m; g.nz = g.pz + 2 * m;
+    g.xoff = (32 - (m % 32)) % 32;
+    g.sy = rup(g.xoff + g.nx, 32);
+    g.sz = g.sy * g.ny;
+    g.dx = grid->dx; g.dy = grid->dy; g.dz = grid->dz;
+    const size_t fe = (size_t)rup(g.sz * g.nz + 128, 64);
+    const size_t guard = 32;
+
+    // CPML slabs (shape as in the context path)
+    CpmlDev cp{};
+    long long psi_total = 0;
+    {
+        const int NX = g.nx, NY = g.ny, NZ = g.nz;
+        const int bx[6][6] = {
+            {2, NX - 2, 2, NY - 2, 2, m},           {2, NX - 2, 2, NY - 2, NZ - m, NZ - 2},
+            {2, NX - 2, 2, m, m, NZ - m},           {2, NX - 2, NY - m, NY - 2, m, NZ - m},
+            {2, m, m, NY - m, m, NZ - m},           {NX - m, NX - 2, m, NY - m, m, NZ - m},
+        };
+        const int na[6] = {3, 3, 2, 2, 1, 1};
+        int blocks = 0;
+        for (int q = 0; q < 6; q++) {
+            PmlSlab S{};
+            S.x0 = bx[q][0]; S.x1 = bx[q][1]; S.y0 = bx[q][2]; S.y1 = bx[q][3]; S.z0 = bx[q][4]; S.z1 = bx[q][5];
+            S.naxes = na[q];
+            if (S.x1 <= S.x0 || S.y1 <= S.y0 || S.z1 <= S.z0) continue;
+            S.gstart = S.x0 - (int)((g.xoff + S.x0) & 3);
+            S.ngroups = (S.x1 - S.gstart + 3) / 4;
+            S.pitch = 4 * S.ngroups;
+            S.gx = 1;
+            S.lgx = 0;
+            while (S.gx < S.ngroups && S.gx < 32) {
+                S.gx *= 2;
+                S.lgx++;
+            }
+            S.gy = 256 / S.gx;
+            S.bx = (S.ngroups + S.gx - 1) / S.gx;
+            S.by = (S.y1 - S.y0 + S.gy - 1) / S.gy;
+            S.first_block = blocks;
+            blocks += S.bx * S.by * (S.z1 - S.z0);
+            S.stride = (long long)S.pitch * (S.y1 - S.y0) * (S.z1 - S.z0);
+            S.psi_off = psi_total;
+            psi_total += 6LL * S.naxes * S.stride;
+            cp.s[cp.nslab++] = S;
+        }
+        cp.nblocks = blocks;
+        cp.dt = dt;
+    }
+
+    // receivers inside gridphy, in input order (as jv_set_geometry keeps them)
+    const float rx = (float)(g.px - 1) * g.dx, ry = (float)(g.py - 1) * g.dy, rz = (float)(g.pz - 1) * g.dz;
+    const float lx = -(float)m * g.dx, ly = -(float)m * g.dy, lz = -(float)m * g.dz;
+    auto inside = [&](const float *q) {
+        return q[0] >= 0.0f && q[0] <= rx && q[1] >= 0.0f && q[1] <= ry && q[2] >= 0.0f && q[2] <= rz;
+    };
+    auto elem = [&](const float *q) -> long long {
+        return g.xoff + gap_num(lx, q[0], g.dx) + g.sy * gap_num(ly, q[1], g.dy) + g.sz * gap_num(lz, q[2], g.dz);
+    };
+    if (!inside(src_xyz)) return fail(JV_EINVAL, "source lies outside gridphy");
+    std::vector<long long> rec;
+    for (int r = 0; r < n_recv; r++)
+        if (inside(recv_xyz + 3 * r)) rec.push_back(elem(recv_xyz + 3 * r));
+    *n_kept = (int)rec.size();
+
+    // carve the scratch array; refuse problems that do not fit
+    unsigned char *base = nullptr;
+    jv_status st = scratch_address(dev, &base);
+    if (st != JV_OK) return st;
+    Carver cv{base, 0, kNoAllocScratchBytes};
+    float *model = cv.take<float>(4 * fe + guard);
+    float *wave = cv.take<float>(9 * fe + guard);
+    float *psi = cv.take<float>((size_t)psi_total);
+    float4 *tabs[3];
+    for (int a = 0; a < 3; a++) tabs[a] = cv.take<float4>((size_t)(a == 0 ? g.nx : a == 1 ? g.ny : g.nz));
+    float *wavelet = cv.take<float>((size_t)nt);
+    StepState *state = cv.take<StepState>(1);
+    long long *rec_d = cv.take<long long>(rec.size() + 1);
+    if (!model || !wave || (psi_total && !psi) || !tabs[0] || !tabs[1] || !tabs[2] || !wavelet || !state || !rec_d)
+        return fail(JV_EINVAL, "problem needs more than the " + std::to_string(kNoAllocScratchBytes >> 20) +
+                                   " MiB no-allocation scratch; use jv_create/jv_forward");
+    if (fe >= ((size_t)1 << 31)) return fail(JV_EINVAL, "grid too large");
+
+    // coefficient tables (constant memory, no allocation)
+    float list[5][4] = {};
+    for (int o = 1; o <= 4; o++) {
+        double c[4];
+        diff_coeff(o, c);
+        for (int i = 0; i < o; i++) list[o][i] = (float)c[i];
+    }
+    double c2[2];
+    diff_coeff(2, c2);
+    const float dc2[2] = {(float)c2[0], (float)c2[1]};
+    if (upload_coefficients(list, dc2) != 0) return fail(JV_ECUDA, "coefficient upload failed");
+
+    // host-side tables, copied into the scratch array
+    std::vector<float4> t[3];
+    {
+        const double N = (double)(m - kPmlHalf);
+        const double l10x7 = (double)(std::log10(1.0f / 0.001f) * 7.0f);
+        const float alpha_max = (float)(3.14159265358979323846 * (double)fm);
+        const int nax[3] = {g.nx, g.ny, g.nz};
+        const float del[3] = {g.dx, g.dy, g.dz};
+        for (int a = 0; a < 3; a++) {
+            const int n = nax[a];
+            t[a].assign(n, make_float4(0.f, 0.f, 0.f, 0.f));
+            for (int c = 0; c < n; c++) {
+                double sI, sH;
+                if (c >= kPmlHalf && c < m) {
+                    sI = m - c;
+                    sH = m - c - 0.5;
+                } else if (c >= n - m && c < n - kPmlHalf) {
+                    sH = c - (n - m - 1);
+                    sI = sH - 0.5;
+                } else {
+                    continue;
+                }
+                const double k0 = l10x7 / (2.0 * N * (double)del[a]);
+                const float qI = (float)sI / (float)N, qH = (float)sH / (float)N;
+                t[a][c].x = (float)(k0 * (double)qI * (double)qI);
+                t[a][c].y = (float)(k0 * (double)qH * (double)qH);
+                t[a][c].z = std::max(alpha_max * (1.0f - qI), 0.0f);
+                t[a][c].w = std::max(alpha_max * (1.0f - qH), 0.0f);
+            }
+        }
+    }
+    std::vector<float> wl(nt);
+    ricker(nt, fm, dt, wl.data());
+    StepState hs{};
+    hs.it = 0;
+    hs.src = elem(src_xyz);
+    hs.tr[0] = d_vx;
+    hs.tr[1] = d_vy;
+    hs.tr[2] = d_vz;
+
+    auto ck = [&](cudaError_t ee, const char *what) -> jv_status {
+        if (ee != cudaSuccess) return fail(JV_ECUDA, std::string(what) + ": " + cudaGetErrorString(ee));
+        return JV_OK;
+    };
+#define NA_CK(expr)                                    \
+    do {                                               \
+        jv_status _s = ck((cudaError_t)(expr), #expr); \
+        if (_s != JV_OK) return _s;                    \
+    } while (0)
+    for (int a = 0; a < 3; a++)
+        NA_CK(cudaMemcpyAsync(tabs[a], t[a].data(), t[a].size() * sizeof(float4), cudaMemcpyHostToDevice, s));
+    NA_CK(cudaMemcpyAsync(wavelet, wl.data(), nt * sizeof(float), cudaMemcpyHostToDevice, s));
+    NA_CK(cudaMemcpyAsync(state, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    if (!rec.empty()) NA_CK(cudaMemcpyAsync(rec_d, rec.data(), rec.size() * sizeof(long long), cudaMemcpyHostToDevice, s));
+    // the previous call left its state here: clear what must start at zero
+    NA_CK(cudaMemsetAsync(model, 0, (4 * fe + guard) * sizeof(float), s));
+    NA_CK(cudaMemsetAsync(wave, 0, (9 * fe + guard) * sizeof(float), s));
+    if (psi_total) NA_CK(cudaMemsetAsync(psi, 0, (size_t)psi_total * sizeof(float), s));
+
+    float *mb = model + guard;
+    float *vp = mb, *rho = mb + fe, *lam = mb + 2 * fe, *mu = mb + 3 * fe;
+    NA_CK(k_model_prep(g, d_vp, d_vs, d_rho, vp, rho, lam, mu, s));
+    WaveDev w{};
+    for (int f = 0; f < 9; f++) w.f[f] = wave + guard + f * fe;
+    for (int a = 0; a < 3; a++) cp.ax[a] = tabs[a];
+    cp.psi = psi;
+    KCfg kc;
+    kc.variant = 2;
+    for (int it = 0; it < nt; it++) {
+        NA_CK(k_vel_pml(g, cp, w, rho, vp, s));
+        NA_CK(k_vel_phy(kFwd, g, w, rho, dt, 1, nullptr, nullptr, kc, s));
+        NA_CK(k_stress_pml(g, cp, w, lam, mu, vp, 0, s));
+        NA_CK(k_stress_phy(kFwd, g, w, lam, mu, dt, 1, wavelet, state, kc, s));
+        NA_CK(k_record(w, rec_d, (int)rec.size(), nt, state, s));
+        NA_CK(k_step_advance(state, +1, s));
+    }
+    NA_CK(cudaStreamSynchronize(s));
+#undef NA_CK
+    jv::set_last_error("");
+    return JV_OK;
+}

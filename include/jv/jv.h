@@ -184,6 +184,25 @@ jv_status jv_last_timing(const jv_ctx *c, double *ms);
 jv_status jv_set_profiling(jv_ctx *c, int on);
 jv_status jv_profile_entry(const jv_ctx *c, int idx, const char **name, double *total_ms, long long *launches);
 
+/* Forward modelling of one shot that allocates no device memory, for
+ * callers that cannot call cudaMalloc/cudaFree when they model (their
+ * memory pool already holds the free device memory, or an allocation could
+ * block or synchronise a latency-critical path).  No counterpart in the
+ * reference.  Inputs are device arrays on gridphy (vp, vs, rho) and host
+ * positions; d_vx/d_vy/d_vz receive [n_kept][nt] traces of the receivers
+ * inside gridphy (*n_kept of them, at most n_recv).  Working memory comes
+ * from one 64 MiB array compiled into the library, held on every device that
+ * loads it; problems that need more are rejected with JV_EINVAL (the
+ * limit is about 0.5 M cells of gridext, e.g. a 60^3 interior with a 10-cell
+ * absorbing layer).  The first call on a device looks up that
+ * array's address.  All calls share
+ * the array: calls whose GPU work overlaps race; the call clears what must
+ * start at zero and returns after its work on `stream` (cudaStream_t, NULL
+ * for the legacy stream) has finished. */
+jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, const float *d_vs, const float *d_rho, float dt,
+                             float fm, int nt, const float *src_xyz, int n_recv, const float *recv_xyz, float *d_vx,
+                             float *d_vy, float *d_vz, int *n_kept, void *stream);
+
 /* Waits for all work of the context. */
 jv_status jv_sync(jv_ctx *c);
 
