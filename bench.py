@@ -169,6 +169,8 @@ def pml_bytes(s, name):
     axes = ax[ix].sum() * iy.sum() * iz.sum() + ay[iy].sum() * ix.sum() * iz.sum() + az[iz].sum() * ix.sum() * iy.sum()
     if name == "vel_pml":
         per = 4 * (6 + 1 + 1 + 3) + 4 * 3
+    elif name == "stress_pml":
+        per = 4 * (3 + 3 + 6) + 4 * 6
     else:
         per = 4 * (3 + 3 + 7) + 4 * 7
     return float(cells * per + axes * 3 * 8)
@@ -323,6 +325,17 @@ def main():
         name, (ms, n) = max(prof.items(), key=lambda kv: kv[1][0])
         b = kernel_bytes(s, name)
         peak, peak_kind = load_peaks()
+        if rank == 0:
+            print(f"per-kernel device time, one instrumented RTM shot ({s.name}, CUDA events on the library stream):",
+                  file=sys.stderr)
+            print(f"  {'kernel':22s} {'launches':>8s} {'us/launch':>10s} {'share':>7s} {'alg. bytes':>12s} "
+                  f"{'GB/s':>8s} {'of peak':>8s}", file=sys.stderr)
+            for k, (kms, kn) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+                kb = kernel_bytes(s, k)
+                us = 1000.0 * kms / max(kn, 1)
+                gbs = kb / (us * 1e-6) / 1e9 if kb else float("nan")
+                print(f"  {k:22s} {kn:8d} {us:10.1f} {kms / tot:7.1%} {kb or 0:12.4g} {gbs:8.0f} "
+                      f"{gbs / peak:8.1%}", file=sys.stderr)
         if b is not None and n > 0:
             avg_s = ms / n / 1000.0
             ach = b / avg_s / 1e9
@@ -364,6 +377,16 @@ def main():
                          f"{c['seconds']:.1f} s, scaled to a full shot",
                "gcell_updates_per_s": round(c["gcells"], 4)}
 
+    # the job's one exchange: sum the FP64 stacks of all replicas (after timing)
+    reduce_ms = None
+    if dist is not None:
+        rep = importlib.import_module("domain-decomposition-release_b200.replicas")
+        barrier()
+        t0 = time.perf_counter()
+        rep.reduce_images(ctx, device=local)
+        barrier()
+        reduce_ms = round(1000.0 * (time.perf_counter() - t0), 2)
+
     launches = sum(v[1] for v in prof.values()) if prof else None
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "shots/h", "n_gpus": world, "steps": args.steps,
@@ -378,6 +401,8 @@ def main():
         "gpu_launches": launches * args.steps if launches else None,
         "wall_s": round(wall, 3),
     }
+    if reduce_ms is not None:
+        line["image_allreduce_ms"] = reduce_ms
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -41,6 +41,7 @@ EXPORTS = (
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
     "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
     "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info", "jv_forward_noalloc",
+    "jv_image_set", "jv_image_set_device",
 )
 
 
@@ -103,6 +104,8 @@ def lib() -> C.CDLL:
     L.jv_image_get.argtypes = [ctxp, C.c_int, dp]
     L.jv_image_finalize.argtypes = [ctxp] + [fp] * 8
     L.jv_image_get_device.argtypes = [ctxp, C.c_int, vp]
+    L.jv_image_set.argtypes = [ctxp, C.c_int, dp]
+    L.jv_image_set_device.argtypes = [ctxp, C.c_int, vp]
     L.jv_set_profiling.argtypes = [ctxp, C.c_int]
     L.jv_profile_entry.argtypes = [ctxp, C.c_int, C.POINTER(C.c_char_p), dp, C.POINTER(C.c_longlong)]
     L.jv_run_project.argtypes = [ctxp]
@@ -237,6 +240,18 @@ class Context:
     def image_to_device(self, kind: int, dev_ptr: int) -> None:
         """Copies one FP64 accumulator into device memory at dev_ptr."""
         _check(lib().jv_image_get_device(self._h, kind, C.c_void_p(int(dev_ptr))))
+
+    def set_image(self, kind: int, arr: np.ndarray) -> None:
+        """Overwrites one FP64 accumulator from a host array of gridphy."""
+        i = self.info()
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.size != i.n_phy:
+            raise JvError(JV_EINVAL, f"image has {a.size} values, gridphy has {i.n_phy}")
+        _check(lib().jv_image_set(self._h, kind, a.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def image_from_device(self, kind: int, dev_ptr: int) -> None:
+        """Overwrites one FP64 accumulator from device memory at dev_ptr."""
+        _check(lib().jv_image_set_device(self._h, kind, C.c_void_p(int(dev_ptr))))
 
     def set_profiling(self, on: bool) -> None:
         _check(lib().jv_set_profiling(self._h, 1 if on else 0))

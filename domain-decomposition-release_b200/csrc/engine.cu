@@ -736,6 +736,17 @@ Status Engine::image_get_device(int kind, double *out) {
     return Status{};
 }
 
+Status Engine::image_set(int kind, const double *src, bool src_on_device) {
+    JV_CU(cudaSetDevice(dev_));
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    double *dst[5] = {img_.ip, img_.pp, img_.ps, img_.sp, img_.ss};
+    if (kind < 0 || kind > 4 || !src) return bad(JV_EINVAL, "bad image kind / input");
+    JV_CU(cudaMemcpyAsync(dst[kind], src, nphy * sizeof(double),
+                          src_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return Status{};
+}
+
 Status Engine::sync() {
     JV_CU(cudaSetDevice(dev_));
     JV_CU(cudaStreamSynchronize(stream_));

@@ -50,6 +50,7 @@ class Engine {
     Status image_get(int kind, double *host_out);
     Status image_finalize(float *host_out[8]);
     Status image_get_device(int kind, double *dev_out);
+    Status image_set(int kind, const double *src, bool src_on_device);
 
     // per-kernel timing with CUDA events (direct launches, no graphs)
     void set_profiling(bool on);

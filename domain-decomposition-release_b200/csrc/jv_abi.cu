@@ -214,6 +214,16 @@ jv_status jv_image_get_device(jv_ctx *c, int kind, double *d_out) {
     return ret(c->eng->image_get_device(kind, d_out));
 }
 
+jv_status jv_image_set(jv_ctx *c, int kind, const double *in) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->image_set(kind, in, false));
+}
+
+jv_status jv_image_set_device(jv_ctx *c, int kind, const double *d_in) {
+    if (!c) return fail(JV_EINVAL, "NULL context");
+    return ret(c->eng->image_set(kind, d_in, true));
+}
+
 jv_status jv_set_profiling(jv_ctx *c, int on) {
     if (!c) return fail(JV_EINVAL, "NULL context");
     c->eng->set_profiling(on != 0);

@@ -163,6 +163,16 @@ jv_status jv_image_finalize(jv_ctx *c, float *img_pp, float *img_ps, float *img_
  * replicas on several GPUs with a collective. */
 jv_status jv_image_get_device(jv_ctx *c, int kind, double *d_out);
 
+/* Overwrites one stacked accumulator (FP64, gridphy) from host memory
+ * (jv_image_set) or from device memory on the context's device
+ * (jv_image_set_device): loads the sum of the partial images of several
+ * shot replicas (reduced by the caller, e.g. MPI_Allreduce or an NCCL
+ * all-reduce) so that jv_image_finalize runs on the whole stack.  The
+ * reference stacks every shot into one MigImage per process
+ * (RTM/rtm3d_0_image_module/rtm3d_image_meat.hpp:74-96). */
+jv_status jv_image_set(jv_ctx *c, int kind, const double *in);
+jv_status jv_image_set_device(jv_ctx *c, int kind, const double *d_in);
+
 /* Whole reference job: rtm3d_blend_model_mpi_module::mpi_sub_rtm3d
  * (RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:18-135):
  * model every shot and write {output_path}v?_seis_0_{shot}.txt, migrate every
