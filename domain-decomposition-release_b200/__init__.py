@@ -59,7 +59,8 @@ class Grid(C.Structure):
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("rec_width", C.c_int), ("precision", C.c_int), ("store_mode", C.c_int),
                 ("use_graphs", C.c_int), ("graph_steps", C.c_int), ("store_budget", C.c_size_t),
-                ("kernel_variant", C.c_int), ("zchunk", C.c_int)]
+                ("kernel_variant", C.c_int), ("zchunk", C.c_int), ("tile_gx", C.c_int), ("tile_gy", C.c_int),
+                ("min_blocks", C.c_int), ("pml_min_blocks", C.c_int)]
 
 
 class Info(C.Structure):

@@ -117,6 +117,105 @@ Engine::~Engine() {
     if (stream_) cudaStreamDestroy(stream_);
 }
 
+// ------------------------------------------------------------ layout helpers
+
+GridDev make_layout(const jv_grid &grid, size_t *field_elems) {
+    GridDev g{};
+    const int m = grid.pml;
+    g.m = m;
+    g.px = grid.nx; g.py = grid.ny; g.pz = grid.nz;
+    g.nx = grid.nx + 2 * m; g.ny = grid.ny + 2 * m; g.nz = grid.nz + 2 * m;
+    g.xoff = (32 - (m % 32)) % 32;
+    g.sy = round_up(g.xoff + g.nx, 32);
+    g.sz = g.sy * g.ny;
+    g.dx = grid.dx; g.dy = grid.dy; g.dz = grid.dz;
+    *field_elems = (size_t)round_up(g.sz * g.nz + 128, 64);
+    return g;
+}
+
+CpmlDev make_pml_slabs(const GridDev &g, long long *psi_total) {
+    const int NX = g.nx, NY = g.ny, NZ = g.nz, m = g.m;
+    // top, bottom (z); front, back (y, physical z); right, left (x, physical y and z)
+    const int bx[6][6] = {
+        {2, NX - 2, 2, NY - 2, 2, m},           {2, NX - 2, 2, NY - 2, NZ - m, NZ - 2},
+        {2, NX - 2, 2, m, m, NZ - m},           {2, NX - 2, NY - m, NY - 2, m, NZ - m},
+        {2, m, m, NY - m, m, NZ - m},           {NX - m, NX - 2, m, NY - m, m, NZ - m},
+    };
+    const int na[6] = {3, 3, 2, 2, 1, 1};
+    CpmlDev c{};
+    long long off = 0;
+    int blocks = 0;
+    for (int q = 0; q < 6; q++) {
+        PmlSlab S{};
+        S.x0 = bx[q][0]; S.x1 = bx[q][1]; S.y0 = bx[q][2]; S.y1 = bx[q][3]; S.z0 = bx[q][4]; S.z1 = bx[q][5];
+        S.naxes = na[q];
+        if (S.x1 <= S.x0 || S.y1 <= S.y0 || S.z1 <= S.z0) continue;
+        S.gstart = S.x0 - (int)((g.xoff + S.x0) & 3);
+        S.ngroups = (S.x1 - S.gstart + 3) / 4;
+        S.pitch = 4 * S.ngroups;
+        // up to 64 groups of a row per block, as many rows as fit 256 threads
+        const int nb = (S.ngroups + 63) / 64;
+        S.gx = (S.ngroups + nb - 1) / nb;
+        S.gy = 256 / S.gx;
+        S.bx = (S.ngroups + S.gx - 1) / S.gx;
+        S.by = (S.y1 - S.y0 + S.gy - 1) / S.gy;
+        S.first_block = blocks;
+        blocks += S.bx * S.by * (S.z1 - S.z0);
+        S.stride = (long long)S.pitch * (S.y1 - S.y0) * (S.z1 - S.z0);
+        S.psi_off = off;
+        off += 6LL * S.naxes * S.stride;
+        c.s[c.nslab++] = S;
+    }
+    c.nblocks = blocks;
+    *psi_total = off;
+    return c;
+}
+
+void pml_axis_tables(const GridDev &g, float fm, std::vector<float4> t[3]) {
+    // d = vp * K, K = log10(1/R) 7 (s/N)^2 / (2 N delta), R = 0.001
+    const int m = g.m;
+    const double N = (double)(m - kPmlHalf);
+    const double l10x7 = (double)(std::log10(1.0f / 0.001f) * 7.0f);
+    const float alpha_max = (float)(3.14159265358979323846 * (double)fm);
+    const int nax[3] = {g.nx, g.ny, g.nz};
+    const float del[3] = {g.dx, g.dy, g.dz};
+    for (int a = 0; a < 3; a++) {
+        const int n = nax[a];
+        t[a].assign(n, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (int c = 0; c < n; c++) {
+            double sI, sH;
+            if (c >= kPmlHalf && c < m) {  // low side: integer node m-c, half node m-c-1/2
+                sI = m - c;
+                sH = m - c - 0.5;
+            } else if (c >= n - m && c < n - kPmlHalf) {  // high side: the two swap
+                sH = c - (n - m - 1);
+                sI = sH - 0.5;
+            } else {
+                continue;
+            }
+            const double k0 = l10x7 / (2.0 * N * (double)del[a]);
+            const float qI = (float)sI / (float)N, qH = (float)sH / (float)N;
+            t[a][c].x = (float)(k0 * (double)qI * (double)qI);
+            t[a][c].y = (float)(k0 * (double)qH * (double)qH);
+            t[a][c].z = std::max(alpha_max * (1.0f - qI), 0.0f);
+            t[a][c].w = std::max(alpha_max * (1.0f - qH), 0.0f);
+        }
+    }
+}
+
+int upload_all_coefficients() {
+    float list[5][4] = {};
+    for (int o = 1; o <= 4; o++) {
+        double c[4];
+        diff_coeff(o, c);
+        for (int i = 0; i < o; i++) list[o][i] = (float)c[i];
+    }
+    double c2[2];
+    diff_coeff(2, c2);
+    const float dc2[2] = {(float)c2[0], (float)c2[1]};
+    return upload_coefficients(list, dc2);
+}
+
 // ------------------------------------------------------------ creation
 
 Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, const float *rho, float dt, float fm,
@@ -132,6 +231,11 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     int rw = opt.rec_width == 0 ? 1 : opt.rec_width;
     if (rw < 1 || rw > kPhyHalf || rw > grid.pml) return bad(JV_EINVAL, "rec_width must be in 1..4 and <= pml_num");
     if (opt.precision != JV_FP32) return bad(JV_ENOTSUP, "only FP32 wavefield storage is built");
+    if ((opt.min_blocks != 0 && opt.min_blocks != 3 && opt.min_blocks != 4) ||
+        (opt.pml_min_blocks != 0 && opt.pml_min_blocks != 3 && opt.pml_min_blocks != 4))
+        return bad(JV_EINVAL, "min_blocks and pml_min_blocks must be 0, 3 or 4");
+    if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
+        return bad(JV_EINVAL, "tile_gx * tile_gy must be <= 256");
     long long next = (long long)(grid.nx + 2 * grid.pml) * (grid.ny + 2 * grid.pml) * (grid.nz + 2 * grid.pml);
     if (next > (1LL << 34)) return bad(JV_EINVAL, "grid too large");
 
@@ -146,6 +250,10 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     E->dev_ = opt.device;
     E->kc_.variant = opt.kernel_variant;
     E->kc_.zchunk = opt.zchunk;
+    E->kc_.gx = opt.tile_gx;
+    E->kc_.gy = opt.tile_gy;
+    if (opt.min_blocks) E->kc_.minb = opt.min_blocks;
+    if (opt.pml_min_blocks) E->kc_.pml_minb = opt.pml_min_blocks;
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
@@ -164,27 +272,11 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_CU(cudaEventCreate(&ev1_));
 
     // coefficient tables (universal constants; uploaded per device)
-    float list[5][4] = {};
-    for (int o = 1; o <= 4; o++) {
-        double c[4];
-        diff_coeff(o, c);
-        for (int i = 0; i < o; i++) list[o][i] = (float)c[i];
-    }
-    double c2[2];
-    diff_coeff(2, c2);
-    float dc2[2] = {(float)c2[0], (float)c2[1]};
-    JV_K(upload_coefficients(list, dc2));
+    JV_K(upload_all_coefficients());
 
     // pitched gridext layout
     const int m = grid_.pml;
-    g_.m = m;
-    g_.px = grid_.nx; g_.py = grid_.ny; g_.pz = grid_.nz;
-    g_.nx = grid_.nx + 2 * m; g_.ny = grid_.ny + 2 * m; g_.nz = grid_.nz + 2 * m;
-    g_.xoff = (32 - (m % 32)) % 32;
-    g_.sy = round_up(g_.xoff + g_.nx, 32);
-    g_.sz = g_.sy * g_.ny;
-    g_.dx = grid_.dx; g_.dy = grid_.dy; g_.dz = grid_.dz;
-    field_elems_ = (size_t)round_up(g_.sz * g_.nz + 128, 64);
+    g_ = make_layout(grid_, &field_elems_);
     if (field_elems_ >= (size_t)1 << 31) return bad(JV_EINVAL, "gridext too large for 32-bit element offsets");
 
     // model
@@ -210,78 +302,16 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + kGuard + f * field_elems_;
 
     // CPML geometry: six slabs covering gridext outside gridphy and outside
-    // the 2-cell outer rim (FD/fdtd3d_0_base_module/fdtd3d_base_6_pml_meat.hpp:29-94),
-    // processed in 16-byte aligned 4-cell x groups; the slab table and axis
-    // tables are shared by both wavefields, the memory-variable arenas are
-    // per wavefield
+    // the 2-cell outer rim; the slab table and axis tables are shared by
+    // both wavefields, the memory-variable arenas are per wavefield
     {
-        const int NX = g_.nx, NY = g_.ny, NZ = g_.nz;
-        const int bx[6][6] = {
-            {2, NX - 2, 2, NY - 2, 2, m},           {2, NX - 2, 2, NY - 2, NZ - m, NZ - 2},
-            {2, NX - 2, 2, m, m, NZ - m},           {2, NX - 2, NY - m, NY - 2, m, NZ - m},
-            {2, m, m, NY - m, m, NZ - m},           {NX - m, NX - 2, m, NY - m, m, NZ - m},
-        };
-        const int na[6] = {3, 3, 2, 2, 1, 1};
-        long long off = 0;
-        int blocks = 0;
-        cpml_proto_ = CpmlDev{};
-        for (int q = 0; q < 6; q++) {
-            PmlSlab S{};
-            S.x0 = bx[q][0]; S.x1 = bx[q][1]; S.y0 = bx[q][2]; S.y1 = bx[q][3]; S.z0 = bx[q][4]; S.z1 = bx[q][5];
-            S.naxes = na[q];
-            if (S.x1 <= S.x0 || S.y1 <= S.y0 || S.z1 <= S.z0) continue;
-            S.gstart = S.x0 - (int)((g_.xoff + S.x0) & 3);
-            S.ngroups = (S.x1 - S.gstart + 3) / 4;
-            S.pitch = 4 * S.ngroups;
-            S.gx = 1;
-            S.lgx = 0;
-            while (S.gx < S.ngroups && S.gx < 32) {
-                S.gx *= 2;
-                S.lgx++;
-            }
-            S.gy = 256 / S.gx;
-            S.bx = (S.ngroups + S.gx - 1) / S.gx;
-            S.by = (S.y1 - S.y0 + S.gy - 1) / S.gy;
-            S.first_block = blocks;
-            blocks += S.bx * S.by * (S.z1 - S.z0);
-            S.stride = (long long)S.pitch * (S.y1 - S.y0) * (S.z1 - S.z0);
-            S.psi_off = off;
-            off += 6LL * S.naxes * S.stride;
-            cpml_proto_.s[cpml_proto_.nslab++] = S;
-        }
-        cpml_proto_.nblocks = blocks;
-        psi_total_ = off;
-        // per-axis damping factors: d = vp * K, K = log10(1/R) 7 (s/N)^2 / (2 N delta)
-        // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620)
-        const double N = (double)(m - kPmlHalf);
-        const double l10x7 = (double)(std::log10(1.0f / 0.001f) * 7.0f);
-        const float alpha_max = (float)(3.14159265358979323846 * (double)fm_);
-        const int nax[3] = {NX, NY, NZ};
-        const float del[3] = {grid_.dx, grid_.dy, grid_.dz};
+        cpml_proto_ = make_pml_slabs(g_, &psi_total_);
+        std::vector<float4> t[3];
+        pml_axis_tables(g_, fm_, t);
         for (int a = 0; a < 3; a++) {
-            const int n = nax[a];
-            std::vector<float4> t(n, make_float4(0.f, 0.f, 0.f, 0.f));
-            for (int c = 0; c < n; c++) {
-                double sI, sH;
-                if (c >= kPmlHalf && c < m) {
-                    sI = m - c;
-                    sH = m - c - 0.5;
-                } else if (c >= n - m && c < n - kPmlHalf) {
-                    sH = c - (n - m - 1);
-                    sI = sH - 0.5;
-                } else {
-                    continue;
-                }
-                const double k0 = l10x7 / (2.0 * N * (double)del[a]);
-                const float qI = (float)sI / (float)N, qH = (float)sH / (float)N;
-                t[c].x = (float)(k0 * (double)qI * (double)qI);
-                t[c].y = (float)(k0 * (double)qH * (double)qH);
-                t[c].z = std::max(alpha_max * (1.0f - qI), 0.0f);
-                t[c].w = std::max(alpha_max * (1.0f - qH), 0.0f);
-            }
-            JV_TRY(alloc(&p, n * sizeof(float4)));
+            JV_TRY(alloc(&p, t[a].size() * sizeof(float4)));
             axis_d_[a] = (float4 *)p;
-            JV_CU(cudaMemcpy(axis_d_[a], t.data(), n * sizeof(float4), cudaMemcpyHostToDevice));
+            JV_CU(cudaMemcpy(axis_d_[a], t[a].data(), t[a].size() * sizeof(float4), cudaMemcpyHostToDevice));
         }
         JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
         cpF_ = make_cpml((float *)p);
@@ -541,17 +571,17 @@ Status Engine::launch_step(int kind) {
     const int rw = opt_.rec_width;
     switch (kind) {
     case kStepModel:
-        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, s));
+        JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, kc_, s));
         JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
         JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, s));
         JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
-        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, s));
+        JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, kc_, s));
         JV_L("vowr_pack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, 0, nslot_, 1, 0, s));
         JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
         JV_L("step_advance", k_step_advance(st_, +1, s));
@@ -561,13 +591,13 @@ Status Engine::launch_step(int kind) {
         // injection + reverse velocity, stress boundary layers of step it-1
         JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, s));
         JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, kc_, s));
-        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
         JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
         JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, kc_, s));
-        JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, s));
+        JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
         JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 1, s));
         JV_L("step_advance", k_step_advance(st_, -1, s));

@@ -31,6 +31,24 @@ void ricker(int nt, float fm, float dt, float *w);
 // message returned by jv_last_error() on the calling thread
 void set_last_error(const std::string &m);
 
+// Pitched gridext layout of a gridphy + pml problem (elem = base + xoff +
+// i + sy*j + sz*k, first gridphy column 128-byte aligned); *field_elems =
+// floats of one field array (gridext plus tail slack for the aligned
+// x groups of the absorbing-layer kernels).
+GridDev make_layout(const jv_grid &grid, size_t *field_elems);
+// The six CPML slabs (FD/fdtd3d_0_base_module/fdtd3d_base_6_pml_meat.hpp:29-94)
+// with their launch shapes and memory-variable arena offsets; *psi_total =
+// floats of one wavefield's memory-variable arena.  dt, ax and psi are
+// left for the caller.
+CpmlDev make_pml_slabs(const GridDev &g, long long *psi_total);
+// Per-axis damping factor tables {K, K_half, alpha, alpha_half}, K = 0
+// outside the axis' absorbing range
+// (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620).
+void pml_axis_tables(const GridDev &g, float fm, std::vector<float4> t[3]);
+// Uploads the staggered coefficient rows of every order and the 4th-order
+// CPML pair to constant memory of the current device.
+int upload_all_coefficients();
+
 struct Status {
     jv_status code = JV_OK;
     std::string msg;

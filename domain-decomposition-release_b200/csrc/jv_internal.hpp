@@ -44,11 +44,12 @@ struct WaveDev {
 // of row (y,z) at psi_off + ((z-z0)*(y1-y0) + (y-y0))*pitch + 4g; array
 // q = 3*axis + t for the velocity update, 3*naxes + 3*axis + t for the
 // stress update (axis 0 = x, 1 = y, 2 = z).  Launch shape: blocks of
-// 256 threads = gx groups x gy rows (gx = 2^lgx), bx*by blocks per plane.
+// 256 threads, thread t -> group t % gx, row t / gx (gx * gy <= 256),
+// bx*by blocks per plane.
 struct PmlSlab {
     int x0, x1, y0, y1, z0, z1;
     int gstart, ngroups;
-    int gx, gy, lgx, bx, by;
+    int gx, gy, bx, by;
     int first_block;
     int naxes, pitch;
     long long psi_off, stride;
@@ -88,6 +89,9 @@ struct StepState {
 struct KCfg {
     int variant = 2;
     int zchunk = 0;
+    int gx = 0, gy = 0;  // variant 2 block: x groups per block, rows per block (0: auto)
+    int minb = 4;        // variant 2: blocks per SM the register budget is set for (3 or 4)
+    int pml_minb = 4;    // CPML kernels: the same
 };
 
 // kernels.cu ------------------------------------------------------------
@@ -100,9 +104,9 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,
                  int rec_w, const float *wavelet, const StepState *st, const KCfg &kc, void *stream);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
-              void *stream);
+              const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
-                 const float *vp, int with_sau, void *stream);
+                 const float *vp, int with_sau, const KCfg &kc, void *stream);
 
 int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream);
 int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream);

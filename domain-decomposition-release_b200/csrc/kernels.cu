@@ -14,6 +14,8 @@
 //   imaging             RTM/rtm3d_0_image_module/rtm3d_iamge_kernel.hpp:6-51,118-135,184-200
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "jv_internal.hpp"
 
 namespace jv {
@@ -423,7 +425,6 @@ __global__ void __launch_bounds__(kTX *kTY) stress_phy_zm(GridDev g, WaveDev w, 
 // rows/planes, with 32-bit element offsets.  Partial groups at the +x end of
 // gridphy compute all four lanes but store only the cells inside gridphy.
 
-constexpr int kGX = 32, kGY = 8;
 
 __device__ __forceinline__ float4 ld4(const float *__restrict__ f, int i) {
     return __ldg(reinterpret_cast<const float4 *>(f + i));
@@ -508,11 +509,11 @@ __device__ __forceinline__ void st4(float *f, int i0, const float *v, int nvalid
     }
 }
 
-template <int MODE, bool IMG>
-__global__ void __launch_bounds__(kGX *kGY, 3) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ rho,
-                                                         float dt, int rec_w, WaveDev rv, ImageDev img) {
-    const int pi0 = (blockIdx.x * kGX + threadIdx.x) * 4;
-    const int pj = blockIdx.y * kGY + threadIdx.y;
+template <int MODE, bool IMG, int MINB>
+__global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ rho,
+                                                       float dt, int rec_w, WaveDev rv, ImageDev img) {
+    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
     const int pk = blockIdx.z;
     if (pi0 >= g.px || pj >= g.py) return;
     constexpr bool kP = (MODE == kBwd || MODE == kRev);
@@ -621,13 +622,13 @@ __global__ void __launch_bounds__(kGX *kGY, 3) vel_phy_v4(GridDev g, WaveDev w, 
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kGX *kGY, 3) stress_phy_v4(GridDev g, WaveDev w, const float *__restrict__ lam,
-                                                            const float *__restrict__ mu, float dt, int rec_w,
-                                                            const float *__restrict__ wavelet,
-                                                            const StepState *__restrict__ st) {
-    const int pi0 = (blockIdx.x * kGX + threadIdx.x) * 4;
-    const int pj = blockIdx.y * kGY + threadIdx.y;
+template <int MODE, int MINB>
+__global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w, const float *__restrict__ lam,
+                                                          const float *__restrict__ mu, float dt, int rec_w,
+                                                          const float *__restrict__ wavelet,
+                                                          const StepState *__restrict__ st) {
+    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
     const int pk = blockIdx.z;
     if (pi0 >= g.px || pj >= g.py) return;
     const int nvalid = min(4, g.px - pi0);
@@ -814,9 +815,10 @@ __device__ __forceinline__ bool pml_pos(const CpmlDev &P, PmlPos &q) {
     const int t = lb / S.bx;
     const int byi = t % S.by;
     q.z = S.z0 + t / S.by;
-    const int grp = bxi * S.gx + (threadIdx.x & (S.gx - 1));
-    q.y = S.y0 + byi * S.gy + (threadIdx.x >> S.lgx);
-    if (grp >= S.ngroups || q.y >= S.y1) return false;
+    const int tr = (int)threadIdx.x / S.gx;
+    const int grp = bxi * S.gx + ((int)threadIdx.x - tr * S.gx);
+    q.y = S.y0 + byi * S.gy + tr;
+    if (tr >= S.gy || grp >= S.ngroups || q.y >= S.y1) return false;
     q.xs = S.gstart + 4 * grp;
     q.mask = 0;
 #pragma unroll
@@ -843,8 +845,9 @@ __device__ __forceinline__ void xcoef4(const CpmlDev &P, const PmlPos &q, float 
 // CPML velocity update of the six absorbing slabs: 4th order, memory
 // variables on the absorbing axes (z-slabs x,y,z; y-slabs x,y; x-slabs x)
 // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_2_kernel_device_{x,y,z}_meat.hpp)
-__global__ void __launch_bounds__(256, 3) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
-                                               const float *__restrict__ vpm) {
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
+                                                  const float *__restrict__ vpm) {
     PmlPos q;
     if (!pml_pos(P, q)) return;
     const int sy = (int)g.sy, sz = (int)g.sz;
@@ -917,9 +920,10 @@ __global__ void __launch_bounds__(256, 3) vel_pml(GridDev g, CpmlDev P, WaveDev 
     st4m(w.f[VZ], i0, v, q.mask);
 }
 
-template <bool WITH_SAU>
-__global__ void __launch_bounds__(256, 3) stress_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ lam,
-                                                  const float *__restrict__ mu, const float *__restrict__ vpm) {
+template <bool WITH_SAU, int MINB>
+__global__ void __launch_bounds__(256, MINB) stress_pml(GridDev g, CpmlDev P, WaveDev w,
+                                                     const float *__restrict__ lam, const float *__restrict__ mu,
+                                                     const float *__restrict__ vpm) {
     PmlPos q;
     if (!pml_pos(P, q)) return;
     const int sy = (int)g.sy, sz = (int)g.sz;
@@ -1165,24 +1169,66 @@ int k_zero_range(float *p, size_t n, void *stream) {
     return cerr();
 }
 
+// Variant-2 launch shape: blocks of gx x-groups (4 cells each) by gy rows.
+// By default a block spans a whole gridphy row when it has at most 64
+// groups (256 cells), else the row is split evenly, so that no thread is
+// idle beyond the last partial group (200 cells = 50 groups = one block
+// row of 50 x 5); gy fills the block up to 256 threads.
+static void v4_shape(const GridDev &g, const KCfg &kc, dim3 *b, dim3 *gr) {
+    const int ngx = (g.px + 3) / 4;
+    int gx = kc.gx;
+    if (gx <= 0) {
+        const int nb = (ngx + 63) / 64;
+        gx = (ngx + nb - 1) / nb;
+    }
+    gx = std::min(std::max(gx, 1), 256);
+    int gy = kc.gy > 0 ? kc.gy : std::max(1, 256 / gx);
+    gy = std::min(std::max(gy, 1), 256 / gx);
+    *b = dim3(gx, gy);
+    *gr = dim3((ngx + gx - 1) / gx, (g.py + gy - 1) / gy, g.pz);
+}
+
+template <int MINB>
+static int launch_vel_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDev &g, const WaveDev &w,
+                         const float *rho, float dt, int rec_w, const WaveDev *rev, const ImageDev *img,
+                         const WaveDev &rv, const ImageDev &im) {
+    switch (mode) {
+    case kFwd: vel_phy_v4<kFwd, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kRtmFwd: vel_phy_v4<kRtmFwd, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kRev: vel_phy_v4<kRev, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kBwd:
+        if (img && rev) vel_phy_v4<kBwd, true, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        else vel_phy_v4<kBwd, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return cerr();
+}
+
+template <int MINB>
+static int launch_stress_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDev &g, const WaveDev &w,
+                            const float *lam, const float *mu, float dt, int rec_w, const float *wavelet,
+                            const StepState *st) {
+    switch (mode) {
+    case kFwd: stress_phy_v4<kFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kRtmFwd: stress_phy_v4<kRtmFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kBwd: stress_phy_v4<kBwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kRev: stress_phy_v4<kRev, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return cerr();
+}
+
 int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w, const WaveDev *rev,
               const ImageDev *img, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     WaveDev rv = rev ? *rev : WaveDev{};
     ImageDev im = img ? *img : ImageDev{};
     if (kc.variant == 2) {
-        dim3 b(kGX, kGY), gr((g.px + 4 * kGX - 1) / (4 * kGX), (g.py + kGY - 1) / kGY, g.pz);
-        switch (mode) {
-        case kFwd: vel_phy_v4<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-        case kRtmFwd: vel_phy_v4<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-        case kRev: vel_phy_v4<kRev, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-        case kBwd:
-            if (img && rev) vel_phy_v4<kBwd, true><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
-            else vel_phy_v4<kBwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
-            break;
-        default: return (int)cudaErrorInvalidValue;
-        }
-        return cerr();
+        dim3 b, gr;
+        v4_shape(g, kc, &b, &gr);
+        if (kc.minb == 4) return launch_vel_v4<4>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+        return launch_vel_v4<3>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
     }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
@@ -1217,15 +1263,10 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
                  const float *wavelet, const StepState *st, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if (kc.variant == 2) {
-        dim3 b(kGX, kGY), gr((g.px + 4 * kGX - 1) / (4 * kGX), (g.py + kGY - 1) / kGY, g.pz);
-        switch (mode) {
-        case kFwd: stress_phy_v4<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-        case kRtmFwd: stress_phy_v4<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-        case kBwd: stress_phy_v4<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-        case kRev: stress_phy_v4<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-        default: return (int)cudaErrorInvalidValue;
-        }
-        return cerr();
+        dim3 b, gr;
+        v4_shape(g, kc, &b, &gr);
+        if (kc.minb == 4) return launch_stress_v4<4>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st);
+        return launch_stress_v4<3>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st);
     }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
@@ -1250,18 +1291,29 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
     return cerr();
 }
 
-int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp, void *stream) {
+int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
+              const KCfg &kc, void *stream) {
     if (c.nblocks <= 0) return 0;
-    vel_pml<<<(unsigned)c.nblocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, rho, vp);
+    const unsigned blocks = (unsigned)c.nblocks;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (kc.pml_minb == 4) vel_pml<4><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+    else vel_pml<3><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
     return cerr();
 }
 
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
-                 const float *vp, int with_sau, void *stream) {
+                 const float *vp, int with_sau, const KCfg &kc, void *stream) {
     if (c.nblocks <= 0) return 0;
     const unsigned blocks = (unsigned)c.nblocks;
-    if (with_sau) stress_pml<true><<<blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
-    else stress_pml<false><<<blocks, 256, 0, (cudaStream_t)stream>>>(g, c, w, lam, mu, vp);
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool m4 = kc.pml_minb == 4;
+    if (with_sau) {
+        if (m4) stress_pml<true, 4><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        else stress_pml<true, 3><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+    } else {
+        if (m4) stress_pml<false, 4><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        else stress_pml<false, 3><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+    }
     return cerr();
 }
 

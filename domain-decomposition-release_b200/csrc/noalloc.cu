@@ -77,8 +77,6 @@ struct Carver {
     }
 };
 
-long long rup(long long v, long long a) { return (v + a - 1) / a * a; }
-
 }  // namespace
 
 extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, const float *d_vs, const float *d_rho,
@@ -97,58 +95,14 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(JV_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
 
-    // layout: the same pitched gridext layout as the context path
+    // layout and CPML slabs: the same as the context path
     const int m = grid->pml;
-    GridDev g{};
-    g.m = m;
-    g.px = grid->nx; g.py = grid->ny; g.pz = grid->nz;
-    g.nx = g.px + 2 * m; g.ny = g.py + 2 * m; g.nz = g.pz + 2 * m;
-    g.xoff = (32 - (m % 32)) % 32;
-    g.sy = rup(g.xoff + g.nx, 32);
-    g.sz = g.sy * g.ny;
-    g.dx = grid->dx; g.dy = grid->dy; g.dz = grid->dz;
-    const size_t fe = (size_t)rup(g.sz * g.nz + 128, 64);
+    size_t fe = 0;
+    const GridDev g = make_layout(*grid, &fe);
     const size_t guard = 32;
-
-    // CPML slabs (shape as in the context path)
-    CpmlDev cp{};
     long long psi_total = 0;
-    {
-        const int NX = g.nx, NY = g.ny, NZ = g.nz;
-        const int bx[6][6] = {
-            {2, NX - 2, 2, NY - 2, 2, m},           {2, NX - 2, 2, NY - 2, NZ - m, NZ - 2},
-            {2, NX - 2, 2, m, m, NZ - m},           {2, NX - 2, NY - m, NY - 2, m, NZ - m},
-            {2, m, m, NY - m, m, NZ - m},           {NX - m, NX - 2, m, NY - m, m, NZ - m},
-        };
-        const int na[6] = {3, 3, 2, 2, 1, 1};
-        int blocks = 0;
-        for (int q = 0; q < 6; q++) {
-            PmlSlab S{};
-            S.x0 = bx[q][0]; S.x1 = bx[q][1]; S.y0 = bx[q][2]; S.y1 = bx[q][3]; S.z0 = bx[q][4]; S.z1 = bx[q][5];
-            S.naxes = na[q];
-            if (S.x1 <= S.x0 || S.y1 <= S.y0 || S.z1 <= S.z0) continue;
-            S.gstart = S.x0 - (int)((g.xoff + S.x0) & 3);
-            S.ngroups = (S.x1 - S.gstart + 3) / 4;
-            S.pitch = 4 * S.ngroups;
-            S.gx = 1;
-            S.lgx = 0;
-            while (S.gx < S.ngroups && S.gx < 32) {
-                S.gx *= 2;
-                S.lgx++;
-            }
-            S.gy = 256 / S.gx;
-            S.bx = (S.ngroups + S.gx - 1) / S.gx;
-            S.by = (S.y1 - S.y0 + S.gy - 1) / S.gy;
-            S.first_block = blocks;
-            blocks += S.bx * S.by * (S.z1 - S.z0);
-            S.stride = (long long)S.pitch * (S.y1 - S.y0) * (S.z1 - S.z0);
-            S.psi_off = psi_total;
-            psi_total += 6LL * S.naxes * S.stride;
-            cp.s[cp.nslab++] = S;
-        }
-        cp.nblocks = blocks;
-        cp.dt = dt;
-    }
+    CpmlDev cp = make_pml_slabs(g, &psi_total);
+    cp.dt = dt;
 
     // receivers inside gridphy, in input order (as jv_set_geometry keeps them)
     const float rx = (float)(g.px - 1) * g.dx, ry = (float)(g.py - 1) * g.dy, rz = (float)(g.pz - 1) * g.dz;
@@ -184,48 +138,11 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
     if (fe >= ((size_t)1 << 31)) return fail(JV_EINVAL, "grid too large");
 
     // coefficient tables (constant memory, no allocation)
-    float list[5][4] = {};
-    for (int o = 1; o <= 4; o++) {
-        double c[4];
-        diff_coeff(o, c);
-        for (int i = 0; i < o; i++) list[o][i] = (float)c[i];
-    }
-    double c2[2];
-    diff_coeff(2, c2);
-    const float dc2[2] = {(float)c2[0], (float)c2[1]};
-    if (upload_coefficients(list, dc2) != 0) return fail(JV_ECUDA, "coefficient upload failed");
+    if (upload_all_coefficients() != 0) return fail(JV_ECUDA, "coefficient upload failed");
 
     // host-side tables, copied into the scratch array
     std::vector<float4> t[3];
-    {
-        const double N = (double)(m - kPmlHalf);
-        const double l10x7 = (double)(std::log10(1.0f / 0.001f) * 7.0f);
-        const float alpha_max = (float)(3.14159265358979323846 * (double)fm);
-        const int nax[3] = {g.nx, g.ny, g.nz};
-        const float del[3] = {g.dx, g.dy, g.dz};
-        for (int a = 0; a < 3; a++) {
-            const int n = nax[a];
-            t[a].assign(n, make_float4(0.f, 0.f, 0.f, 0.f));
-            for (int c = 0; c < n; c++) {
-                double sI, sH;
-                if (c >= kPmlHalf && c < m) {
-                    sI = m - c;
-                    sH = m - c - 0.5;
-                } else if (c >= n - m && c < n - kPmlHalf) {
-                    sH = c - (n - m - 1);
-                    sI = sH - 0.5;
-                } else {
-                    continue;
-                }
-                const double k0 = l10x7 / (2.0 * N * (double)del[a]);
-                const float qI = (float)sI / (float)N, qH = (float)sH / (float)N;
-                t[a][c].x = (float)(k0 * (double)qI * (double)qI);
-                t[a][c].y = (float)(k0 * (double)qH * (double)qH);
-                t[a][c].z = std::max(alpha_max * (1.0f - qI), 0.0f);
-                t[a][c].w = std::max(alpha_max * (1.0f - qH), 0.0f);
-            }
-        }
-    }
+    pml_axis_tables(g, fm, t);
     std::vector<float> wl(nt);
     ricker(nt, fm, dt, wl.data());
     StepState hs{};
@@ -264,9 +181,9 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
     KCfg kc;
     kc.variant = 2;
     for (int it = 0; it < nt; it++) {
-        NA_CK(k_vel_pml(g, cp, w, rho, vp, s));
+        NA_CK(k_vel_pml(g, cp, w, rho, vp, kc, s));
         NA_CK(k_vel_phy(kFwd, g, w, rho, dt, 1, nullptr, nullptr, kc, s));
-        NA_CK(k_stress_pml(g, cp, w, lam, mu, vp, 0, s));
+        NA_CK(k_stress_pml(g, cp, w, lam, mu, vp, 0, kc, s));
         NA_CK(k_stress_phy(kFwd, g, w, lam, mu, dt, 1, wavelet, state, kc, s));
         NA_CK(k_record(w, rec_d, (int)rec.size(), nt, state, s));
         NA_CK(k_step_advance(state, +1, s));

@@ -77,6 +77,10 @@ typedef struct jv_options {
     size_t store_budget;/* max bytes of HBM for the boundary store (0 -> auto)   */
     int kernel_variant; /* interior kernels: 0 one plane per block, 1 z-marching, 2 x-vectorised (default) */
     int zchunk;         /* z planes per block for variant 1 (0 -> auto)          */
+    int tile_gx;        /* variant 2: 4-cell x groups per block (0 -> auto)      */
+    int tile_gy;        /* variant 2: rows per block (0 -> auto)                 */
+    int min_blocks;     /* interior kernels: register budget for 3 or 4 blocks/SM (0 -> 4) */
+    int pml_min_blocks; /* absorbing-layer kernels: the same (0 -> 4)            */
 } jv_options;
 
 /* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,

@@ -54,6 +54,9 @@ def _create(**kw):
     (dict(nt=0), "nt must be"),
     (dict(rec_width=5), "rec_width"),
     (dict(pml=4, rec_width=4, precision=7), "FP32"),
+    (dict(min_blocks=5), "min_blocks"),
+    (dict(pml_min_blocks=2), "min_blocks"),
+    (dict(tile_gx=200, tile_gy=2), "tile_gx"),
 ])
 def test_invalid_problems_rejected_without_device(kw, msg):
     with pytest.raises(jv.JvError) as e:
