@@ -368,13 +368,27 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
                 segs_h_.push_back(sg);
             }
         per_step_ = off;
-        seg_blocks_ = blk;
+        if (blk >= (1LL << 31) || per_step_ >= (1LL << 31)) return bad(JV_EINVAL, "boundary store too large");
+        nslot_ = nt_ > 1 ? nt_ - 1 : 0;
+        vowr_ = VowrDev{};
+        vowr_.per_step = per_step_;
+        vowr_.nslot = nslot_;
+        vowr_.all_blocks = (int)blk;
+        std::vector<int> blk_seg((size_t)blk);
+        for (size_t q = 0; q < segs_h_.size(); q++) {
+            const SegDev &S = segs_h_[q];
+            const long long nb = ((long long)S.nxb * S.nyb * S.nzb + 255) / 256;
+            for (long long b = 0; b < nb; b++) blk_seg[(size_t)(S.nblk_first + b)] = (int)q;
+            if (S.fld <= VZ) vowr_.vel_blocks = (int)(S.nblk_first + nb);
+        }
         if (!segs_h_.empty()) {
             JV_TRY(alloc(&p, segs_h_.size() * sizeof(SegDev)));
-            segs_d_ = (SegDev *)p;
-            JV_CU(cudaMemcpy(segs_d_, segs_h_.data(), segs_h_.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+            vowr_.segs = (const SegDev *)p;
+            JV_CU(cudaMemcpy(p, segs_h_.data(), segs_h_.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
+            JV_TRY(alloc(&p, blk_seg.size() * sizeof(int)));
+            vowr_.blk_seg = (const int *)p;
+            JV_CU(cudaMemcpy(p, blk_seg.data(), blk_seg.size() * sizeof(int), cudaMemcpyHostToDevice));
         }
-        nslot_ = nt_ > 1 ? nt_ - 1 : 0;
     }
     JV_CU(cudaStreamSynchronize(stream_));
     return Status{};
@@ -522,6 +536,7 @@ Status Engine::check_finite(const char *after) {
     JV_K(k_count_nonfinite(F_.f[0], kNumFld * field_elems_, 0, nf_ + 0, stream_));
     if (R_.f[0]) JV_K(k_count_nonfinite(R_.f[0], kNumFld * field_elems_, 0, nf_ + 1, stream_));
     JV_K(k_count_nonfinite(img_.ip, 5 * nphy, 1, nf_ + 2, stream_));
+    if (shot_img_.ip) JV_K(k_count_nonfinite(shot_img_.ip, 5 * shot_img_pitch_, 0, nf_ + 2, stream_));
     unsigned long long h[8];
     JV_CU(cudaMemcpyAsync(h, nf_, sizeof(h), cudaMemcpyDeviceToHost, stream_));
     JV_CU(cudaStreamSynchronize(stream_));
@@ -564,7 +579,9 @@ Status Engine::check_finite(const char *after) {
         if (check_finite_) JV_TRY(check_finite(name));                      \
     } while (0)
 
-Status Engine::launch_step(int kind) {
+// The kernels of one time step of `kind`.  They read the time step as
+// st_->it + off; advance == true ends the step with st_->it += direction.
+Status Engine::launch_step(int kind, int off, bool advance) {
     cur_kind_ = kind;
     void *s = (void *)stream_;
     const float dt = dt_;
@@ -574,33 +591,33 @@ Status Engine::launch_step(int kind) {
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, kc_, s));
-        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
-        JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, s));
-        JV_L("step_advance", k_step_advance(st_, +1, s));
+        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s));
+        JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, off, s));
+        if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, kc_, s));
-        JV_L("vowr_pack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, 0, nslot_, 1, 0, s));
-        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
-        JV_L("step_advance", k_step_advance(st_, +1, s));
+        JV_L("vowr_pack", k_vowr(g_, F_, vowr_, st_, off, 1, 0, s));
+        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s));
+        if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmRev:
         // UPDATE 1: source subtraction (fused) + backward stress, receiver
         // injection + reverse velocity, stress boundary layers of step it-1
-        JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, s));
-        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, kc_, s));
+        JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, off, s));
+        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, off, kc_, s));
         JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
         JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 2, s));
+        JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
-        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &img_, kc_, s));
+        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
         JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
-        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, kc_, s));
-        JV_L("vowr_unpack", k_vowr(g_, F_, segs_d_, (int)segs_h_.size(), seg_blocks_, per_step_, store_, st_, -1, nslot_, 0, 1, s));
-        JV_L("step_advance", k_step_advance(st_, -1, s));
+        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s));
+        JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 1, s));
+        if (advance) JV_L("step_advance", k_step_advance(st_, -1, s));
         break;
     default: return bad(JV_EINVAL, "unknown step kind");
     }
@@ -611,7 +628,7 @@ Status Engine::run_loop(int kind, int nsteps) {
     if (nsteps <= 0) return Status{};
     if (!opt_.use_graphs || prof_ || check_finite_) {
         for (int i = 0; i < nsteps; i++) {
-            JV_TRY(launch_step(kind));
+            JV_TRY(launch_step(kind, 0, true));
             if (prof_ && prof_pending_.size() > 4096) JV_TRY(prof_collect());
         }
         if (prof_) JV_TRY(prof_collect());
@@ -628,7 +645,14 @@ Status Engine::run_loop(int kind, int nsteps) {
         cudaGraph_t gr;
         JV_CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
         Status st;
-        for (int i = 0; i < steps && st; i++) st = launch_step(kind);
+        // one capture of `steps` time steps: step i reads st_->it + dir*i,
+        // and one advance by dir*steps ends the chunk
+        const int dir = kind == kStepRtmRev ? -1 : +1;
+        for (int i = 0; i < steps && st; i++) st = launch_step(kind, dir * i, false);
+        if (st) {
+            int ek = k_step_advance(st_, dir * steps, stream_);
+            if (ek != 0) st = bad(JV_ECUDA, std::string("step_advance: ") + cudaGetErrorString((cudaError_t)ek));
+        }
         cudaError_t e = cudaStreamEndCapture(stream_, &gr);
         if (!st) {
             if (e == cudaSuccess) cudaGraphDestroy(gr);
@@ -690,6 +714,17 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
         cpR_ = make_cpml((float *)p);
     }
+    if (!shot_img_.ip) {
+        // five arrays at a pitch of whole 256-byte lines, so that every
+        // array starts 16-byte aligned (the image update uses float4 access)
+        void *p;
+        const size_t pitch = (size_t)round_up((long long)g_.px * g_.py * g_.pz, 64);
+        JV_TRY(alloc(&p, 5 * pitch * sizeof(float)));
+        float *b = (float *)p;
+        shot_img_.ip = b; shot_img_.pp = b + pitch; shot_img_.ps = b + 2 * pitch; shot_img_.sp = b + 3 * pitch;
+        shot_img_.ss = b + 4 * pitch;
+        shot_img_pitch_ = pitch;
+    }
     if (!store_ && per_step_ > 0 && nslot_ > 0) {
         size_t bytes = (size_t)per_step_ * nslot_ * sizeof(float);
         size_t freeb = 0, totalb = 0;
@@ -701,6 +736,7 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         void *p;
         JV_TRY(alloc(&p, bytes));
         store_ = (float *)p;
+        vowr_.store = store_;
     }
     const float *obs[3] = {d_ox, d_oy, d_oz};
     JV_CU(cudaEventRecord(ev0_, stream_));
@@ -713,7 +749,9 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
     JV_TRY(zero_wave(R_, kNumFld));
     JV_TRY(zero_psi(cpR_));
     JV_TRY(set_state(nt_ - 1, src, nullptr, obs));
+    JV_CU(cudaMemsetAsync(shot_img_.ip, 0, 5 * shot_img_pitch_ * sizeof(float), stream_));
     JV_TRY(run_loop(kStepRtmRev, nt_));
+    JV_K(k_image_stack(g_, shot_img_, img_, stream_));
     JV_CU(cudaEventRecord(ev1_, stream_));
     JV_CU(cudaEventSynchronize(ev1_));
     JV_CU(cudaGetLastError());

@@ -89,7 +89,7 @@ class Engine {
     Status alloc_all(const float *vp, const float *vs, const float *rho);
     Status check_shot(int shot, long long *src) const;
     Status run_loop(int kind, int nsteps);
-    Status launch_step(int kind);
+    Status launch_step(int kind, int off, bool advance);
     Status cu(cudaError_t e, const char *what) const;
     Status zero_wave(const WaveDev &w, int nfld);
     Status zero_psi(const CpmlDev &c);
@@ -129,13 +129,14 @@ class Engine {
 
     // VOWR store
     std::vector<SegDev> segs_h_;
-    SegDev *segs_d_ = nullptr;
-    long long seg_blocks_ = 0;
+    VowrDev vowr_{};
     long long per_step_ = 0;
     float *store_ = nullptr;
     int nslot_ = 0;
 
-    ImageDev img_{};
+    StackDev img_{};             // FP64 stacks over shots
+    ImageDev shot_img_{};        // FP32 image of the shot being migrated
+    size_t shot_img_pitch_ = 0;  // floats between its five arrays
     float *fin_ = nullptr;  // 8 * n_phy finalize buffer
 
     // graphs: key = kind * 100000 + steps

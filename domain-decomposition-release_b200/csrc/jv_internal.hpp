@@ -63,8 +63,18 @@ struct CpmlDev {
     float *psi;               // this wavefield's memory-variable arena
 };
 
+// The image of the shot being migrated: FP32 accumulators over its time
+// steps, as the reference keeps them (RTM/rtm3d_0_image_module/
+// rtm3d_iamge_kernel.hpp:6-51, RTM = src/jarvis_cpp/jarvis/.jarvis_2_app/
+// .jarvis_3_seismology/elastic_1_rtm3d_model_mpi); added into the FP64
+// stacks at the end of the shot.
 struct ImageDev {
-    double *ip, *pp, *ps, *sp, *ss;  // gridphy, dense x-fastest
+    float *ip, *pp, *ps, *sp, *ss;  // gridphy, dense x-fastest
+};
+
+// The stacks over shots (FP64), gridphy, dense x-fastest.
+struct StackDev {
+    double *ip, *pp, *ps, *sp, *ss;
 };
 
 struct SegDev {          // one VOWR face box
@@ -72,6 +82,18 @@ struct SegDev {          // one VOWR face box
     int x0, nxb, y0, nyb, z0, nzb;
     long long off;       // offset in the packed per-step record
     long long nblk_first;
+};
+
+// The VOWR boundary store and its face boxes.  Boxes of the velocity
+// fields come first; each box is cut into blocks of 256 cells and
+// blk_seg maps a block to its box.
+struct VowrDev {
+    const SegDev *segs;
+    const int *blk_seg;
+    int vel_blocks, all_blocks;
+    long long per_step;  // floats of one step's record
+    int nslot;           // records in the store
+    float *store;
 };
 
 // Per-step state in device memory, read by the kernels of a captured
@@ -101,19 +123,27 @@ int k_zero_range(float *p, size_t n, void *stream);
 
 int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w,
               const WaveDev *rev, const ImageDev *img, const KCfg &kc, void *stream);
+// it_off: the kernels of a step read the time step as st->it + it_off (a
+// captured chunk of steps advances st->it once, at its end)
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,
-                 int rec_w, const float *wavelet, const StepState *st, const KCfg &kc, void *stream);
+                 int rec_w, const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
               const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
                  const float *vp, int with_sau, const KCfg &kc, void *stream);
 
-int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream);
-int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream);
-int k_vowr(const GridDev &g, const WaveDev &w, const SegDev *segs, int nseg, long long nblk, long long per_step,
-           float *store, const StepState *st, int slot_shift, int nslot, int pack, int which, void *stream);
+int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, int it_off,
+             void *stream);
+int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, int it_off,
+                 void *stream);
+// pack (1) or unpack (0) record st->it + slot_shift; which: 0 all fields,
+// 1 the velocity fields, 2 the stress fields
+int k_vowr(const GridDev &g, const WaveDev &w, const VowrDev &v, const StepState *st, int slot_shift, int pack,
+           int which, void *stream);
 int k_step_advance(StepState *st, int delta, void *stream);
-int k_image_finalize(const GridDev &g, const ImageDev &img, float *out /* 8 arrays */, void *stream);
+int k_image_finalize(const GridDev &g, const StackDev &img, float *out /* 8 arrays */, void *stream);
+// stack += shot image (FP64 sums of the FP32 shot accumulators)
+int k_image_stack(const GridDev &g, const ImageDev &shot, const StackDev &stack, void *stream);
 int upload_coefficients(const float list[5][4], const float dc2[2]);
 int k_count_nonfinite(const void *p, size_t n, int is_double, unsigned long long *out, void *stream);
 

@@ -139,11 +139,11 @@ __global__ void __launch_bounds__(kTX *kTY) vel_phy(GridDev g, WaveDev w, const 
             const float rsx = ld(rv.f[VX], i) - rpx, rsy = ld(rv.f[VY], i) - rpy, rsz = ld(rv.f[VZ], i) - rpz;
             const float ssx = vx - px, ssy = vy - py, ssz = vz - pz;
             const long long o = pi + (long long)g.px * (pj + (long long)g.py * pk);
-            img.ip[o] += (double)(px * px + py * py + pz * pz);
-            img.pp[o] += (double)(px * rpx + py * rpy + pz * rpz);
-            img.ps[o] += (double)(px * rsx + py * rsy + pz * rsz);
-            img.sp[o] += (double)(ssx * rpx + ssy * rpy + ssz * rpz);
-            img.ss[o] += (double)(ssx * rsx + ssy * rsy + ssz * rsz);
+            img.ip[o] += px * px + py * py + pz * pz;
+            img.pp[o] += px * rpx + py * rpy + pz * rpz;
+            img.ps[o] += px * rsx + py * rsy + pz * rsz;
+            img.sp[o] += ssx * rpx + ssy * rpy + ssz * rpz;
+            img.ss[o] += ssx * rsx + ssy * rsy + ssz * rsz;
         }
     }
 }
@@ -152,7 +152,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kTX *kTY) stress_phy(GridDev g, WaveDev w, const float *__restrict__ lam,
                                                       const float *__restrict__ mu, float dt, int rec_w,
                                                       const float *__restrict__ wavelet,
-                                                      const StepState *__restrict__ st) {
+                                                      const StepState *__restrict__ st, int it_off) {
     const int pi = blockIdx.x * kTX + threadIdx.x;
     const int pj = blockIdx.y * kTY + threadIdx.y;
     const int pk = blockIdx.z;
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(kTX *kTY) stress_phy(GridDev g, WaveDev w, con
     if (MODE != kRev && i == st->src) {
         // explosive source, applied before the stress update of step it
         // (FD/fdtd3d_2_phy_mpi_module/fdtd3d_phy_mpi_3_stress_kernel.hpp:1308-1364)
-        const float s = wavelet[st->it];
+        const float s = wavelet[st->it + it_off];
         if (MODE == kBwd) {
             sxx -= s; syy -= s; szz -= s;
         } else {
@@ -316,11 +316,11 @@ __global__ void __launch_bounds__(kTX *kTY) vel_phy_zm(GridDev g, WaveDev w, con
                 const float rsx = ld(rv.f[VX], i) - rpx, rsy = ld(rv.f[VY], i) - rpy, rsz = ld(rv.f[VZ], i) - rpz;
                 const float ssx = vx - px, ssy = vy - py, ssz = vz - pz;
                 const long long q = pi + (long long)g.px * (pj + (long long)g.py * k);
-                img.ip[q] += (double)(px * px + py * py + pz * pz);
-                img.pp[q] += (double)(px * rpx + py * rpy + pz * rpz);
-                img.ps[q] += (double)(px * rsx + py * rsy + pz * rsz);
-                img.sp[q] += (double)(ssx * rpx + ssy * rpy + ssz * rpz);
-                img.ss[q] += (double)(ssx * rsx + ssy * rsy + ssz * rsz);
+                img.ip[q] += px * px + py * py + pz * pz;
+                img.pp[q] += px * rpx + py * rpy + pz * rpz;
+                img.ps[q] += px * rsx + py * rsy + pz * rsz;
+                img.sp[q] += ssx * rpx + ssy * rpy + ssz * rpz;
+                img.ss[q] += ssx * rsx + ssy * rsy + ssz * rsz;
             }
         }
 #pragma unroll
@@ -337,7 +337,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kTX *kTY) stress_phy_zm(GridDev g, WaveDev w, const float *__restrict__ lam,
                                                          const float *__restrict__ mu, float dt, int rec_w,
                                                          const float *__restrict__ wavelet,
-                                                         const StepState *__restrict__ st, int zc) {
+                                                         const StepState *__restrict__ st, int zc, int it_off) {
     const int pi = blockIdx.x * kTX + threadIdx.x;
     const int pj = blockIdx.y * kTY + threadIdx.y;
     const int k0 = blockIdx.z * zc;
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(kTX *kTY) stress_phy_zm(GridDev g, WaveDev w, 
         const float l2m = l + 2.0f * m;
         float sxx = w.f[SXX][i], syy = w.f[SYY][i], szz = w.f[SZZ][i];
         if (MODE != kRev && i == src) {
-            const float s = wavelet[st->it];
+            const float s = wavelet[st->it + it_off];
             if (MODE == kBwd) {
                 sxx -= s; syy -= s; szz -= s;
             } else {
@@ -606,17 +606,35 @@ __global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, co
             f4a(rpy, ld4(rv.f[VYP], i0));
             f4a(rpz, ld4(rv.f[VZP], i0));
             const long long o0 = pi0 + (long long)g.px * (pj + (long long)g.py * pk);
+            float a[5][4];
 #pragma unroll
             for (int c = 0; c < 4; c++) {
-                if (c >= nvalid) break;
                 const float rsx = rvx[c] - rpx[c], rsy = rvy[c] - rpy[c], rsz = rvz[c] - rpz[c];
                 const float ssx = vx[c] - px[c], ssy = vy[c] - py[c], ssz = vz[c] - pz[c];
-                const long long o = o0 + c;
-                img.ip[o] += (double)(px[c] * px[c] + py[c] * py[c] + pz[c] * pz[c]);
-                img.pp[o] += (double)(px[c] * rpx[c] + py[c] * rpy[c] + pz[c] * rpz[c]);
-                img.ps[o] += (double)(px[c] * rsx + py[c] * rsy + pz[c] * rsz);
-                img.sp[o] += (double)(ssx * rpx[c] + ssy * rpy[c] + ssz * rpz[c]);
-                img.ss[o] += (double)(ssx * rsx + ssy * rsy + ssz * rsz);
+                a[0][c] = px[c] * px[c] + py[c] * py[c] + pz[c] * pz[c];
+                a[1][c] = px[c] * rpx[c] + py[c] * rpy[c] + pz[c] * rpz[c];
+                a[2][c] = px[c] * rsx + py[c] * rsy + pz[c] * rsz;
+                a[3][c] = ssx * rpx[c] + ssy * rpy[c] + ssz * rpz[c];
+                a[4][c] = ssx * rsx + ssy * rsy + ssz * rsz;
+            }
+            float *dst[5] = {img.ip, img.pp, img.ps, img.sp, img.ss};
+            bool al = nvalid == 4;
+#pragma unroll
+            for (int q = 0; q < 5; q++) al = al && ((reinterpret_cast<uintptr_t>(dst[q] + o0) & 15) == 0);
+            if (al) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) {
+                    float4 *p4 = reinterpret_cast<float4 *>(dst[q] + o0);
+                    float4 v = *p4;
+                    v.x += a[q][0]; v.y += a[q][1]; v.z += a[q][2]; v.w += a[q][3];
+                    *p4 = v;
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; q++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        if (c < nvalid) dst[q][o0 + c] += a[q][c];
             }
         }
     }
@@ -626,7 +644,7 @@ template <int MODE, int MINB>
 __global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w, const float *__restrict__ lam,
                                                           const float *__restrict__ mu, float dt, int rec_w,
                                                           const float *__restrict__ wavelet,
-                                                          const StepState *__restrict__ st) {
+                                                          const StepState *__restrict__ st, int it_off) {
     const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int pj = blockIdx.y * blockDim.y + threadIdx.y;
     const int pk = blockIdx.z;
@@ -684,7 +702,8 @@ __global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w,
         const long long src = st->src;
         const long long d = src - (long long)i0;
         if (d >= 0 && d < nvalid) {
-            const float sv = (MODE == kBwd) ? -wavelet[st->it] : wavelet[st->it];
+            const float w0 = wavelet[st->it + it_off];
+            const float sv = (MODE == kBwd) ? -w0 : w0;
 #pragma unroll
             for (int c = 0; c < 4; c++)
                 if (c == (int)d) {
@@ -1019,10 +1038,10 @@ __global__ void __launch_bounds__(256, MINB) stress_pml(GridDev g, CpmlDev P, Wa
 // ------------------------------------------------------------ receivers
 
 __global__ void record(WaveDev w, const long long *__restrict__ rec, int nrec, int nt,
-                       const StepState *__restrict__ st) {
+                       const StepState *__restrict__ st, int it_off) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrec) return;
-    const int it = st->it;
+    const int it = st->it + it_off;
     float *tx = st->tr[0], *ty = st->tr[1], *tz = st->tr[2];
     const long long i = rec[r];
     const long long o = (long long)r * nt + it;
@@ -1032,10 +1051,10 @@ __global__ void record(WaveDev w, const long long *__restrict__ rec, int nrec, i
 }
 
 __global__ void inject_rec(WaveDev w, const long long *__restrict__ rec, int nrec, int nt,
-                           const StepState *__restrict__ st) {
+                           const StepState *__restrict__ st, int it_off) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrec) return;
-    const int it = st->it;
+    const int it = st->it + it_off;
     const float *tx = st->obs[0], *ty = st->obs[1], *tz = st->obs[2];
     const long long i = rec[r];
     const long long o = (long long)r * nt + it;
@@ -1049,26 +1068,22 @@ __global__ void inject_rec(WaveDev w, const long long *__restrict__ rec, int nre
 // One block per 256 elements of one face box; the block finds its box by
 // the prefix of block counts.  pack: field -> store[slot]; else the
 // reverse.  which: 0 all fields, 1 velocities only, 2 stresses only.
-__global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, const SegDev *__restrict__ segs, int nseg,
-                                            long long per_step, float *store, const StepState *__restrict__ st,
-                                            int slot_shift, int nslot, int pack, int which) {
+// blocks [b0, b0 + gridDim.x) of the face boxes; one cell per thread
+__global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, VowrDev v, const StepState *__restrict__ st,
+                                            int slot_shift, int pack, int b0) {
     const int slot = st->it + slot_shift;
-    if (slot < 0 || slot >= nslot) return;
-    const long long b = blockIdx.x;
-    int s = 0;
-    while (s + 1 < nseg && segs[s + 1].nblk_first <= b) s++;
-    const SegDev S = segs[s];
-    const bool isvel = S.fld <= VZ;
-    if ((which == 1 && !isvel) || (which == 2 && isvel)) return;
-    const long long e = (b - S.nblk_first) * 256 + threadIdx.x;
-    const long long cnt = (long long)S.nxb * S.nyb * S.nzb;
+    if (slot < 0 || slot >= v.nslot) return;
+    const int b = b0 + (int)blockIdx.x;
+    const SegDev &S = v.segs[v.blk_seg[b]];
+    const int e = (b - (int)S.nblk_first) * 256 + (int)threadIdx.x;
+    const int cnt = S.nxb * S.nyb * S.nzb;
     if (e >= cnt) return;
-    const int x = S.x0 + (int)(e % S.nxb);
-    const long long t = e / S.nxb;
-    const int y = S.y0 + (int)(t % S.nyb);
-    const int z = S.z0 + (int)(t / S.nyb);
-    const long long i = g.xoff + x + g.sy * y + g.sz * z;
-    float *rec = store + (long long)slot * per_step + S.off + e;
+    const int t = e / S.nxb;
+    const int x = S.x0 + (e - t * S.nxb);
+    const int z = t / S.nyb;
+    const int y = S.y0 + (t - z * S.nyb);
+    const int i = (int)g.xoff + x + (int)g.sy * y + (int)g.sz * (S.z0 + z);
+    float *rec = v.store + (long long)slot * v.per_step + S.off + e;
     if (pack) *rec = w.f[S.fld][i];
     else w.f[S.fld][i] = *rec;
 }
@@ -1122,7 +1137,16 @@ __global__ void zero_range(float *p, size_t n) {
 
 // out: 8 float arrays of gridphy: compensated pp, ps, sp, ss, then the
 // Laplacians of the uncompensated images (cells 2..n-3, zero elsewhere).
-__global__ void image_finalize(GridDev g, ImageDev img, float *out) {
+__global__ void image_stack(long long n, ImageDev shot, StackDev st) {
+    const float *src[5] = {shot.ip, shot.pp, shot.ps, shot.sp, shot.ss};
+    double *dst[5] = {st.ip, st.pp, st.ps, st.sp, st.ss};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) dst[q][i] += (double)src[q][i];
+    }
+}
+
+__global__ void image_finalize(GridDev g, StackDev img, float *out) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y, z = blockIdx.z;
     if (x >= g.px) return;
@@ -1208,12 +1232,12 @@ static int launch_vel_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDe
 template <int MINB>
 static int launch_stress_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDev &g, const WaveDev &w,
                             const float *lam, const float *mu, float dt, int rec_w, const float *wavelet,
-                            const StepState *st) {
+                            const StepState *st, int it_off) {
     switch (mode) {
-    case kFwd: stress_phy_v4<kFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-    case kRtmFwd: stress_phy_v4<kRtmFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-    case kBwd: stress_phy_v4<kBwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-    case kRev: stress_phy_v4<kRev, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kFwd: stress_phy_v4<kFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kRtmFwd: stress_phy_v4<kRtmFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kBwd: stress_phy_v4<kBwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kRev: stress_phy_v4<kRev, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
     default: return (int)cudaErrorInvalidValue;
     }
     return cerr();
@@ -1260,32 +1284,33 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 }
 
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt, int rec_w,
-                 const float *wavelet, const StepState *st, const KCfg &kc, void *stream) {
+                 const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     if (kc.variant == 2) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
-        if (kc.minb == 4) return launch_stress_v4<4>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st);
-        return launch_stress_v4<3>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st);
+        if (kc.minb == 4)
+            return launch_stress_v4<4>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
+        return launch_stress_v4<3>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
     }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
         dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, (g.pz + zc - 1) / zc);
         switch (mode) {
-        case kFwd: stress_phy_zm<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
-        case kRtmFwd: stress_phy_zm<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
-        case kBwd: stress_phy_zm<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
-        case kRev: stress_phy_zm<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc); break;
+        case kFwd: stress_phy_zm<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc, it_off); break;
+        case kRtmFwd: stress_phy_zm<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc, it_off); break;
+        case kBwd: stress_phy_zm<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc, it_off); break;
+        case kRev: stress_phy_zm<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, zc, it_off); break;
         default: return (int)cudaErrorInvalidValue;
         }
         return cerr();
     }
     dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
     switch (mode) {
-    case kFwd: stress_phy<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-    case kRtmFwd: stress_phy<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-    case kBwd: stress_phy<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
-    case kRev: stress_phy<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st); break;
+    case kFwd: stress_phy<kFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kRtmFwd: stress_phy<kRtmFwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kBwd: stress_phy<kBwd><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kRev: stress_phy<kRev><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
     default: return (int)cudaErrorInvalidValue;
     }
     return cerr();
@@ -1317,23 +1342,26 @@ int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const flo
     return cerr();
 }
 
-int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream) {
+int k_record(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, int it_off,
+             void *stream) {
     if (nrec <= 0) return 0;
-    record<<<(nrec + 127) / 128, 128, 0, (cudaStream_t)stream>>>(w, rec, nrec, nt, st);
+    record<<<(nrec + 127) / 128, 128, 0, (cudaStream_t)stream>>>(w, rec, nrec, nt, st, it_off);
     return cerr();
 }
 
-int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, void *stream) {
+int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const StepState *st, int it_off,
+                 void *stream) {
     if (nrec <= 0) return 0;
-    inject_rec<<<(nrec + 127) / 128, 128, 0, (cudaStream_t)stream>>>(w, rec, nrec, nt, st);
+    inject_rec<<<(nrec + 127) / 128, 128, 0, (cudaStream_t)stream>>>(w, rec, nrec, nt, st, it_off);
     return cerr();
 }
 
-int k_vowr(const GridDev &g, const WaveDev &w, const SegDev *segs, int nseg, long long nblk, long long per_step,
-           float *store, const StepState *st, int slot_shift, int nslot, int pack, int which, void *stream) {
-    if (nseg <= 0 || nblk <= 0) return 0;
-    vowr<<<(unsigned)nblk, 256, 0, (cudaStream_t)stream>>>(g, w, segs, nseg, per_step, store, st, slot_shift, nslot,
-                                                            pack, which);
+int k_vowr(const GridDev &g, const WaveDev &w, const VowrDev &v, const StepState *st, int slot_shift, int pack,
+           int which, void *stream) {
+    const int b0 = which == 2 ? v.vel_blocks : 0;
+    const int b1 = which == 1 ? v.vel_blocks : v.all_blocks;
+    if (b1 <= b0) return 0;
+    vowr<<<(unsigned)(b1 - b0), 256, 0, (cudaStream_t)stream>>>(g, w, v, st, slot_shift, pack, b0);
     return cerr();
 }
 
@@ -1349,7 +1377,13 @@ int k_count_nonfinite(const void *p, size_t n, int is_double, unsigned long long
     return cerr();
 }
 
-int k_image_finalize(const GridDev &g, const ImageDev &img, float *out, void *stream) {
+int k_image_stack(const GridDev &g, const ImageDev &shot, const StackDev &stack, void *stream) {
+    const long long n = (long long)g.px * g.py * g.pz;
+    image_stack<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(n, shot, stack);
+    return cerr();
+}
+
+int k_image_finalize(const GridDev &g, const StackDev &img, float *out, void *stream) {
     dim3 b(128), gr((g.px + 127) / 128, g.py, g.pz);
     image_finalize<<<gr, b, 0, (cudaStream_t)stream>>>(g, img, out);
     return cerr();

@@ -184,8 +184,8 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
         NA_CK(k_vel_pml(g, cp, w, rho, vp, kc, s));
         NA_CK(k_vel_phy(kFwd, g, w, rho, dt, 1, nullptr, nullptr, kc, s));
         NA_CK(k_stress_pml(g, cp, w, lam, mu, vp, 0, kc, s));
-        NA_CK(k_stress_phy(kFwd, g, w, lam, mu, dt, 1, wavelet, state, kc, s));
-        NA_CK(k_record(w, rec_d, (int)rec.size(), nt, state, s));
+        NA_CK(k_stress_phy(kFwd, g, w, lam, mu, dt, 1, wavelet, state, 0, kc, s));
+        NA_CK(k_record(w, rec_d, (int)rec.size(), nt, state, 0, s));
         NA_CK(k_step_advance(state, +1, s));
     }
     NA_CK(cudaStreamSynchronize(s));
