@@ -41,8 +41,10 @@ EXPORTS = (
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
     "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
     "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info", "jv_forward_noalloc",
-    "jv_image_set", "jv_image_set_device",
+    "jv_image_set", "jv_image_set_device", "jv_run_project_shard", "jv_read_argfile",
 )
+
+REDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_size_t, C.c_void_p)
 
 
 class JvError(RuntimeError):
@@ -61,6 +63,25 @@ class Options(C.Structure):
                 ("use_graphs", C.c_int), ("graph_steps", C.c_int), ("store_budget", C.c_size_t),
                 ("kernel_variant", C.c_int), ("zchunk", C.c_int), ("tile_gx", C.c_int), ("tile_gy", C.c_int),
                 ("min_blocks", C.c_int), ("pml_min_blocks", C.c_int)]
+
+
+class ArgFileC(C.Structure):
+    _fields_ = [("model_path", C.c_char * 1024), ("shot_path", C.c_char * 1024), ("rece_path", C.c_char * 1024),
+                ("output_path", C.c_char * 1024), ("is_output", C.c_int), ("t_snap", C.c_int), ("pml_num", C.c_int),
+                ("fm", C.c_float), ("dt", C.c_float), ("T", C.c_float), ("x_divide_num", C.c_int),
+                ("y_divide_num", C.c_int), ("z_divide_num", C.c_int), ("slots_per_node", C.c_int),
+                ("rec_width", C.c_int)]
+
+
+def read_argfile(proj_path: str) -> dict:
+    """The project's argfile as libjv reads it (jv_read_argfile)."""
+    a = ArgFileC()
+    _check(lib().jv_read_argfile(proj_path.encode(), C.byref(a)))
+    out = {}
+    for name, _ in ArgFileC._fields_:
+        v = getattr(a, name)
+        out[name] = v.decode() if isinstance(v, bytes) else v
+    return out
 
 
 class Info(C.Structure):
@@ -110,6 +131,8 @@ def lib() -> C.CDLL:
     L.jv_set_profiling.argtypes = [ctxp, C.c_int]
     L.jv_profile_entry.argtypes = [ctxp, C.c_int, C.POINTER(C.c_char_p), dp, C.POINTER(C.c_longlong)]
     L.jv_run_project.argtypes = [ctxp]
+    L.jv_run_project_shard.argtypes = [ctxp, C.c_int, C.c_int, REDUCE_FN, C.c_void_p]
+    L.jv_read_argfile.argtypes = [C.c_char_p, C.POINTER(ArgFileC)]
     L.jv_forward_noalloc.argtypes = [C.POINTER(Grid), vp, vp, vp, C.c_float, C.c_float, C.c_int, fp, C.c_int, fp,
                                      vp, vp, vp, C.POINTER(C.c_int), vp]
     L.jv_last_timing.argtypes = [ctxp, dp]
@@ -271,6 +294,21 @@ class Context:
 
     def run_project(self) -> None:
         _check(lib().jv_run_project(self._h))
+
+    def run_project_shard(self, rank: int, world: int, reduce=None) -> None:
+        """jv_run_project_shard; `reduce(arr)` sums a float64 numpy array in
+        place over the job's ranks."""
+        if reduce is None:
+            cb = C.cast(None, REDUCE_FN)
+        else:
+            def _cb(ptr, n, _user):
+                try:
+                    reduce(np.ctypeslib.as_array(ptr, shape=(n,)))
+                    return 0
+                except Exception:  # reported to the library as a failed reduce
+                    return 1
+            cb = REDUCE_FN(_cb)
+        _check(lib().jv_run_project_shard(self._h, rank, world, cb, None))
 
     def sync(self) -> None:
         _check(lib().jv_sync(self._h))

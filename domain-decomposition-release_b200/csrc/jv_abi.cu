@@ -131,6 +131,33 @@ jv_status jv_open(const char *proj_path, const jv_options *opt, jv_ctx **out) {
     return JV_OK;
 }
 
+jv_status jv_read_argfile(const char *proj_path, jv_argfile *out) {
+    if (!proj_path || !out) return fail(JV_EINVAL, "jv_read_argfile: NULL argument");
+    jv::ArgFile a;
+    std::string m = jv::read_argfile(proj_path, &a);
+    if (!m.empty()) return fail(JV_EIO, m);
+    std::memset(out, 0, sizeof(*out));
+    const std::string *src[4] = {&a.model_path, &a.shot_path, &a.recv_path, &a.output_path};
+    char *dst[4] = {out->model_path, out->shot_path, out->rece_path, out->output_path};
+    for (int q = 0; q < 4; q++) {
+        if (src[q]->size() >= sizeof(out->model_path)) return fail(JV_EINVAL, "path too long: " + *src[q]);
+        std::memcpy(dst[q], src[q]->c_str(), src[q]->size() + 1);
+    }
+    out->is_output = a.is_output ? 1 : 0;
+    out->t_snap = a.t_snap;
+    out->pml_num = a.pml_num;
+    out->fm = a.fm;
+    out->dt = a.dt;
+    out->T = a.T;
+    out->x_divide_num = a.x_divide_num;
+    out->y_divide_num = a.y_divide_num;
+    out->z_divide_num = a.z_divide_num;
+    out->slots_per_node = a.slots_per_node;
+    out->rec_width = a.rec_width;
+    g_err.clear();
+    return JV_OK;
+}
+
 jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz) {
     if (!c) return fail(JV_EINVAL, "NULL context");
     jv::Status s = c->eng->set_geometry(n_shot, shot_xyz, n_recv, recv_xyz);
@@ -236,17 +263,25 @@ jv_status jv_profile_entry(const jv_ctx *c, int idx, const char **name, double *
     return JV_OK;
 }
 
-jv_status jv_run_project(jv_ctx *c) {
+jv_status jv_run_project(jv_ctx *c) { return jv_run_project_shard(c, 0, 1, nullptr, nullptr); }
+
+jv_status jv_run_project_shard(jv_ctx *c, int rank, int world, jv_reduce_fn reduce, void *user) {
     if (!c) return fail(JV_EINVAL, "NULL context");
     if (!c->from_project) return fail(JV_ESTATE, "jv_run_project needs a context made by jv_open");
+    if (world < 1 || rank < 0 || rank >= world) return fail(JV_EINVAL, "rank must be in [0, world)");
+    if (world > 1 && !reduce) return fail(JV_EINVAL, "a job of several ranks needs a reduce function");
     jv_info inf;
     c->eng->info(&inf);
     const int nshot = inf.n_shot, nrec = inf.n_recv, nt = inf.nt;
     const size_t per = (size_t)nrec * nt;
-    // phase 1: model every shot, keep its traces (mpi_sub_rtm3d :20-38)
-    std::vector<float> all((size_t)nshot * 3 * per);
-    for (int s = 0; s < nshot; s++) {
-        float *t = all.data() + (size_t)s * 3 * per;
+    // this rank's shots: s % world == rank (every shot exactly once over the job)
+    std::vector<int> mine;
+    for (int s = rank; s < nshot; s += world) mine.push_back(s);
+    // phase 1: model the shots, keep their traces (mpi_sub_rtm3d :20-38)
+    std::vector<float> all(mine.size() * 3 * per);
+    for (size_t q0 = 0; q0 < mine.size(); q0++) {
+        const int s = mine[q0];
+        float *t = all.data() + q0 * 3 * per;
         jv_status st = jv_forward(c, s, t, t + per, t + 2 * per);
         if (st != JV_OK) return st;
         if (nrec > 0) {
@@ -257,16 +292,29 @@ jv_status jv_run_project(jv_ctx *c) {
             }
         }
     }
-    // phase 2: migrate every shot into one image (:45-122)
+    // phase 2: migrate the shots into one stack (:45-122)
     jv_status st = jv_image_reset(c);
     if (st != JV_OK) return st;
-    for (int s = 0; s < nshot; s++) {
-        float *t = all.data() + (size_t)s * 3 * per;
-        st = jv_rtm_shot(c, s, t, t + per, t + 2 * per);
+    for (size_t q0 = 0; q0 < mine.size(); q0++) {
+        float *t = all.data() + q0 * 3 * per;
+        st = jv_rtm_shot(c, mine[q0], t, t + per, t + 2 * per);
         if (st != JV_OK) return st;
     }
-    // Laplacian, compensation, save (:123-134)
     const size_t n = (size_t)inf.n_phy;
+    // sum the partial stacks of all ranks, before the Laplacian and the
+    // compensation (the reference applies both to the stack of all shots)
+    if (world > 1) {
+        std::vector<double> buf(n);
+        for (int k = 0; k < 5; k++) {
+            st = jv_image_get(c, k, buf.data());
+            if (st != JV_OK) return st;
+            if (reduce(buf.data(), n, user) != 0) return fail(JV_ECANCELED, "the reduce function failed");
+            st = jv_image_set(c, k, buf.data());
+            if (st != JV_OK) return st;
+        }
+    }
+    if (rank != 0) return JV_OK;
+    // Laplacian, compensation, save (:123-134)
     std::vector<float> im(8 * n);
     float *o[8];
     for (int q = 0; q < 8; q++) o[q] = im.data() + q * n;

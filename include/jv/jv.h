@@ -105,6 +105,22 @@ jv_status jv_create(const jv_grid *grid, const float *vp, const float *vs, const
  * optional argfile keys "rec_width" and "precision" override opt. */
 jv_status jv_open(const char *proj_path, const jv_options *opt, jv_ctx **out);
 
+/* The argfile of a reference project directory as ArgList::mpi_read_arg_file
+ * reads it (FD/fdtd3d_0_base_module/fdtd3d_base_1_interface.hpp:50-112):
+ * JSON with // comments, paths prefixed with proj_path.  rec_width is the
+ * optional key of that name (0 when absent). */
+typedef struct jv_argfile {
+    char model_path[1024];
+    char shot_path[1024];
+    char rece_path[1024];
+    char output_path[1024];
+    int is_output, t_snap, pml_num;
+    float fm, dt, T;
+    int x_divide_num, y_divide_num, z_divide_num, slots_per_node;
+    int rec_width;
+} jv_argfile;
+jv_status jv_read_argfile(const char *proj_path, jv_argfile *out);
+
 /* Sets the survey: shot and receiver positions (x,y,z metres).  Only the
  * points inside gridphy are kept (SubGeometry::get_sub_shot_and_recv,
  * jarvis_device_geometry_meat.hpp:65-128).  Shots keep their input index. */
@@ -183,6 +199,21 @@ jv_status jv_image_set_device(jv_ctx *c, int kind, const double *d_in);
  * shot, then write image_pp_0*.raw and image_pp_laplace_0*.raw with the
  * reference's names and formats.  Only for contexts made by jv_open. */
 jv_status jv_run_project(jv_ctx *c);
+
+/* In-place sum of n doubles over every rank of the caller's job (for
+ * example MPI_Allreduce with MPI_IN_PLACE, or an NCCL all-reduce of a host
+ * staging buffer); returns 0 on success. */
+typedef int (*jv_reduce_fn)(double *buf, size_t n, void *user);
+
+/* jv_run_project for a job of `world` processes (one GPU each), the
+ * replacement of the reference's MPI job (rtm3d_blend_elastic_model_mpi_meat.hpp:
+ * 18-135).  The reference splits the model into subdomains over its ranks;
+ * here every rank holds the whole model and takes the shots s with
+ * s % world == rank: it models them and writes their trace files,
+ * migrates them, sums the five stacks over the job with `reduce` (called
+ * five times, on every rank, in the same order), and rank 0 writes the
+ * images.  world == 1 (reduce may be NULL) is jv_run_project. */
+jv_status jv_run_project_shard(jv_ctx *c, int rank, int world, jv_reduce_fn reduce, void *user);
 
 /* Device time (ms) of the last jv_forward* / jv_rtm_shot* call, measured
  * with CUDA events around its kernels. */

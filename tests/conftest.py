@@ -48,3 +48,18 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.float64)
     d = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (d if d > 0 else 1.0))
+
+
+def build_compat_driver(name: str, out_dir: str) -> str:
+    """Compiles tests/compat/<name>.cpp (a driver written against the jarvis
+    class names) against include/jv/jarvis_compat.hpp and libjv.so."""
+    import subprocess
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    libdir = os.path.join(ROOT, PKG)
+    exe = os.path.join(out_dir, name)
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(cuda, "include"), os.path.join(ROOT, "tests", "compat", name + ".cpp"),
+           "-L", libdir, "-ljv", "-L", os.path.join(cuda, "lib64"), "-lcudart", f"-Wl,-rpath,{libdir}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe

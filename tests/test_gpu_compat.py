@@ -1,0 +1,119 @@
+"""The jarvis-named drivers (tests/compat/*.cpp over jv/jarvis_compat.hpp)
+and the sharded project job (jv_run_project_shard) on the GPU: the same
+files and traces as jv_run_project and the in-memory calls."""
+import subprocess
+import threading
+
+import numpy as np
+import pytest
+
+import make_golden as mg
+from conftest import build_compat_driver, pkg, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+jv = pkg()
+
+
+def _read_outputs(project, d, s):
+    out = {}
+    for sh in range(s.shots.shape[0]):
+        for c in ("vx", "vy", "vz"):
+            out[f"{c}_{sh}"] = project.read_traces(f"{d}/out/{c}_seis_0_{sh}.txt")
+    suf = project.size_info(s.nx, s.ny, s.nz)
+    for nm in ("image_pp_0", "image_pp_laplace_0", "image_ps_0", "image_sp_0", "image_ss_0", "image_ipfd_0"):
+        out[nm] = np.fromfile(f"{d}/out/{nm}{suf}.raw", np.float32)
+    return out
+
+
+def test_rtm_driver_matches_run_project(tmp_path, project):
+    s = mg.case_survey("pin_w1")
+    d1, d2 = str(tmp_path / "a") + "/", str(tmp_path / "b") + "/"
+    project.write_project(d1, s)
+    project.write_project(d2, s)
+    exe = build_compat_driver("rtm_main", str(tmp_path))
+    r = subprocess.run([exe, d1], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    with jv.Context.open(d2) as ctx:
+        ctx.run_project()
+    a, b = _read_outputs(project, d1, s), _read_outputs(project, d2, s)
+    for k in b:
+        assert np.array_equal(a[k], b[k]), k
+    f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_pin_w1.npz")
+    assert rel_l2(a["image_pp_laplace_0"].reshape(s.nz, s.ny, s.nx), f["lap_pp"]) <= 5e-5
+
+
+def test_forward_driver_matches_context(tmp_path, project, synth):
+    s = synth.small_case(n=(16, 14, 12), pml=5, nt=50, seed=3)
+    d = str(tmp_path / "p") + "/"
+    project.write_project(d, s)
+    exe = build_compat_driver("forward_main", str(tmp_path))
+    out = str(tmp_path / "vz.raw")
+    r = subprocess.run([exe, d, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    with jv.Context.open(d) as ctx:
+        vz = ctx.forward(0)[2]
+    got = np.fromfile(out, np.float32).reshape(vz.shape)
+    assert np.array_equal(got, vz)
+
+
+def test_sharded_job_on_two_contexts_matches_single(tmp_path, project, synth):
+    """Two ranks of one job, each its own context on the same GPU and its
+    own host thread; the reduce callback sums through a host barrier (no
+    kernel waits on another)."""
+    s = synth.small_case(n=(18, 16, 14), pml=5, nt=60, seed=8,
+                         shot_idx=[(4, 5, 2), (12, 9, 3), (9, 9, 9)])
+    dref, dsh = str(tmp_path / "ref") + "/", str(tmp_path / "sh") + "/"
+    project.write_project(dref, s)
+    project.write_project(dsh, s)
+    with jv.Context.open(dref) as ctx:
+        ctx.run_project()
+
+    world = 2
+    slots = [None] * world
+    bar = threading.Barrier(world, timeout=120)
+    errors = []
+
+    def make_reduce(rank):
+        def reduce(arr):
+            slots[rank] = arr.copy()
+            bar.wait()
+            total = slots[0] + slots[1]
+            bar.wait()
+            arr[:] = total
+        return reduce
+
+    ctxs = [jv.Context.open(dsh) for _ in range(world)]
+
+    def run(rank):
+        try:
+            ctxs[rank].run_project_shard(rank, world, make_reduce(rank))
+        except Exception as e:  # checked below
+            errors.append(e)
+            bar.abort()
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(world)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=300)
+    for c in ctxs:
+        c.close()
+    assert not errors, errors
+    a, b = _read_outputs(project, dsh, s), _read_outputs(project, dref, s)
+    for k in b:
+        if k.startswith("v"):
+            assert np.array_equal(a[k], b[k]), k
+        else:
+            assert rel_l2(a[k], b[k]) <= 1e-6, (k, rel_l2(a[k], b[k]))
+
+
+def test_shard_arguments_checked(tmp_path, project, synth):
+    s = synth.small_case(n=(10, 10, 10), pml=4, nt=10)
+    d = str(tmp_path / "p") + "/"
+    project.write_project(d, s)
+    with jv.Context.open(d) as ctx:
+        with pytest.raises(jv.JvError):
+            ctx.run_project_shard(2, 2)
+        with pytest.raises(jv.JvError):
+            ctx.run_project_shard(0, 2)  # several ranks need a reduce function
