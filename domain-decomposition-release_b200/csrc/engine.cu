@@ -133,7 +133,8 @@ GridDev make_layout(const jv_grid &grid, size_t *field_elems) {
     return g;
 }
 
-CpmlDev make_pml_slabs(const GridDev &g, long long *psi_total) {
+CpmlDev make_pml_slabs(const GridDev &g, int zp, long long *psi_total) {
+    zp = zp == 2 ? 2 : 1;
     const int NX = g.nx, NY = g.ny, NZ = g.nz, m = g.m;
     // top, bottom (z); front, back (y, physical z); right, left (x, physical y and z)
     const int bx[6][6] = {
@@ -160,13 +161,14 @@ CpmlDev make_pml_slabs(const GridDev &g, long long *psi_total) {
         S.bx = (S.ngroups + S.gx - 1) / S.gx;
         S.by = (S.y1 - S.y0 + S.gy - 1) / S.gy;
         S.first_block = blocks;
-        blocks += S.bx * S.by * (S.z1 - S.z0);
+        blocks += S.bx * S.by * ((S.z1 - S.z0 + zp - 1) / zp);
         S.stride = (long long)S.pitch * (S.y1 - S.y0) * (S.z1 - S.z0);
         S.psi_off = off;
         off += 6LL * S.naxes * S.stride;
         c.s[c.nslab++] = S;
     }
     c.nblocks = blocks;
+    c.zp = zp;
     *psi_total = off;
     return c;
 }
@@ -234,6 +236,9 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if ((opt.min_blocks != 0 && opt.min_blocks != 3 && opt.min_blocks != 4) ||
         (opt.pml_min_blocks != 0 && opt.pml_min_blocks != 3 && opt.pml_min_blocks != 4))
         return bad(JV_EINVAL, "min_blocks and pml_min_blocks must be 0, 3 or 4");
+    if (opt.planes_per_thread < 0 || opt.planes_per_thread > 2 || opt.pml_planes_per_thread < 0 ||
+        opt.pml_planes_per_thread > 2)
+        return bad(JV_EINVAL, "planes_per_thread and pml_planes_per_thread must be 0, 1 or 2");
     if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
         return bad(JV_EINVAL, "tile_gx * tile_gy must be <= 256");
     long long next = (long long)(grid.nx + 2 * grid.pml) * (grid.ny + 2 * grid.pml) * (grid.nz + 2 * grid.pml);
@@ -254,6 +259,8 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     E->kc_.gy = opt.tile_gy;
     if (opt.min_blocks) E->kc_.minb = opt.min_blocks;
     if (opt.pml_min_blocks) E->kc_.pml_minb = opt.pml_min_blocks;
+    if (opt.planes_per_thread) E->kc_.zp = opt.planes_per_thread;
+    if (opt.pml_planes_per_thread) E->kc_.pml_zp = opt.pml_planes_per_thread;
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
@@ -305,7 +312,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     // the 2-cell outer rim; the slab table and axis tables are shared by
     // both wavefields, the memory-variable arenas are per wavefield
     {
-        cpml_proto_ = make_pml_slabs(g_, &psi_total_);
+        cpml_proto_ = make_pml_slabs(g_, kc_.pml_zp, &psi_total_);
         std::vector<float4> t[3];
         pml_axis_tables(g_, fm_, t);
         for (int a = 0; a < 3; a++) {

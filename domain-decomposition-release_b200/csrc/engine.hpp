@@ -40,7 +40,7 @@ GridDev make_layout(const jv_grid &grid, size_t *field_elems);
 // with their launch shapes and memory-variable arena offsets; *psi_total =
 // floats of one wavefield's memory-variable arena.  dt, ax and psi are
 // left for the caller.
-CpmlDev make_pml_slabs(const GridDev &g, long long *psi_total);
+CpmlDev make_pml_slabs(const GridDev &g, int zp, long long *psi_total);
 // Per-axis damping factor tables {K, K_half, alpha, alpha_half}, K = 0
 // outside the axis' absorbing range
 // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620).

@@ -58,6 +58,7 @@ struct PmlSlab {
 struct CpmlDev {
     PmlSlab s[6];
     int nslab, nblocks;
+    int zp;                   // planes a thread updates (1 or 2); blocks cover zp planes
     float dt;                 // |time step|
     const float4 *ax[3];      // per axis, per extended index: {K, K_half, alpha, alpha_half}, K = 0 outside
     float *psi;               // this wavefield's memory-variable arena
@@ -114,6 +115,8 @@ struct KCfg {
     int gx = 0, gy = 0;  // variant 2 block: x groups per block, rows per block (0: auto)
     int minb = 4;        // variant 2: blocks per SM the register budget is set for (3 or 4)
     int pml_minb = 4;    // CPML kernels: the same
+    int zp = 1;          // variant 2: z planes per thread (1 or 2)
+    int pml_zp = 1;      // CPML kernels: the same
 };
 
 // kernels.cu ------------------------------------------------------------

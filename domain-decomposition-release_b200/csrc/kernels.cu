@@ -509,13 +509,12 @@ __device__ __forceinline__ void st4(float *f, int i0, const float *v, int nvalid
     }
 }
 
-template <int MODE, bool IMG, int MINB>
-__global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ rho,
-                                                       float dt, int rec_w, WaveDev rv, ImageDev img) {
-    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
-    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
-    const int pk = blockIdx.z;
-    if (pi0 >= g.px || pj >= g.py) return;
+// One 4-cell group (x cells pi0..pi0+3 of row pj, plane pk) of the
+// velocity update.
+template <int MODE, bool IMG>
+__device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
+                                           float dt, int rec_w, const WaveDev &rv, const ImageDev &img, int pi0,
+                                           int pj, int pk) {
     constexpr bool kP = (MODE == kBwd || MODE == kRev);
     const int nvalid = min(4, g.px - pi0);
     const int sy = (int)g.sy, sz = (int)g.sz;
@@ -640,15 +639,28 @@ __global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, co
     }
 }
 
-template <int MODE, int MINB>
-__global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w, const float *__restrict__ lam,
-                                                          const float *__restrict__ mu, float dt, int rec_w,
-                                                          const float *__restrict__ wavelet,
-                                                          const StepState *__restrict__ st, int it_off) {
+
+// Blocks of blockDim.x groups x blockDim.y rows x ZP planes; a thread
+// updates its group in ZP consecutive planes.
+template <int MODE, bool IMG, int MINB, int ZP>
+__global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ rho,
+                                                       float dt, int rec_w, WaveDev rv, ImageDev img) {
     const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int pj = blockIdx.y * blockDim.y + threadIdx.y;
-    const int pk = blockIdx.z;
     if (pi0 >= g.px || pj >= g.py) return;
+#pragma unroll
+    for (int zz = 0; zz < ZP; zz++) {
+        const int pk = blockIdx.z * ZP + zz;
+        if (pk < g.pz) vel_group4<MODE, IMG>(g, w, rho, dt, rec_w, rv, img, pi0, pj, pk);
+    }
+}
+
+// One 4-cell group of the stress update (source fused).
+template <int MODE>
+__device__ __forceinline__ void stress_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ lam,
+                                              const float *__restrict__ mu, float dt, int rec_w,
+                                              const float *__restrict__ wavelet, const StepState *__restrict__ st,
+                                              int it_off, int pi0, int pj, int pk) {
     const int nvalid = min(4, g.px - pi0);
     const int sy = (int)g.sy, sz = (int)g.sz;
     const int i0 = (int)g.xoff + (pi0 + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
@@ -744,6 +756,21 @@ __global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w,
     }
 }
 
+template <int MODE, int MINB, int ZP>
+__global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w, const float *__restrict__ lam,
+                                                          const float *__restrict__ mu, float dt, int rec_w,
+                                                          const float *__restrict__ wavelet,
+                                                          const StepState *__restrict__ st, int it_off) {
+    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
+    if (pi0 >= g.px || pj >= g.py) return;
+#pragma unroll
+    for (int zz = 0; zz < ZP; zz++) {
+        const int pk = blockIdx.z * ZP + zz;
+        if (pk < g.pz) stress_group4<MODE>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off, pi0, pj, pk);
+    }
+}
+
 // ---------------------------------------------------------------- CPML
 
 // Damping coefficients of one absorbing axis at one cell
@@ -822,6 +849,8 @@ struct PmlPos {
     long long psi;       // arena offset of the group's first memory variable
     long long stride;    // floats between memory arrays of the slab
     int naxes;
+    int z1;              // end plane of the slab
+    int plane;           // memory-variable floats of one slab plane
 };
 __device__ __forceinline__ bool pml_pos(const CpmlDev &P, PmlPos &q) {
     const int b = blockIdx.x;
@@ -833,7 +862,7 @@ __device__ __forceinline__ bool pml_pos(const CpmlDev &P, PmlPos &q) {
     const int bxi = lb % S.bx;
     const int t = lb / S.bx;
     const int byi = t % S.by;
-    q.z = S.z0 + t / S.by;
+    q.z = S.z0 + (t / S.by) * P.zp;
     const int tr = (int)threadIdx.x / S.gx;
     const int grp = bxi * S.gx + ((int)threadIdx.x - tr * S.gx);
     q.y = S.y0 + byi * S.gy + tr;
@@ -846,6 +875,8 @@ __device__ __forceinline__ bool pml_pos(const CpmlDev &P, PmlPos &q) {
     q.psi = S.psi_off + ((long long)(q.z - S.z0) * (S.y1 - S.y0) + (q.y - S.y0)) * S.pitch + 4 * grp;
     q.stride = S.stride;
     q.naxes = S.naxes;
+    q.z1 = S.z1;
+    q.plane = (S.y1 - S.y0) * S.pitch;
     return true;
 }
 
@@ -864,11 +895,9 @@ __device__ __forceinline__ void xcoef4(const CpmlDev &P, const PmlPos &q, float 
 // CPML velocity update of the six absorbing slabs: 4th order, memory
 // variables on the absorbing axes (z-slabs x,y,z; y-slabs x,y; x-slabs x)
 // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_2_kernel_device_{x,y,z}_meat.hpp)
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
-                                                  const float *__restrict__ vpm) {
-    PmlPos q;
-    if (!pml_pos(P, q)) return;
+__device__ __forceinline__ void vel_pml_group(const GridDev &g, const CpmlDev &P, const WaveDev &w,
+                                              const float *__restrict__ rho, const float *__restrict__ vpm,
+                                              const PmlPos &q) {
     const int sy = (int)g.sy, sz = (int)g.sz;
     const int i0 = (int)g.xoff + q.xs + sy * q.y + sz * q.z;
     const float c0 = c_dc2[0], c1 = c_dc2[1];
@@ -939,12 +968,10 @@ __global__ void __launch_bounds__(256, MINB) vel_pml(GridDev g, CpmlDev P, WaveD
     st4m(w.f[VZ], i0, v, q.mask);
 }
 
-template <bool WITH_SAU, int MINB>
-__global__ void __launch_bounds__(256, MINB) stress_pml(GridDev g, CpmlDev P, WaveDev w,
-                                                     const float *__restrict__ lam, const float *__restrict__ mu,
-                                                     const float *__restrict__ vpm) {
-    PmlPos q;
-    if (!pml_pos(P, q)) return;
+template <bool WITH_SAU>
+__device__ __forceinline__ void stress_pml_group(const GridDev &g, const CpmlDev &P, const WaveDev &w,
+                                                 const float *__restrict__ lam, const float *__restrict__ mu,
+                                                 const float *__restrict__ vpm, const PmlPos &q) {
     const int sy = (int)g.sy, sz = (int)g.sz;
     const int i0 = (int)g.xoff + q.xs + sy * q.y + sz * q.z;
     const float c0 = c_dc2[0], c1 = c_dc2[1];
@@ -1033,6 +1060,37 @@ __global__ void __launch_bounds__(256, MINB) stress_pml(GridDev g, CpmlDev P, Wa
 #pragma unroll
     for (int c = 0; c < 4; c++) a[c] += dt * m[c] * (vz_y[c] + vy_z[c]);
     st4m(w.f[SYZ], i0, a, q.mask);
+}
+
+// Blocks of 256 threads over (slab, row block, plane block); a thread
+// updates its group in P.zp consecutive planes of its slab.
+template <int MINB, int ZP>
+__global__ void __launch_bounds__(256, MINB) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
+                                                  const float *__restrict__ vpm) {
+    PmlPos q;
+    if (!pml_pos(P, q)) return;
+#pragma unroll
+    for (int zz = 0; zz < ZP; zz++) {
+        if (q.z >= q.z1) break;
+        vel_pml_group(g, P, w, rho, vpm, q);
+        q.z++;
+        q.psi += q.plane;
+    }
+}
+
+template <bool WITH_SAU, int MINB, int ZP>
+__global__ void __launch_bounds__(256, MINB) stress_pml(GridDev g, CpmlDev P, WaveDev w,
+                                                     const float *__restrict__ lam, const float *__restrict__ mu,
+                                                     const float *__restrict__ vpm) {
+    PmlPos q;
+    if (!pml_pos(P, q)) return;
+#pragma unroll
+    for (int zz = 0; zz < ZP; zz++) {
+        if (q.z >= q.z1) break;
+        stress_pml_group<WITH_SAU>(g, P, w, lam, mu, vpm, q);
+        q.z++;
+        q.psi += q.plane;
+    }
 }
 
 // ------------------------------------------------------------ receivers
@@ -1208,36 +1266,37 @@ static void v4_shape(const GridDev &g, const KCfg &kc, dim3 *b, dim3 *gr) {
     gx = std::min(std::max(gx, 1), 256);
     int gy = kc.gy > 0 ? kc.gy : std::max(1, 256 / gx);
     gy = std::min(std::max(gy, 1), 256 / gx);
+    const int zp = kc.zp == 2 ? 2 : 1;
     *b = dim3(gx, gy);
-    *gr = dim3((ngx + gx - 1) / gx, (g.py + gy - 1) / gy, g.pz);
+    *gr = dim3((ngx + gx - 1) / gx, (g.py + gy - 1) / gy, (g.pz + zp - 1) / zp);
 }
 
-template <int MINB>
+template <int MINB, int ZP>
 static int launch_vel_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDev &g, const WaveDev &w,
                          const float *rho, float dt, int rec_w, const WaveDev *rev, const ImageDev *img,
                          const WaveDev &rv, const ImageDev &im) {
     switch (mode) {
-    case kFwd: vel_phy_v4<kFwd, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-    case kRtmFwd: vel_phy_v4<kRtmFwd, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-    case kRev: vel_phy_v4<kRev, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kFwd: vel_phy_v4<kFwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kRtmFwd: vel_phy_v4<kRtmFwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kRev: vel_phy_v4<kRev, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
     case kBwd:
-        if (img && rev) vel_phy_v4<kBwd, true, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
-        else vel_phy_v4<kBwd, false, MINB><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        if (img && rev) vel_phy_v4<kBwd, true, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        else vel_phy_v4<kBwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
         break;
     default: return (int)cudaErrorInvalidValue;
     }
     return cerr();
 }
 
-template <int MINB>
+template <int MINB, int ZP>
 static int launch_stress_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDev &g, const WaveDev &w,
                             const float *lam, const float *mu, float dt, int rec_w, const float *wavelet,
                             const StepState *st, int it_off) {
     switch (mode) {
-    case kFwd: stress_phy_v4<kFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
-    case kRtmFwd: stress_phy_v4<kRtmFwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
-    case kBwd: stress_phy_v4<kBwd, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
-    case kRev: stress_phy_v4<kRev, MINB><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kFwd: stress_phy_v4<kFwd, MINB, ZP><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kRtmFwd: stress_phy_v4<kRtmFwd, MINB, ZP><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kBwd: stress_phy_v4<kBwd, MINB, ZP><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
+    case kRev: stress_phy_v4<kRev, MINB, ZP><<<gr, b, 0, s>>>(g, w, lam, mu, dt, rec_w, wavelet, st, it_off); break;
     default: return (int)cudaErrorInvalidValue;
     }
     return cerr();
@@ -1251,8 +1310,12 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
     if (kc.variant == 2) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
-        if (kc.minb == 4) return launch_vel_v4<4>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
-        return launch_vel_v4<3>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+        if (kc.zp == 2) {
+            if (kc.minb == 4) return launch_vel_v4<4, 2>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+            return launch_vel_v4<3, 2>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+        }
+        if (kc.minb == 4) return launch_vel_v4<4, 1>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+        return launch_vel_v4<3, 1>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
     }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
@@ -1289,9 +1352,14 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
     if (kc.variant == 2) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
+        if (kc.zp == 2) {
+            if (kc.minb == 4)
+                return launch_stress_v4<4, 2>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
+            return launch_stress_v4<3, 2>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
+        }
         if (kc.minb == 4)
-            return launch_stress_v4<4>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
-        return launch_stress_v4<3>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
+            return launch_stress_v4<4, 1>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
+        return launch_stress_v4<3, 1>(mode, gr, b, s, g, w, lam, mu, dt, rec_w, wavelet, st, it_off);
     }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
@@ -1321,8 +1389,13 @@ int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float 
     if (c.nblocks <= 0) return 0;
     const unsigned blocks = (unsigned)c.nblocks;
     cudaStream_t s = (cudaStream_t)stream;
-    if (kc.pml_minb == 4) vel_pml<4><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
-    else vel_pml<3><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+    if (c.zp == 2) {
+        if (kc.pml_minb == 4) vel_pml<4, 2><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+        else vel_pml<3, 2><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+    } else {
+        if (kc.pml_minb == 4) vel_pml<4, 1><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+        else vel_pml<3, 1><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+    }
     return cerr();
 }
 
@@ -1332,12 +1405,22 @@ int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const flo
     const unsigned blocks = (unsigned)c.nblocks;
     cudaStream_t s = (cudaStream_t)stream;
     const bool m4 = kc.pml_minb == 4;
-    if (with_sau) {
-        if (m4) stress_pml<true, 4><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
-        else stress_pml<true, 3><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+    if (c.zp == 2) {
+        if (with_sau) {
+            if (m4) stress_pml<true, 4, 2><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+            else stress_pml<true, 3, 2><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        } else {
+            if (m4) stress_pml<false, 4, 2><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+            else stress_pml<false, 3, 2><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        }
     } else {
-        if (m4) stress_pml<false, 4><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
-        else stress_pml<false, 3><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        if (with_sau) {
+            if (m4) stress_pml<true, 4, 1><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+            else stress_pml<true, 3, 1><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        } else {
+            if (m4) stress_pml<false, 4, 1><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+            else stress_pml<false, 3, 1><<<blocks, 256, 0, s>>>(g, c, w, lam, mu, vp);
+        }
     }
     return cerr();
 }

@@ -101,7 +101,7 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
     const GridDev g = make_layout(*grid, &fe);
     const size_t guard = 32;
     long long psi_total = 0;
-    CpmlDev cp = make_pml_slabs(g, &psi_total);
+    CpmlDev cp = make_pml_slabs(g, 1, &psi_total);
     cp.dt = dt;
 
     // receivers inside gridphy, in input order (as jv_set_geometry keeps them)

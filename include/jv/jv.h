@@ -81,6 +81,8 @@ typedef struct jv_options {
     int tile_gy;        /* variant 2: rows per block (0 -> auto)                 */
     int min_blocks;     /* interior kernels: register budget for 3 or 4 blocks/SM (0 -> 4) */
     int pml_min_blocks; /* absorbing-layer kernels: the same (0 -> 4)            */
+    int planes_per_thread;     /* variant 2: z planes a thread updates, 1 or 2 (0 -> 1) */
+    int pml_planes_per_thread; /* absorbing-layer kernels: the same (0 -> 1)      */
 } jv_options;
 
 /* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,

@@ -164,3 +164,31 @@ def test_errors_are_status_codes(synth):
         with pytest.raises(jv.JvError) as e:
             ctx.forward(0)
         assert "outside gridphy" in str(e.value)
+
+
+OPTION_SETS = [
+    dict(planes_per_thread=2),
+    dict(pml_planes_per_thread=2),
+    dict(min_blocks=3, pml_min_blocks=3),
+    dict(tile_gx=3, tile_gy=7),
+    dict(planes_per_thread=2, pml_planes_per_thread=2, tile_gx=5, tile_gy=9),
+]
+
+
+@pytest.mark.parametrize("kw", OPTION_SETS)
+def test_launch_options_do_not_change_results(synth, kw):
+    """Launch shapes, register budgets and planes per thread change only how
+    the cells are assigned to threads (odd sizes, so partial groups, rows
+    and plane pairs all occur)."""
+    s = synth.small_case(n=(23, 17, 15), pml=7, nt=70, seed=31, anomaly=(0.1, 3.0), shot_idx=[(11, 8, 3)])
+    out = []
+    for opts in (dict(), kw):
+        with jv.Context.from_survey(s, **opts) as ctx:
+            tr = ctx.forward(0)
+            ctx.rtm_shot(0, tr)
+            out.append((tr, ctx.images()))
+    (t0, i0), (t1, i1) = out
+    for a, b in zip(t0, t1):
+        assert rel_l2(a, b) <= 1e-6
+    for k in i0:
+        assert rel_l2(i0[k], i1[k]) <= 1e-6, k
