@@ -179,7 +179,10 @@ OPTION_SETS = [
 def test_launch_options_do_not_change_results(synth, kw):
     """Launch shapes, register budgets and planes per thread change only how
     the cells are assigned to threads (odd sizes, so partial groups, rows
-    and plane pairs all occur)."""
+    and plane pairs all occur).  A different register budget can change
+    which multiply-adds the compiler contracts, so results agree to FP32
+    rounding: traces 1e-6; images, whose correlation sums cancel, 2e-5
+    (the tolerance against the FP64 oracle is 5e-5)."""
     s = synth.small_case(n=(23, 17, 15), pml=7, nt=70, seed=31, anomaly=(0.1, 3.0), shot_idx=[(11, 8, 3)])
     out = []
     for opts in (dict(), kw):
@@ -191,4 +194,4 @@ def test_launch_options_do_not_change_results(synth, kw):
     for a, b in zip(t0, t1):
         assert rel_l2(a, b) <= 1e-6
     for k in i0:
-        assert rel_l2(i0[k], i1[k]) <= 1e-6, k
+        assert rel_l2(i0[k], i1[k]) <= 2e-5, k
