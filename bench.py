@@ -348,6 +348,7 @@ def main():
     # end to end through the host-pointer ABI: pinned H2D of the traces,
     # D2H of the 8 finalized images, every step
     e2e = None
+    modes = None
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
     if e2e_steps > 0:
         host = torch.empty((3, nrec, nt), dtype=torch.float32, pin_memory=True)
@@ -366,6 +367,37 @@ def main():
             te = float(t.item())
         e2e = {"value": round(e2e_steps * world / te * 3600.0, 3), "unit": "shots/h",
                "h2d_bytes_per_step": int(3 * nrec * nt * 4), "d2h_bytes_per_step": int(8 * info.n_phy * 4)}
+
+        # the same shots as one batch (jv_rtm_batch: the next shot's traces
+        # copied while the current one runs, images read once per batch)
+        # and as queued jobs (jv_submit / jv_wait), host buffers as above
+        def timed(fn):
+            barrier()
+            t1 = time.perf_counter()
+            fn()
+            barrier()
+            tt = time.perf_counter() - t1
+            if dist is not None:
+                tq = torch.tensor([tt], dtype=torch.float64, device=f"cuda:{local}")
+                dist.all_reduce(tq, op=dist.ReduceOp.MAX)
+                tt = float(tq.item())
+            return round(e2e_steps * world / tt * 3600.0, 3)
+
+        def batched():
+            ctx.rtm_batch([0] * e2e_steps, [hobs] * e2e_steps)
+            ctx.finalize()
+
+        def served():
+            ids = [ctx.submit(jv.JOB_RTM, 0, obs=hobs) for _ in range(e2e_steps)]
+            for i in ids:
+                if ctx.wait(i) != 0:
+                    raise RuntimeError("served job failed")
+            ctx.finalize()
+
+        modes = {"unit": "shots/h", "plain_e2e": e2e["value"], "batched_e2e": timed(batched),
+                 "served_e2e": timed(served),
+                 "note": "plain: one jv_rtm_shot + jv_image_finalize per shot; batched: one jv_rtm_batch of the "
+                         "shots, one finalize; served: the shots as queued RTM jobs, one finalize"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -403,7 +435,7 @@ def main():
                    "rec_width": s.rec_width, "n_recv": nrec, "mode": "plain one-shot-per-call, graph time loop",
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "clocks": clk,
         "gpu_launches": launches * args.steps if launches else None,
         "gpu_launches_note": "kernels of the timed shots, counted from one instrumented shot (graph path)",
         "wall_s": round(wall, 3),

@@ -41,8 +41,11 @@ EXPORTS = (
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
     "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
     "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info", "jv_forward_noalloc",
-    "jv_image_set", "jv_image_set_device", "jv_run_project_shard", "jv_read_argfile",
+    "jv_image_set", "jv_image_set_device", "jv_run_project_shard", "jv_read_argfile", "jv_rtm_batch",
+    "jv_submit", "jv_poll", "jv_wait", "jv_cancel",
 )
+JOB_FORWARD, JOB_RTM = 0, 1
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELLED = 0, 1, 2, 3
 
 REDUCE_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_size_t, C.c_void_p)
 
@@ -64,6 +67,11 @@ class Options(C.Structure):
                 ("kernel_variant", C.c_int), ("zchunk", C.c_int), ("tile_gx", C.c_int), ("tile_gy", C.c_int),
                 ("min_blocks", C.c_int), ("pml_min_blocks", C.c_int), ("planes_per_thread", C.c_int),
                 ("pml_planes_per_thread", C.c_int)]
+
+
+class Job(C.Structure):
+    _fields_ = [("kind", C.c_int), ("shot", C.c_int), ("obs", C.POINTER(C.c_float) * 3),
+                ("out", C.POINTER(C.c_float) * 3)]
 
 
 class ArgFileC(C.Structure):
@@ -132,6 +140,11 @@ def lib() -> C.CDLL:
     L.jv_set_profiling.argtypes = [ctxp, C.c_int]
     L.jv_profile_entry.argtypes = [ctxp, C.c_int, C.POINTER(C.c_char_p), dp, C.POINTER(C.c_longlong)]
     L.jv_run_project.argtypes = [ctxp]
+    L.jv_rtm_batch.argtypes = [ctxp, C.c_int, C.POINTER(C.c_int), C.POINTER(fp)]
+    L.jv_submit.argtypes = [ctxp, C.POINTER(Job), C.POINTER(C.c_longlong)]
+    L.jv_poll.argtypes = [ctxp, C.c_longlong, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.jv_wait.argtypes = [ctxp, C.c_longlong, C.c_double, C.POINTER(C.c_int)]
+    L.jv_cancel.argtypes = [ctxp, C.c_longlong]
     L.jv_run_project_shard.argtypes = [ctxp, C.c_int, C.c_int, REDUCE_FN, C.c_void_p]
     L.jv_read_argfile.argtypes = [C.c_char_p, C.POINTER(ArgFileC)]
     L.jv_forward_noalloc.argtypes = [C.POINTER(Grid), vp, vp, vp, C.c_float, C.c_float, C.c_int, fp, C.c_int, fp,
@@ -295,6 +308,54 @@ class Context:
 
     def run_project(self) -> None:
         _check(lib().jv_run_project(self._h))
+
+    def rtm_batch(self, shots, obs) -> None:
+        """jv_rtm_batch: obs[k] = (vx, vy, vz) float32 host arrays of shots[k]."""
+        n = len(shots)
+        keep = [np.ascontiguousarray(a, dtype=np.float32) for o in obs for a in o]
+        ptrs = (C.POINTER(C.c_float) * (3 * n))(*[_fptr(a) for a in keep])
+        sh = (C.c_int * n)(*[int(s) for s in shots])
+        _check(lib().jv_rtm_batch(self._h, n, sh, ptrs))
+
+    def submit(self, kind: int, shot: int, obs=None, out=None) -> int:
+        """jv_submit; the arrays in obs / out must live until the job ends
+        (this object keeps references to them)."""
+        j = Job()
+        j.kind, j.shot = kind, shot
+        refs = []
+        for q in range(3):
+            if obs is not None:
+                a = np.ascontiguousarray(obs[q], dtype=np.float32)
+                refs.append(a)
+                j.obs[q] = _fptr(a)
+            if out is not None and out[q] is not None:
+                if out[q].dtype != np.float32 or not out[q].flags.c_contiguous:
+                    raise JvError(JV_EINVAL, "job outputs must be C-contiguous float32 arrays")
+                refs.append(out[q])
+                j.out[q] = _fptr(out[q])
+        jid = C.c_longlong()
+        _check(lib().jv_submit(self._h, C.byref(j), C.byref(jid)))
+        self._job_refs = getattr(self, "_job_refs", {})
+        self._job_refs[jid.value] = refs
+        return jid.value
+
+    def poll(self, jid: int):
+        """(state, result) of a job."""
+        st, res = C.c_int(), C.c_int()
+        _check(lib().jv_poll(self._h, jid, C.byref(st), C.byref(res)))
+        if st.value in (JOB_DONE, JOB_CANCELLED):
+            getattr(self, "_job_refs", {}).pop(jid, None)
+        return st.value, res.value
+
+    def wait(self, jid: int, timeout: float = -1.0) -> int:
+        """Waits for a job; returns its result (JvError on JV_ETIMEOUT)."""
+        res = C.c_int()
+        _check(lib().jv_wait(self._h, jid, timeout, C.byref(res)))
+        getattr(self, "_job_refs", {}).pop(jid, None)
+        return res.value
+
+    def cancel(self, jid: int) -> None:
+        _check(lib().jv_cancel(self._h, jid))
 
     def run_project_shard(self, rank: int, world: int, reduce=None) -> None:
         """jv_run_project_shard; `reduce(arr)` sums a float64 numpy array in

@@ -822,6 +822,12 @@ Status Engine::image_set(int kind, const double *src, bool src_on_device) {
     return Status{};
 }
 
+Status Engine::wait_event(cudaEvent_t e) {
+    JV_CU(cudaSetDevice(dev_));
+    JV_CU(cudaStreamWaitEvent(stream_, e, 0));
+    return Status{};
+}
+
 Status Engine::sync() {
     JV_CU(cudaSetDevice(dev_));
     JV_CU(cudaStreamSynchronize(stream_));

@@ -77,9 +77,13 @@ class Engine {
     Status sync();
     void info(jv_info *i) const;
     double last_ms() const { return last_ms_; }
+    void set_last_ms(double ms) { last_ms_ = ms; }
     int nrec() const { return nrec_; }
     int nt() const { return nt_; }
     cudaStream_t stream() const { return stream_; }
+    int device() const { return dev_; }
+    // the next kernels of this context wait for `e` (recorded on another stream)
+    Status wait_event(cudaEvent_t e);
 
     // project bookkeeping (jv_open)
     std::string output_path;

@@ -3,10 +3,16 @@
 // keeps the message for jv_last_error(); nothing here aborts.
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine.hpp"
@@ -31,32 +37,121 @@ namespace jv {
 void set_last_error(const std::string &m) { g_err = m; }
 }  // namespace jv
 
+// One submitted job and what became of it.
+struct JobRec {
+    jv_job job{};
+    int state = JV_JOB_QUEUED;
+    jv_status result = JV_OK;
+    std::string msg;
+};
+
 struct jv_ctx {
     std::unique_ptr<jv::Engine> eng;
     bool from_project = false;
     jv::ArgFile arg;
     std::vector<float> shots, recvs;
-    // device scratch for host-pointer calls
-    float *d_tr = nullptr;
-    size_t d_tr_elems = 0;
+    // device trace buffers for host-pointer calls (the second one lets a
+    // batch copy the next shot's traces while the current shot runs)
+    float *d_tr[2] = {nullptr, nullptr};
+    size_t d_tr_elems[2] = {0, 0};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copy[2] = {nullptr, nullptr};
+    // job queue, served in submission order by one worker thread
+    std::mutex mu;
+    std::condition_variable cv;       // the worker waits for jobs / stop
+    std::condition_variable done_cv;  // callers wait for jobs to end
+    std::deque<long long> queue;
+    std::map<long long, JobRec> jobs;
+    long long next_id = 1;
+    bool running = false, stop = false;
+    std::thread worker;
+
+    bool busy() {
+        std::lock_guard<std::mutex> l(mu);
+        return running || !queue.empty();
+    }
+    // cancels queued jobs, lets the running one finish, joins the worker
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> l(mu);
+            stop = true;
+            for (long long id : queue) {
+                jobs[id].state = JV_JOB_CANCELLED;
+                jobs[id].result = JV_ECANCELED;
+                jobs[id].msg = "context closed";
+            }
+            queue.clear();
+        }
+        cv.notify_all();
+        done_cv.notify_all();
+        if (worker.joinable()) worker.join();
+    }
     ~jv_ctx() {
-        if (d_tr) cudaFree(d_tr);
+        shutdown();
+        if (eng) cudaSetDevice(eng->device());
+        for (int q = 0; q < 2; q++) {
+            if (d_tr[q]) cudaFree(d_tr[q]);
+            if (ev_copy[q]) cudaEventDestroy(ev_copy[q]);
+        }
+        if (copy_stream) cudaStreamDestroy(copy_stream);
     }
 };
 
-static jv_status ensure_traces(jv_ctx *c, size_t elems) {
-    if (c->d_tr_elems >= elems) return JV_OK;
-    if (c->d_tr) cudaFree(c->d_tr);
-    c->d_tr = nullptr;
-    c->d_tr_elems = 0;
+static jv_status ensure_traces(jv_ctx *c, size_t elems, int which = 0) {
+    if (c->d_tr_elems[which] >= elems) return JV_OK;
+    cudaSetDevice(c->eng->device());
+    if (c->d_tr[which]) cudaFree(c->d_tr[which]);
+    c->d_tr[which] = nullptr;
+    c->d_tr_elems[which] = 0;
     if (elems == 0) return JV_OK;
-    cudaError_t e = cudaMalloc(&c->d_tr, elems * sizeof(float));
+    cudaError_t e = cudaMalloc(&c->d_tr[which], elems * sizeof(float));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(JV_ENOMEM, std::string("trace buffer: ") + cudaGetErrorString(e));
     }
-    c->d_tr_elems = elems;
+    c->d_tr_elems[which] = elems;
     return JV_OK;
+}
+
+// calls that use the engine are refused while jobs are queued or running
+#define JV_IDLE(c)                                                                           \
+    do {                                                                                     \
+        if (!(c)) return fail(JV_EINVAL, "NULL context");                                    \
+        if ((c)->busy()) return fail(JV_ESTATE, "jobs are queued or running on this context"); \
+    } while (0)
+
+// host-pointer forward modelling / migration of one shot (no idle check)
+static jv_status forward_host(jv_ctx *c, int shot, float *vx, float *vy, float *vz) {
+    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
+    jv_status st = ensure_traces(c, 3 * per);
+    if (st != JV_OK) return st;
+    float *d = c->d_tr[0];
+    st = ret(c->eng->forward(shot, vx ? d : nullptr, vy ? d + per : nullptr, vz ? d + 2 * per : nullptr));
+    if (st != JV_OK) return st;
+    float *h[3] = {vx, vy, vz};
+    for (int q = 0; q < 3; q++)
+        if (h[q] && per) {
+            cudaError_t e = cudaMemcpyAsync(h[q], d + q * per, per * sizeof(float), cudaMemcpyDeviceToHost,
+                                            c->eng->stream());
+            if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+        }
+    cudaError_t e = cudaStreamSynchronize(c->eng->stream());
+    if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+    return JV_OK;
+}
+
+static jv_status rtm_host(jv_ctx *c, int shot, const float *ox, const float *oy, const float *oz) {
+    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
+    if (per && (!ox || !oy || !oz)) return fail(JV_EINVAL, "observed traces must not be NULL");
+    jv_status st = ensure_traces(c, 3 * per);
+    if (st != JV_OK) return st;
+    const float *h[3] = {ox, oy, oz};
+    for (int q = 0; q < 3 && per; q++) {
+        cudaError_t e = cudaMemcpyAsync(c->d_tr[0] + q * per, h[q], per * sizeof(float), cudaMemcpyHostToDevice,
+                                        c->eng->stream());
+        if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+    }
+    return ret(c->eng->rtm_shot(shot, c->d_tr[0], c->d_tr[0] + per, c->d_tr[0] + 2 * per));
 }
 
 extern "C" {
@@ -159,7 +254,7 @@ jv_status jv_read_argfile(const char *proj_path, jv_argfile *out) {
 }
 
 jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     jv::Status s = c->eng->set_geometry(n_shot, shot_xyz, n_recv, recv_xyz);
     if (s) {
         c->shots.assign(shot_xyz, shot_xyz + 3 * (size_t)n_shot);
@@ -175,84 +270,220 @@ jv_status jv_get_info(const jv_ctx *c, jv_info *info) {
 }
 
 jv_status jv_forward_device(jv_ctx *c, int shot, float *d_vx, float *d_vy, float *d_vz) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->forward(shot, d_vx, d_vy, d_vz));
 }
 
 jv_status jv_forward(jv_ctx *c, int shot, float *vx, float *vy, float *vz) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
-    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
-    jv_status st = ensure_traces(c, 3 * per);
-    if (st != JV_OK) return st;
-    float *d = c->d_tr;
-    st = jv_forward_device(c, shot, vx ? d : nullptr, vy ? d + per : nullptr, vz ? d + 2 * per : nullptr);
-    if (st != JV_OK) return st;
-    float *h[3] = {vx, vy, vz};
-    for (int q = 0; q < 3; q++)
-        if (h[q] && per) {
-            cudaError_t e = cudaMemcpyAsync(h[q], d + q * per, per * sizeof(float), cudaMemcpyDeviceToHost,
-                                            c->eng->stream());
-            if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
-        }
-    cudaError_t e = cudaStreamSynchronize(c->eng->stream());
-    if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
-    return JV_OK;
+    JV_IDLE(c);
+    return forward_host(c, shot, vx, vy, vz);
 }
 
 jv_status jv_rtm_shot_device(jv_ctx *c, int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->rtm_shot(shot, d_ox, d_oy, d_oz));
 }
 
 jv_status jv_rtm_shot(jv_ctx *c, int shot, const float *ox, const float *oy, const float *oz) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
+    return rtm_host(c, shot, ox, oy, oz);
+}
+
+jv_status jv_rtm_batch(jv_ctx *c, int n, const int *shots, const float *const *obs) {
+    JV_IDLE(c);
+    if (n < 0 || (n > 0 && (!shots || !obs))) return fail(JV_EINVAL, "jv_rtm_batch: bad arguments");
     const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
-    if (per && (!ox || !oy || !oz)) return fail(JV_EINVAL, "observed traces must not be NULL");
+    for (int k = 0; k < n && per; k++)
+        for (int q = 0; q < 3; q++)
+            if (!obs[3 * k + q]) return fail(JV_EINVAL, "observed traces must not be NULL");
+    for (int b = 0; b < 2 && n > b; b++) {
+        jv_status st = ensure_traces(c, 3 * per, b);
+        if (st != JV_OK) return st;
+    }
+    cudaSetDevice(c->eng->device());
+    if (!c->copy_stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+        for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaEventCreateWithFlags(&c->ev_copy[b], cudaEventDisableTiming);
+        if (e != cudaSuccess) return fail(JV_ECUDA, std::string("batch stream: ") + cudaGetErrorString(e));
+    }
+    // shot k's traces go to buffer k % 2 on the copy stream; buffer k % 2
+    // is free once shot k - 2 has finished, which jv_rtm_shot waits for
+    auto issue = [&](int k) -> jv_status {
+        float *d = c->d_tr[k % 2];
+        for (int q = 0; q < 3 && per; q++) {
+            cudaError_t e = cudaMemcpyAsync(d + q * per, obs[3 * k + q], per * sizeof(float), cudaMemcpyHostToDevice,
+                                            c->copy_stream);
+            if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+        }
+        cudaError_t e = cudaEventRecord(c->ev_copy[k % 2], c->copy_stream);
+        if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+        return JV_OK;
+    };
+    jv_status st = n > 0 ? issue(0) : JV_OK;
+    double total = 0.0;
+    for (int k = 0; k < n && st == JV_OK; k++) {
+        if (k + 1 < n) st = issue(k + 1);
+        if (st != JV_OK) break;
+        st = ret(c->eng->wait_event(c->ev_copy[k % 2]));
+        if (st != JV_OK) break;
+        float *d = c->d_tr[k % 2];
+        st = ret(c->eng->rtm_shot(shots[k], d, d + per, d + 2 * per));
+        total += c->eng->last_ms();
+    }
+    cudaStreamSynchronize(c->copy_stream);
+    if (st == JV_OK) c->eng->set_last_ms(total);
+    return st;
+}
+
+// ---------------------------------------------------------------- jobs
+
+static jv_status run_job(jv_ctx *c, const jv_job &j) {
+    if (j.kind == JV_JOB_FORWARD) return forward_host(c, j.shot, j.out[0], j.out[1], j.out[2]);
+    if (j.obs[0] || j.obs[1] || j.obs[2]) return rtm_host(c, j.shot, j.obs[0], j.obs[1], j.obs[2]);
+    // no observed traces: model them on the device, then migrate them
+    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
     jv_status st = ensure_traces(c, 3 * per);
     if (st != JV_OK) return st;
-    const float *h[3] = {ox, oy, oz};
-    for (int q = 0; q < 3 && per; q++) {
-        cudaError_t e = cudaMemcpyAsync(c->d_tr + q * per, h[q], per * sizeof(float), cudaMemcpyHostToDevice,
-                                        c->eng->stream());
-        if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+    float *d = c->d_tr[0];
+    st = ret(c->eng->forward(j.shot, d, d + per, d + 2 * per));
+    if (st != JV_OK) return st;
+    return ret(c->eng->rtm_shot(j.shot, d, d + per, d + 2 * per));
+}
+
+static void worker_main(jv_ctx *c) {
+    cudaSetDevice(c->eng->device());
+    for (;;) {
+        long long id;
+        jv_job job;
+        {
+            std::unique_lock<std::mutex> l(c->mu);
+            c->cv.wait(l, [&] { return c->stop || !c->queue.empty(); });
+            if (c->queue.empty()) return;  // stop requested, nothing left
+            id = c->queue.front();
+            c->queue.pop_front();
+            JobRec &r = c->jobs[id];
+            r.state = JV_JOB_RUNNING;
+            job = r.job;
+            c->running = true;
+        }
+        const jv_status st = run_job(c, job);
+        const std::string msg = st == JV_OK ? std::string() : g_err;
+        {
+            std::lock_guard<std::mutex> l(c->mu);
+            JobRec &r = c->jobs[id];
+            r.state = JV_JOB_DONE;
+            r.result = st;
+            r.msg = msg;
+            c->running = false;
+        }
+        c->done_cv.notify_all();
     }
-    return jv_rtm_shot_device(c, shot, c->d_tr, c->d_tr + per, c->d_tr + 2 * per);
+}
+
+jv_status jv_submit(jv_ctx *c, const jv_job *job, long long *id) {
+    if (!c || !job || !id) return fail(JV_EINVAL, "jv_submit: NULL argument");
+    if (job->kind != JV_JOB_FORWARD && job->kind != JV_JOB_RTM) return fail(JV_EINVAL, "unknown job kind");
+    jv_info inf;
+    c->eng->info(&inf);
+    if (job->shot < 0 || job->shot >= inf.n_shot) return fail(JV_EINVAL, "shot index out of range");
+    {
+        std::lock_guard<std::mutex> l(c->mu);
+        if (c->stop) return fail(JV_ESTATE, "context is closing");
+        *id = c->next_id++;
+        JobRec r;
+        r.job = *job;
+        c->jobs[*id] = r;
+        c->queue.push_back(*id);
+        if (!c->worker.joinable()) c->worker = std::thread(worker_main, c);
+    }
+    c->cv.notify_one();
+    g_err.clear();
+    return JV_OK;
+}
+
+jv_status jv_poll(jv_ctx *c, long long id, int *state, jv_status *result) {
+    if (!c || !state) return fail(JV_EINVAL, "jv_poll: NULL argument");
+    std::lock_guard<std::mutex> l(c->mu);
+    auto it = c->jobs.find(id);
+    if (it == c->jobs.end()) return fail(JV_EINVAL, "no such job");
+    *state = it->second.state;
+    if (result) *result = it->second.result;
+    g_err = it->second.msg;
+    return JV_OK;
+}
+
+jv_status jv_wait(jv_ctx *c, long long id, double timeout_s, jv_status *result) {
+    if (!c) return fail(JV_EINVAL, "jv_wait: NULL context");
+    std::unique_lock<std::mutex> l(c->mu);
+    auto it = c->jobs.find(id);
+    if (it == c->jobs.end()) return fail(JV_EINVAL, "no such job");
+    auto ended = [&] { return it->second.state == JV_JOB_DONE || it->second.state == JV_JOB_CANCELLED; };
+    if (timeout_s < 0) {
+        c->done_cv.wait(l, ended);
+    } else if (!c->done_cv.wait_for(l, std::chrono::duration<double>(timeout_s), ended)) {
+        g_err = "job still " + std::string(it->second.state == JV_JOB_RUNNING ? "running" : "queued");
+        return JV_ETIMEOUT;
+    }
+    if (result) *result = it->second.result;
+    g_err = it->second.msg;
+    return JV_OK;
+}
+
+jv_status jv_cancel(jv_ctx *c, long long id) {
+    if (!c) return fail(JV_EINVAL, "jv_cancel: NULL context");
+    {
+        std::lock_guard<std::mutex> l(c->mu);
+        auto it = c->jobs.find(id);
+        if (it == c->jobs.end()) return fail(JV_EINVAL, "no such job");
+        if (it->second.state != JV_JOB_QUEUED) return fail(JV_ESTATE, "job has already started");
+        for (auto q = c->queue.begin(); q != c->queue.end(); ++q)
+            if (*q == id) {
+                c->queue.erase(q);
+                break;
+            }
+        it->second.state = JV_JOB_CANCELLED;
+        it->second.result = JV_ECANCELED;
+        it->second.msg = "cancelled before it started";
+    }
+    c->done_cv.notify_all();
+    g_err.clear();
+    return JV_OK;
 }
 
 jv_status jv_image_reset(jv_ctx *c) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->image_reset());
 }
 
 jv_status jv_image_get(jv_ctx *c, int kind, double *out) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->image_get(kind, out));
 }
 
 jv_status jv_image_finalize(jv_ctx *c, float *img_pp, float *img_ps, float *img_sp, float *img_ss, float *lap_pp,
                             float *lap_ps, float *lap_sp, float *lap_ss) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     float *o[8] = {img_pp, img_ps, img_sp, img_ss, lap_pp, lap_ps, lap_sp, lap_ss};
     return ret(c->eng->image_finalize(o));
 }
 
 jv_status jv_image_get_device(jv_ctx *c, int kind, double *d_out) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->image_get_device(kind, d_out));
 }
 
 jv_status jv_image_set(jv_ctx *c, int kind, const double *in) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->image_set(kind, in, false));
 }
 
 jv_status jv_image_set_device(jv_ctx *c, int kind, const double *d_in) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->image_set(kind, d_in, true));
 }
 
 jv_status jv_set_profiling(jv_ctx *c, int on) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     c->eng->set_profiling(on != 0);
     return JV_OK;
 }
@@ -266,7 +497,7 @@ jv_status jv_profile_entry(const jv_ctx *c, int idx, const char **name, double *
 jv_status jv_run_project(jv_ctx *c) { return jv_run_project_shard(c, 0, 1, nullptr, nullptr); }
 
 jv_status jv_run_project_shard(jv_ctx *c, int rank, int world, jv_reduce_fn reduce, void *user) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     if (!c->from_project) return fail(JV_ESTATE, "jv_run_project needs a context made by jv_open");
     if (world < 1 || rank < 0 || rank >= world) return fail(JV_EINVAL, "rank must be in [0, world)");
     if (world > 1 && !reduce) return fail(JV_EINVAL, "a job of several ranks needs a reduce function");
@@ -344,7 +575,7 @@ jv_status jv_last_timing(const jv_ctx *c, double *ms) {
 }
 
 jv_status jv_sync(jv_ctx *c) {
-    if (!c) return fail(JV_EINVAL, "NULL context");
+    JV_IDLE(c);
     return ret(c->eng->sync());
 }
 

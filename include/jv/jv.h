@@ -163,6 +163,16 @@ jv_status jv_rtm_shot(jv_ctx *c, int shot, const float *obs_vx, const float *obs
 jv_status jv_rtm_shot_device(jv_ctx *c, int shot, const float *d_obs_vx, const float *d_obs_vy,
                              const float *d_obs_vz);
 
+/* Migrates n shots (indices shots[0..n-1]) and stacks them, as the
+ * per-shot loop of rtm3d_blend_model_mpi_module::mpi_sub_rtm3d does
+ * (RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:50-113).
+ * obs holds 3*n host pointers: vx, vy, vz of shot k at obs[3k..3k+2], each
+ * [n_recv][nt] float32.  The copy of shot k+1's traces to the device runs
+ * on a second stream while shot k's kernels run (page-locked host memory
+ * lets the copies overlap).  jv_last_timing gives the summed device time
+ * of the shots. */
+jv_status jv_rtm_batch(jv_ctx *c, int n, const int *shots, const float *const *obs);
+
 /* Image selectors. */
 typedef enum jv_image_kind { JV_IMG_IP = 0, JV_IMG_PP = 1, JV_IMG_PS = 2, JV_IMG_SP = 3, JV_IMG_SS = 4 } jv_image_kind;
 
@@ -216,6 +226,39 @@ typedef int (*jv_reduce_fn)(double *buf, size_t n, void *user);
  * five times, on every rank, in the same order), and rank 0 writes the
  * images.  world == 1 (reduce may be NULL) is jv_run_project. */
 jv_status jv_run_project_shard(jv_ctx *c, int rank, int world, jv_reduce_fn reduce, void *user);
+
+/* Jobs: forward modelling or migration of one shot, queued on the context
+ * and run in submission order by a worker thread of the library, so that a
+ * serving loop submits work and collects it later (jv_submit / jv_poll /
+ * jv_wait / jv_cancel).  The reference has no queue: its driver runs the
+ * shots of one job in a loop.  While jobs are queued or running, the other
+ * calls that use the context return JV_ESTATE; the job calls are safe from
+ * any thread.  Host buffers named in a job must stay valid until it ends. */
+typedef enum jv_job_kind { JV_JOB_FORWARD = 0, JV_JOB_RTM = 1 } jv_job_kind;
+typedef enum jv_job_state {
+    JV_JOB_QUEUED = 0,
+    JV_JOB_RUNNING = 1,
+    JV_JOB_DONE = 2,
+    JV_JOB_CANCELLED = 3
+} jv_job_state;
+typedef struct jv_job {
+    int kind;            /* jv_job_kind                                              */
+    int shot;            /* shot index of the context's geometry                     */
+    const float *obs[3]; /* RTM: observed vx, vy, vz traces (host, [n_recv][nt]);
+                            all NULL: the job models them on the device first         */
+    float *out[3];       /* FORWARD: traces written here (host; NULL skips one)       */
+} jv_job;
+/* Queues a copy of *job; *id identifies it in the other job calls. */
+jv_status jv_submit(jv_ctx *c, const jv_job *job, long long *id);
+/* Non-blocking: *state (jv_job_state) and, once done, *result (may be NULL);
+ * a failed job's message becomes jv_last_error(). */
+jv_status jv_poll(jv_ctx *c, long long id, int *state, jv_status *result);
+/* Waits for the job to end, at most timeout_s seconds (< 0: no limit);
+ * returns JV_ETIMEOUT if it has not ended by then. */
+jv_status jv_wait(jv_ctx *c, long long id, double timeout_s, jv_status *result);
+/* Cancels a queued job (its result becomes JV_ECANCELED); a job that has
+ * started runs to its end (JV_ESTATE). jv_close cancels the queued ones. */
+jv_status jv_cancel(jv_ctx *c, long long id);
 
 /* Device time (ms) of the last jv_forward* / jv_rtm_shot* call, measured
  * with CUDA events around its kernels. */
