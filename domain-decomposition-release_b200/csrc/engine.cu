@@ -239,6 +239,7 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread < 0 || opt.planes_per_thread > 2 || opt.pml_planes_per_thread < 0 ||
         opt.pml_planes_per_thread > 2)
         return bad(JV_EINVAL, "planes_per_thread and pml_planes_per_thread must be 0, 1 or 2");
+    if (opt.kernel_variant < 0 || opt.kernel_variant > 3) return bad(JV_EINVAL, "kernel_variant must be 0..3");
     if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
         return bad(JV_EINVAL, "tile_gx * tile_gy must be <= 256");
     long long next = (long long)(grid.nx + 2 * grid.pml) * (grid.ny + 2 * grid.pml) * (grid.nz + 2 * grid.pml);
@@ -307,6 +308,12 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
     JV_CU(cudaMemsetAsync(p, 0, kGuard * sizeof(float), stream_));
     for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + kGuard + f * field_elems_;
+    if (kc_.variant == 3) {
+        JV_TRY(alloc(&p, sizeof(int)));
+        zm_err_ = (int *)p;
+        JV_CU(cudaMemsetAsync(zm_err_, 0, sizeof(int), stream_));
+        JV_K(k_make_wave_maps(g_, F_, lam_, mu_, zm_err_, &mapsF_));
+    }
 
     // CPML geometry: six slabs covering gridext outside gridphy and outside
     // the 2-cell outer rim; the slab table and axis tables are shared by
@@ -598,7 +605,7 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, kc_, s));
-        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s));
+        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
         JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, off, s));
         if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
@@ -607,14 +614,14 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, kc_, s));
         JV_L("vowr_pack", k_vowr(g_, F_, vowr_, st_, off, 1, 0, s));
-        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s));
+        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
         if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmRev:
         // UPDATE 1: source subtraction (fused) + backward stress, receiver
         // injection + reverse velocity, stress boundary layers of step it-1
         JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, off, s));
-        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, off, kc_, s));
+        JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
         JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
         JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
@@ -622,7 +629,7 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // reverse stress, velocity boundary layers of step it-1
         JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
         JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
-        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s));
+        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsR_));
         JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 1, s));
         if (advance) JV_L("step_advance", k_step_advance(st_, -1, s));
         break;
@@ -701,6 +708,7 @@ Status Engine::forward(int shot, float *d_vx, float *d_vy, float *d_vz) {
     JV_CU(cudaEventRecord(ev1_, stream_));
     JV_CU(cudaEventSynchronize(ev1_));
     JV_CU(cudaGetLastError());
+    JV_TRY(check_zm_err());
     float ms = 0.f;
     JV_CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
     last_ms_ = ms;
@@ -718,6 +726,7 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
         JV_CU(cudaMemsetAsync(p, 0, kGuard * sizeof(float), stream_));
         for (int f = 0; f < kNumFld; f++) R_.f[f] = (float *)p + kGuard + f * field_elems_;
+        if (kc_.variant == 3) JV_K(k_make_wave_maps(g_, R_, lam_, mu_, zm_err_, &mapsR_));
         JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
         cpR_ = make_cpml((float *)p);
     }
@@ -762,6 +771,7 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
     JV_CU(cudaEventRecord(ev1_, stream_));
     JV_CU(cudaEventSynchronize(ev1_));
     JV_CU(cudaGetLastError());
+    JV_TRY(check_zm_err());
     float ms = 0.f;
     JV_CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
     last_ms_ = ms;
@@ -825,6 +835,17 @@ Status Engine::image_set(int kind, const double *src, bool src_on_device) {
 Status Engine::wait_event(cudaEvent_t e) {
     JV_CU(cudaSetDevice(dev_));
     JV_CU(cudaStreamWaitEvent(stream_, e, 0));
+    return Status{};
+}
+
+Status Engine::check_zm_err() {
+    if (!zm_err_) return Status{};
+    int h = 0;
+    JV_CU(cudaMemcpy(&h, zm_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        JV_CU(cudaMemset(zm_err_, 0, sizeof(int)));
+        return bad(JV_ETIMEOUT, "a shared-memory tile of the z-marching stress kernel did not arrive in time");
+    }
     return Status{};
 }
 

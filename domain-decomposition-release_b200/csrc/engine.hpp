@@ -110,6 +110,9 @@ class Engine {
 
     GridDev g_{};
     KCfg kc_{};
+    WaveMaps mapsF_{}, mapsR_{};  // TMA descriptors of the velocity fields (variant 3)
+    int *zm_err_ = nullptr;       // device flag of variant 3's bounded waits
+    Status check_zm_err();
     size_t field_elems_ = 0;  // elements per pitched field
     std::vector<void *> allocs_;
     size_t dev_bytes_ = 0;

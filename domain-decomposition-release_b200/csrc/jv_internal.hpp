@@ -107,6 +107,28 @@ struct StepState {
     const float *obs[3]; // traces injected into the receiver wavefield
 };
 
+// TMA descriptor of one field array (a CUtensorMap, opaque outside
+// kernels.cu): the pitched gridext array as a 3-D tensor, boxes of one
+// plane of a row tile with its x/y halo.
+struct alignas(64) FieldMap {
+    unsigned char bytes[128];
+};
+// Descriptors for the z-marching stress kernel (variant 3) of one
+// wavefield: planes of vx, vy, vz with their x/y halo, and core tiles (the
+// tile's cells only) of vx, vy, vz, lam, mu and the seven stress fields;
+// and its launch facts.
+constexpr int kZmCore = 12;  // vx vy vz lam mu sxx syy szz sxy sxz syz sau
+struct WaveMaps {
+    FieldMap halo[3];
+    FieldMap core[kZmCore];
+    bool ok = false; // false: variant 3 is not available for this grid
+    int rows = 0;    // rows of a tile
+    int boxw = 0, boxh = 0;  // halo box
+    int corew = 0;           // core box width (rows = `rows`)
+    int nsm = 0;     // CTAs of the persistent grid
+    int *err = nullptr;  // device flag: a bounded wait in the kernel ran out
+};
+
 // interior-kernel choice: variant 0 = one z plane per block, 1 = z-marching
 // over chunks of zchunk planes (0: the whole column)
 struct KCfg {
@@ -129,7 +151,13 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 // it_off: the kernels of a step read the time step as st->it + it_off (a
 // captured chunk of steps advances st->it once, at its end)
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,
-                 int rec_w, const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream);
+                 int rec_w, const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream,
+                 const WaveMaps *maps = nullptr);
+// Builds the TMA descriptors of w's velocity fields for variant 3 (leaves
+// maps->ok false when the grid does not suit it: more than 248 cells in x
+// or the driver entry point missing).  Returns a cudaError_t.
+int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
+                     WaveMaps *maps);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
               const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,

@@ -12,9 +12,13 @@
 //   damping profile     FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620
 //   receivers           FD/fdtd3d_0_base_module/fdtd3d_base_4_seisrecord_meat.hpp:57-107
 //   imaging             RTM/rtm3d_0_image_module/rtm3d_iamge_kernel.hpp:6-51,118-135,184-200
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
+#include <cstring>
 
 #include "jv_internal.hpp"
 
@@ -771,6 +775,240 @@ __global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w,
     }
 }
 
+// ------------------------------------------ z-marching stress (variant 3)
+//
+// One CTA per SM, persistent.  The (row tile, plane) items of gridphy are
+// split evenly over the CTAs; a CTA marches its items in z, one cell per
+// thread (tile = all px cells of kZmRows rows).  Everything an item reads
+// comes through TMA (cp.async.bulk.tensor), two items ahead, into a double
+// buffer: the planes of vx, vy, vz with a 4-cell x/y halo (x/y stencils),
+// and core tiles of lam, mu, the stress values and the vx, vy, vz plane
+// five above (the entry that the register window of z stencils takes in
+// next).  Threads read only shared memory and registers, and store the
+// updated stress straight to global memory.  Every wait on a TMA barrier is
+// bounded: when it runs out the CTA sets *err and stops.
+
+constexpr int kZmRows = 4;
+constexpr int kZmHalo = 4;
+constexpr int kZmMaxThreads = 800;  // px * kZmRows; the register budget is set for this block size
+
+// the descriptors of one launch, passed as one kernel parameter
+struct ZmMaps {
+    CUtensorMap halo[3];
+    CUtensorMap core[kZmCore];
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// true when the phase with this parity has completed, false after ~1 s
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > 2000000000LL) return false;
+    }
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+// floats of one halo plane / one core tile in shared memory (whole 128-byte lines)
+__host__ __device__ __forceinline__ int zm_hb(int boxw, int boxh) { return (boxw * boxh + 31) / 32 * 32; }
+__host__ __device__ __forceinline__ int zm_cb(int corew) { return (corew * kZmRows + 31) / 32 * 32; }
+
+template <int MODE>
+__global__ void __launch_bounds__(kZmMaxThreads, 1)
+    stress_zm3(GridDev g, const __grid_constant__ ZmMaps maps, WaveDev w, float dt, int rec_w,
+               const float *__restrict__ wavelet, const StepState *__restrict__ st, int it_off, int boxw, int boxh,
+               int corew, int ytiles, int *err) {
+    constexpr int NC = (MODE == kFwd) ? kZmCore - 1 : kZmCore;  // sau is not read in forward modelling
+    extern __shared__ __align__(128) float sm[];
+    const int hb = zm_hb(boxw, boxh), cb = zm_cb(corew);
+    const int stage = 3 * hb + kZmCore * cb;
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_abort;
+    const int total = ytiles * g.pz;
+    const int w0 = (int)((long long)total * blockIdx.x / gridDim.x);
+    const int w1 = (int)((long long)total * (blockIdx.x + 1) / gridDim.x);
+    if (w0 >= w1) return;
+    const int tid = threadIdx.x;
+    const int r = tid / g.px, x = tid - r * g.px;
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const uint32_t bytes_all = (uint32_t)(3 * boxw * boxh + NC * corew * kZmRows) * 4u;
+    const uint32_t bytes_feed = (uint32_t)(3 * corew * kZmRows) * 4u;  // the window feed's share
+    const int m = g.m;
+    const int XH = (int)g.xoff + m - kZmHalo;  // TMA x of the halo box (a multiple of 4)
+    const int XC = (int)g.xoff + m;            // TMA x of the core box (a multiple of 32)
+    auto issue = [&](int item, int b) {
+        const int yt = item / g.pz, z = item - yt * g.pz;
+        const uint32_t bar = b ? bar1 : bar0;
+        const int Y = m + yt * kZmRows, Z = m + z;
+        float *base = sm + b * stage;
+        // the window's next entry: vx, vy, vz five planes above; it exists
+        // inside gridext except for the last plane when pml is 4, where
+        // the run ends and nothing is fetched
+        const bool feed = Z + 5 < g.nz;
+        mbar_expect(bar, feed ? bytes_all : bytes_all - bytes_feed);
+        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], XH, Y - kZmHalo, Z, bar);
+        if (feed)
+            for (int f = 0; f < 3; f++)
+                tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], XC, Y, Z + 5, bar);
+        for (int f = 3; f < NC; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], XC, Y, Z, bar);
+    };
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar1, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        issue(w0, 0);
+        if (w0 + 1 < w1) issue(w0 + 1, 1);
+    }
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    const float *cx = c_list[(MODE == kBwd) ? rim_order(x, g.px, rec_w) : kPhyHalf];
+    float rv[3][9];  // z window: planes z-4 .. z+4 of vx, vy, vz
+    const float *fv[3] = {w.f[VX], w.f[VY], w.f[VZ]};
+    int cur_yt = -1, cur_z = -2;
+    for (int k = w0; k < w1; k++) {
+        const int yt = k / g.pz, z = k - yt * g.pz;
+        const int y = yt * kZmRows + r;
+        const bool live = y < g.py;
+        const int i0 = (int)g.xoff + (x + m) + sy * (y + m) + sz * (z + m);
+        const int b = (k - w0) & 1;
+        const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
+        const float *base = sm + b * stage;
+        const int cc = r * corew + x;  // the cell in a core tile
+        if (yt != cur_yt || z != cur_z + 1) {
+            // a new run of planes: fill the z window from global memory
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+#pragma unroll
+                for (int q = 0; q < 9; q++) rv[f][q] = live ? __ldg(fv[f] + i0 + (q - 4) * sz) : 0.f;
+            }
+        }
+        cur_yt = yt;
+        cur_z = z;
+        if (!mbar_wait_bounded(b ? bar1 : bar0, parity)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+        }
+        if (live) {
+            const float *V = base, *U = base + hb, *Wz = base + 2 * hb;
+            const float *P = base + 3 * hb;  // core tiles
+            const int c0 = (r + kZmHalo) * boxw + (x + kZmHalo);
+            const float *cy = c_list[(MODE == kBwd) ? rim_order(y, g.py, rec_w) : kPhyHalf];
+            const float *cz = c_list[(MODE == kBwd) ? rim_order(z, g.pz, rec_w) : kPhyHalf];
+            float t, Nx, Ny, Nz, Sxy, Sxz, Syz;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cx[q] * (V[c0 + q] - V[c0 - q - 1]);
+            Nx = t * rdx;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cy[q] * (V[c0 + (q + 1) * boxw] - V[c0 - q * boxw]);
+            Sxy = t * rdy;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cz[q] * (rv[0][4 + q + 1] - rv[0][4 - q]);
+            Sxz = t * rdz;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cx[q] * (U[c0 + q + 1] - U[c0 - q]);
+            Sxy += t * rdx;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cy[q] * (U[c0 + q * boxw] - U[c0 - (q + 1) * boxw]);
+            Ny = t * rdy;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cz[q] * (rv[1][4 + q + 1] - rv[1][4 - q]);
+            Syz = t * rdz;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cx[q] * (Wz[c0 + q + 1] - Wz[c0 - q]);
+            Sxz += t * rdx;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cy[q] * (Wz[c0 + (q + 1) * boxw] - Wz[c0 - q * boxw]);
+            Syz += t * rdy;
+            t = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; q++) t += cz[q] * (rv[2][4 + q] - rv[2][4 - q - 1]);
+            Nz = t * rdz;
+            const float l = P[3 * cb + cc], mm = P[4 * cb + cc];
+            float sxx = P[5 * cb + cc], syy = P[6 * cb + cc], szz = P[7 * cb + cc];
+            if (MODE != kRev) {
+                // explosive source, applied before the stress update of step it
+                if ((long long)i0 == st->src) {
+                    const float w0v = wavelet[st->it + it_off];
+                    const float sv = (MODE == kBwd) ? -w0v : w0v;
+                    sxx += sv;
+                    syy += sv;
+                    szz += sv;
+                }
+            }
+            const float l2m = l + 2.0f * mm;
+            sxx += dt * (l2m * Nx + l * Ny + l * Nz);
+            syy += dt * (l * Nx + l2m * Ny + l * Nz);
+            szz += dt * (l * Nx + l * Ny + l2m * Nz);
+            w.f[SXX][i0] = sxx;
+            w.f[SYY][i0] = syy;
+            w.f[SZZ][i0] = szz;
+            w.f[SXY][i0] = P[8 * cb + cc] + dt * mm * Sxy;
+            w.f[SXZ][i0] = P[9 * cb + cc] + dt * mm * Sxz;
+            w.f[SYZ][i0] = P[10 * cb + cc] + dt * mm * Syz;
+            if (MODE != kFwd) w.f[SAU][i0] = P[11 * cb + cc] + dt * (l + 2.0f * mm) * (Nx + Ny + Nz);
+            // advance the z window: the plane five above came in with this item
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+#pragma unroll
+                for (int q = 0; q < 8; q++) rv[f][q] = rv[f][q + 1];
+                rv[f][8] = P[f * cb + cc];
+            }
+        }
+        __syncthreads();  // every thread is done with buffer b
+        if (s_abort) {
+            // stop issuing; give the copies still in flight (this item's and
+            // the next one's) a bounded time to land before the CTA leaves
+            if (tid == 0) {
+                mbar_wait_bounded(b ? bar1 : bar0, parity);
+                if (k + 1 < w1) {
+                    const int k1 = k + 1 - w0;
+                    mbar_wait_bounded((k1 & 1) ? bar1 : bar0, (uint32_t)((k1 >> 1) & 1));
+                }
+            }
+            __syncthreads();
+            return;
+        }
+        if (tid == 0 && k + 2 < w1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(k + 2, b);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- CPML
 
 // Damping coefficients of one absorbing axis at one cell
@@ -1307,7 +1545,7 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
     cudaStream_t s = (cudaStream_t)stream;
     WaveDev rv = rev ? *rev : WaveDev{};
     ImageDev im = img ? *img : ImageDev{};
-    if (kc.variant == 2) {
+    if (kc.variant == 2 || kc.variant == 3) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
         if (kc.zp == 2) {
@@ -1346,10 +1584,98 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
     return cerr();
 }
 
+// dynamic shared memory of stress_zm3: two stages of three halo planes and the core tiles
+static size_t zm3_smem(int boxw, int boxh, int corew) {
+    return (size_t)2 * (3 * zm_hb(boxw, boxh) + kZmCore * zm_cb(corew)) * sizeof(float);
+}
+
+int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
+                     WaveMaps *maps) {
+    maps->ok = false;
+    const int pxr = (g.px + 3) / 4 * 4;
+    const int boxw = pxr + 2 * kZmHalo, boxh = kZmRows + 2 * kZmHalo;
+    if (g.px * kZmRows > kZmMaxThreads || boxw > 256) return 0;  // the tile would not fit one CTA / one TMA box
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return 0;
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    static_assert(sizeof(CUtensorMap) == sizeof(FieldMap), "descriptor size");
+    // the pitched gridext array as a 3-D tensor; box (bw, bh, 1)
+    auto make = [&](const float *base, int bw, int bh, FieldMap *out) -> bool {
+        CUtensorMap tm;
+        const cuuint64_t dims[3] = {(cuuint64_t)g.sy, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(float), (cuuint64_t)g.sz * sizeof(float)};
+        const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        CUresult r = encode(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+        std::memcpy(out->bytes, &tm, sizeof(tm));
+        return true;
+    };
+    const int vel[3] = {VX, VY, VZ};
+    for (int f = 0; f < 3; f++)
+        if (!make(w.f[vel[f]], boxw, boxh, &maps->halo[f]) || !make(w.f[vel[f]], pxr, kZmRows, &maps->core[f]))
+            return 0;
+    const float *pts[kZmCore - 3] = {lam, mu, w.f[SXX], w.f[SYY], w.f[SZZ], w.f[SXY], w.f[SXZ], w.f[SYZ], w.f[SAU]};
+    for (int f = 0; f < kZmCore - 3; f++)
+        if (!make(pts[f], pxr, kZmRows, &maps->core[3 + f])) return 0;
+    const size_t smem = zm3_smem(boxw, boxh, pxr);
+    cudaError_t e = cudaFuncSetAttribute(stress_zm3<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress_zm3<kRtmFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress_zm3<kBwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress_zm3<kRev>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return (int)e;
+    maps->rows = kZmRows;
+    maps->boxw = boxw;
+    maps->boxh = boxh;
+    maps->corew = pxr;
+    maps->nsm = nsm;
+    maps->err = err_flag;
+    maps->ok = true;
+    return 0;
+}
+
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt, int rec_w,
-                 const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream) {
+                 const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream,
+                 const WaveMaps *maps) {
     cudaStream_t s = (cudaStream_t)stream;
-    if (kc.variant == 2) {
+    if (kc.variant == 3 && maps && maps->ok) {
+        ZmMaps zm;
+        static_assert(sizeof(ZmMaps) == sizeof(maps->halo) + sizeof(maps->core), "descriptor layout");
+        std::memcpy(zm.halo, maps->halo, sizeof(maps->halo));
+        std::memcpy(zm.core, maps->core, sizeof(maps->core));
+        const int ytiles = (g.py + maps->rows - 1) / maps->rows;
+        const long long items = (long long)ytiles * g.pz;
+        const int grid = (int)std::min<long long>(maps->nsm, items);
+        const dim3 b(g.px * maps->rows);
+        const size_t smem = zm3_smem(maps->boxw, maps->boxh, maps->corew);
+        switch (mode) {
+#define JV_ZM3(M)                                                                                              \
+    stress_zm3<M><<<grid, b, smem, s>>>(g, zm, w, dt, rec_w, wavelet, st, it_off, maps->boxw, maps->boxh,      \
+                                        maps->corew, ytiles, maps->err)
+        case kFwd: JV_ZM3(kFwd); break;
+        case kRtmFwd: JV_ZM3(kRtmFwd); break;
+        case kBwd: JV_ZM3(kBwd); break;
+        case kRev: JV_ZM3(kRev); break;
+#undef JV_ZM3
+        default: return (int)cudaErrorInvalidValue;
+        }
+        return cerr();
+    }
+    if (kc.variant == 2 || kc.variant == 3) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
         if (kc.zp == 2) {

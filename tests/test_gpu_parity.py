@@ -33,7 +33,7 @@ SMALL = [
 ]
 
 
-VARIANTS = [0, 1, 2]  # interior kernels: one plane per block, z-marching, x-vectorised
+VARIANTS = [0, 1, 2, 3]  # interior kernels: one plane per block, z-marching, x-vectorised, + TMA z-march stress
 
 
 @pytest.mark.parametrize("kw", SMALL)
