@@ -132,7 +132,7 @@ struct WaveMaps {
 // interior-kernel choice: variant 0 = one z plane per block, 1 = z-marching
 // over chunks of zchunk planes (0: the whole column)
 struct KCfg {
-    int variant = 2;
+    int variant = 3;
     int zchunk = 0;
     int gx = 0, gy = 0;  // variant 2 block: x groups per block, rows per block (0: auto)
     int minb = 4;        // variant 2: blocks per SM the register budget is set for (3 or 4)

@@ -831,19 +831,24 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
-// floats of one halo plane / one core tile in shared memory (whole 128-byte lines)
-__host__ __device__ __forceinline__ int zm_hb(int boxw, int boxh) { return (boxw * boxh + 31) / 32 * 32; }
-__host__ __device__ __forceinline__ int zm_cb(int corew) { return (corew * kZmRows + 31) / 32 * 32; }
+// Shared-memory geometry, fixed so that stencil offsets are immediates:
+// a halo plane is a 256-float-wide box (row pitch 256) of kZmRows + 8 rows;
+// a core tile (px rounded up to 4 wide, dense rows) sits in a region of
+// kZmRows * 256 floats.
+constexpr int kZmPitch = 256;
+constexpr int kZmBoxH = kZmRows + 2 * kZmHalo;
+constexpr int kZmHB = kZmPitch * kZmBoxH;  // floats of one halo plane
+constexpr int kZmCB = kZmPitch * kZmRows;  // floats of one core-tile region
+constexpr int kZmStage = 3 * kZmHB + kZmCore * kZmCB;
 
 template <int MODE>
 __global__ void __launch_bounds__(kZmMaxThreads, 1)
     stress_zm3(GridDev g, const __grid_constant__ ZmMaps maps, WaveDev w, float dt, int rec_w,
-               const float *__restrict__ wavelet, const StepState *__restrict__ st, int it_off, int boxw, int boxh,
-               int corew, int ytiles, int *err) {
+               const float *__restrict__ wavelet, const StepState *__restrict__ st, int it_off, int corew,
+               int ytiles, int *err) {
     constexpr int NC = (MODE == kFwd) ? kZmCore - 1 : kZmCore;  // sau is not read in forward modelling
     extern __shared__ __align__(128) float sm[];
-    const int hb = zm_hb(boxw, boxh), cb = zm_cb(corew);
-    const int stage = 3 * hb + kZmCore * cb;
+    constexpr int hb = kZmHB, cb = kZmCB, stage = kZmStage, boxw = kZmPitch;
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_abort;
     const int total = ytiles * g.pz;
@@ -853,7 +858,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     const int tid = threadIdx.x;
     const int r = tid / g.px, x = tid - r * g.px;
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
-    const uint32_t bytes_all = (uint32_t)(3 * boxw * boxh + NC * corew * kZmRows) * 4u;
+    const uint32_t bytes_all = (uint32_t)(3 * kZmHB + NC * corew * kZmRows) * 4u;
     const uint32_t bytes_feed = (uint32_t)(3 * corew * kZmRows) * 4u;  // the window feed's share
     const int m = g.m;
     const int XH = (int)g.xoff + m - kZmHalo;  // TMA x of the halo box (a multiple of 4)
@@ -1585,16 +1590,15 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 }
 
 // dynamic shared memory of stress_zm3: two stages of three halo planes and the core tiles
-static size_t zm3_smem(int boxw, int boxh, int corew) {
-    return (size_t)2 * (3 * zm_hb(boxw, boxh) + kZmCore * zm_cb(corew)) * sizeof(float);
-}
+static size_t zm3_smem() { return (size_t)2 * kZmStage * sizeof(float); }
 
 int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
                      WaveMaps *maps) {
     maps->ok = false;
     const int pxr = (g.px + 3) / 4 * 4;
-    const int boxw = pxr + 2 * kZmHalo, boxh = kZmRows + 2 * kZmHalo;
-    if (g.px * kZmRows > kZmMaxThreads || boxw > 256) return 0;  // the tile would not fit one CTA / one TMA box
+    const int boxw = kZmPitch, boxh = kZmBoxH;
+    // the tile must fit one CTA, and a row with its halo one box
+    if (g.px * kZmRows > kZmMaxThreads || pxr + 2 * kZmHalo > kZmPitch) return 0;
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -1625,7 +1629,7 @@ int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     const float *pts[kZmCore - 3] = {lam, mu, w.f[SXX], w.f[SYY], w.f[SZZ], w.f[SXY], w.f[SXZ], w.f[SYZ], w.f[SAU]};
     for (int f = 0; f < kZmCore - 3; f++)
         if (!make(pts[f], pxr, kZmRows, &maps->core[3 + f])) return 0;
-    const size_t smem = zm3_smem(boxw, boxh, pxr);
+    const size_t smem = zm3_smem();
     cudaError_t e = cudaFuncSetAttribute(stress_zm3<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(stress_zm3<kRtmFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1661,11 +1665,10 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
         const long long items = (long long)ytiles * g.pz;
         const int grid = (int)std::min<long long>(maps->nsm, items);
         const dim3 b(g.px * maps->rows);
-        const size_t smem = zm3_smem(maps->boxw, maps->boxh, maps->corew);
+        const size_t smem = zm3_smem();
         switch (mode) {
 #define JV_ZM3(M)                                                                                              \
-    stress_zm3<M><<<grid, b, smem, s>>>(g, zm, w, dt, rec_w, wavelet, st, it_off, maps->boxw, maps->boxh,      \
-                                        maps->corew, ytiles, maps->err)
+    stress_zm3<M><<<grid, b, smem, s>>>(g, zm, w, dt, rec_w, wavelet, st, it_off, maps->corew, ytiles, maps->err)
         case kFwd: JV_ZM3(kFwd); break;
         case kRtmFwd: JV_ZM3(kRtmFwd); break;
         case kBwd: JV_ZM3(kBwd); break;
