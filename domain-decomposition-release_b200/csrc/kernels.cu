@@ -778,8 +778,9 @@ __global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w,
 // ------------------------------------------ z-marching stress (variant 3)
 //
 // One CTA per SM, persistent.  The (row tile, plane) items of gridphy are
-// split evenly over the CTAs; a CTA marches its items in z, one cell per
-// thread (tile = all px cells of kZmRows rows).  Everything an item reads
+// split evenly over the CTAs; a CTA marches its items in z, one pair of
+// x cells per thread (tile = all px cells of kZmRows rows, float2 shared-
+// memory and global accesses).  Everything an item reads
 // comes through TMA (cp.async.bulk.tensor), two items ahead, into a double
 // buffer: the planes of vx, vy, vz with a 4-cell x/y halo (x/y stencils),
 // and core tiles of lam, mu, the stress values and the vx, vy, vz plane
@@ -790,7 +791,8 @@ __global__ void __launch_bounds__(256, MINB) stress_phy_v4(GridDev g, WaveDev w,
 
 constexpr int kZmRows = 4;
 constexpr int kZmHalo = 4;
-constexpr int kZmMaxThreads = 800;  // px * kZmRows; the register budget is set for this block size
+constexpr int kZmCPT = 2;           // cells per thread (an x pair, float2 accesses)
+constexpr int kZmMaxThreads = 512;  // ceil(px / 2) * kZmRows; the register budget is set for this block size
 
 // the descriptors of one launch, passed as one kernel parameter
 struct ZmMaps {
@@ -856,7 +858,9 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     const int w1 = (int)((long long)total * (blockIdx.x + 1) / gridDim.x);
     if (w0 >= w1) return;
     const int tid = threadIdx.x;
-    const int r = tid / g.px, x = tid - r * g.px;
+    const int hx = (g.px + 1) / 2;               // x pairs of a row
+    const int r = tid / hx, x = 2 * (tid - r * hx);
+    const int nval = min(kZmCPT, g.px - x);      // 1 for the last pair of an odd row
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     const uint32_t bytes_all = (uint32_t)(3 * kZmHB + NC * corew * kZmRows) * 4u;
     const uint32_t bytes_feed = (uint32_t)(3 * corew * kZmRows) * 4u;  // the window feed's share
@@ -892,25 +896,28 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     }
     const int sy = (int)g.sy, sz = (int)g.sz;
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    const float *cx = c_list[(MODE == kBwd) ? rim_order(x, g.px, rec_w) : kPhyHalf];
-    float rv[3][9];  // z window: planes z-4 .. z+4 of vx, vy, vz
+    const float *cx[2] = {c_list[(MODE == kBwd) ? rim_order(x, g.px, rec_w) : kPhyHalf],
+                          c_list[(MODE == kBwd) ? rim_order(min(x + 1, g.px - 1), g.px, rec_w) : kPhyHalf]};
+    float2 rv[3][9];  // z windows of the pair: planes z-4 .. z+4 of vx, vy, vz
     const float *fv[3] = {w.f[VX], w.f[VY], w.f[VZ]};
     int cur_yt = -1, cur_z = -2;
     for (int k = w0; k < w1; k++) {
         const int yt = k / g.pz, z = k - yt * g.pz;
         const int y = yt * kZmRows + r;
         const bool live = y < g.py;
-        const int i0 = (int)g.xoff + (x + m) + sy * (y + m) + sz * (z + m);
+        const int i0 = (int)g.xoff + (x + m) + sy * (y + m) + sz * (z + m);  // even: float2-aligned
         const int b = (k - w0) & 1;
         const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
         const float *base = sm + b * stage;
-        const int cc = r * corew + x;  // the cell in a core tile
+        const int cc = r * corew + x;  // the pair in a core tile
         if (yt != cur_yt || z != cur_z + 1) {
-            // a new run of planes: fill the z window from global memory
+            // a new run of planes: fill the z windows from global memory
 #pragma unroll
             for (int f = 0; f < 3; f++) {
 #pragma unroll
-                for (int q = 0; q < 9; q++) rv[f][q] = live ? __ldg(fv[f] + i0 + (q - 4) * sz) : 0.f;
+                for (int q = 0; q < 9; q++)
+                    rv[f][q] = live ? __ldg(reinterpret_cast<const float2 *>(fv[f] + i0 + (q - 4) * sz))
+                                    : make_float2(0.f, 0.f);
             }
         }
         cur_yt = yt;
@@ -920,77 +927,156 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
             atomicExch(err, 1);
         }
         if (live) {
-            const float *V = base, *U = base + hb, *Wz = base + 2 * hb;
             const float *P = base + 3 * hb;  // core tiles
             const int c0 = (r + kZmHalo) * boxw + (x + kZmHalo);
             const float *cy = c_list[(MODE == kBwd) ? rim_order(y, g.py, rec_w) : kPhyHalf];
             const float *cz = c_list[(MODE == kBwd) ? rim_order(z, g.pz, rec_w) : kPhyHalf];
-            float t, Nx, Ny, Nz, Sxy, Sxz, Syz;
-            t = 0.f;
+            // x window of a field around the pair: e[j] = f[x - 4 + j], j = 0..9
+            auto xwin2 = [&](const float *F, float *e) {
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cx[q] * (V[c0 + q] - V[c0 - q - 1]);
-            Nx = t * rdx;
-            t = 0.f;
+                for (int j = 0; j < 5; j++) {
+                    const float2 v = *reinterpret_cast<const float2 *>(F + c0 - 4 + 2 * j);
+                    e[2 * j] = v.x;
+                    e[2 * j + 1] = v.y;
+                }
+            };
+            auto ld2 = [&](const float *F, int off) { return *reinterpret_cast<const float2 *>(F + off); };
+            float e[10];
+            float Nx[2], Ny[2], Nz[2], Sxy[2], Sxz[2], Syz[2];
+            // vx: Dm_x -> Nx, Dp_y -> Sxy, Dp_z -> Sxz
+            xwin2(base, e);
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cy[q] * (V[c0 + (q + 1) * boxw] - V[c0 - q * boxw]);
-            Sxy = t * rdy;
-            t = 0.f;
+            for (int c = 0; c < 2; c++) {
+                float t = 0.f;
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cz[q] * (rv[0][4 + q + 1] - rv[0][4 - q]);
-            Sxz = t * rdz;
-            t = 0.f;
+                for (int q = 0; q < 4; q++) t += cx[c][q] * (e[4 + c + q] - e[4 + c - q - 1]);
+                Nx[c] = t * rdx;
+            }
+            {
+                float2 t = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cx[q] * (U[c0 + q + 1] - U[c0 - q]);
-            Sxy += t * rdx;
-            t = 0.f;
+                for (int q = 0; q < 4; q++) {
+                    const float2 a = ld2(base, c0 + (q + 1) * boxw), bb = ld2(base, c0 - q * boxw);
+                    t.x += cy[q] * (a.x - bb.x);
+                    t.y += cy[q] * (a.y - bb.y);
+                }
+                Sxy[0] = t.x * rdy;
+                Sxy[1] = t.y * rdy;
+                t = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cy[q] * (U[c0 + q * boxw] - U[c0 - (q + 1) * boxw]);
-            Ny = t * rdy;
-            t = 0.f;
+                for (int q = 0; q < 4; q++) {
+                    t.x += cz[q] * (rv[0][4 + q + 1].x - rv[0][4 - q].x);
+                    t.y += cz[q] * (rv[0][4 + q + 1].y - rv[0][4 - q].y);
+                }
+                Sxz[0] = t.x * rdz;
+                Sxz[1] = t.y * rdz;
+            }
+            // vy: Dp_x -> Sxy, Dm_y -> Ny, Dp_z -> Syz
+            xwin2(base + hb, e);
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cz[q] * (rv[1][4 + q + 1] - rv[1][4 - q]);
-            Syz = t * rdz;
-            t = 0.f;
+            for (int c = 0; c < 2; c++) {
+                float t = 0.f;
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cx[q] * (Wz[c0 + q + 1] - Wz[c0 - q]);
-            Sxz += t * rdx;
-            t = 0.f;
+                for (int q = 0; q < 4; q++) t += cx[c][q] * (e[4 + c + q + 1] - e[4 + c - q]);
+                Sxy[c] += t * rdx;
+            }
+            {
+                float2 t = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cy[q] * (Wz[c0 + (q + 1) * boxw] - Wz[c0 - q * boxw]);
-            Syz += t * rdy;
-            t = 0.f;
+                for (int q = 0; q < 4; q++) {
+                    const float2 a = ld2(base + hb, c0 + q * boxw), bb = ld2(base + hb, c0 - (q + 1) * boxw);
+                    t.x += cy[q] * (a.x - bb.x);
+                    t.y += cy[q] * (a.y - bb.y);
+                }
+                Ny[0] = t.x * rdy;
+                Ny[1] = t.y * rdy;
+                t = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int q = 0; q < 4; q++) t += cz[q] * (rv[2][4 + q] - rv[2][4 - q - 1]);
-            Nz = t * rdz;
-            const float l = P[3 * cb + cc], mm = P[4 * cb + cc];
-            float sxx = P[5 * cb + cc], syy = P[6 * cb + cc], szz = P[7 * cb + cc];
+                for (int q = 0; q < 4; q++) {
+                    t.x += cz[q] * (rv[1][4 + q + 1].x - rv[1][4 - q].x);
+                    t.y += cz[q] * (rv[1][4 + q + 1].y - rv[1][4 - q].y);
+                }
+                Syz[0] = t.x * rdz;
+                Syz[1] = t.y * rdz;
+            }
+            // vz: Dp_x -> Sxz, Dp_y -> Syz, Dm_z -> Nz
+            xwin2(base + 2 * hb, e);
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                float t = 0.f;
+#pragma unroll
+                for (int q = 0; q < 4; q++) t += cx[c][q] * (e[4 + c + q + 1] - e[4 + c - q]);
+                Sxz[c] += t * rdx;
+            }
+            {
+                float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float2 a = ld2(base + 2 * hb, c0 + (q + 1) * boxw), bb = ld2(base + 2 * hb, c0 - q * boxw);
+                    t.x += cy[q] * (a.x - bb.x);
+                    t.y += cy[q] * (a.y - bb.y);
+                }
+                Syz[0] += t.x * rdy;
+                Syz[1] += t.y * rdy;
+                t = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    t.x += cz[q] * (rv[2][4 + q].x - rv[2][4 - q - 1].x);
+                    t.y += cz[q] * (rv[2][4 + q].y - rv[2][4 - q - 1].y);
+                }
+                Nz[0] = t.x * rdz;
+                Nz[1] = t.y * rdz;
+            }
+            const float2 l2 = ld2(P, 3 * cb + cc), m2 = ld2(P, 4 * cb + cc);
+            const float l[2] = {l2.x, l2.y}, mm[2] = {m2.x, m2.y};
+            float2 s0 = ld2(P, 5 * cb + cc), s1 = ld2(P, 6 * cb + cc), s2 = ld2(P, 7 * cb + cc);
+            float sxx[2] = {s0.x, s0.y}, syy[2] = {s1.x, s1.y}, szz[2] = {s2.x, s2.y};
             if (MODE != kRev) {
                 // explosive source, applied before the stress update of step it
-                if ((long long)i0 == st->src) {
+                const long long d = st->src - (long long)i0;
+                if (d >= 0 && d < nval) {
                     const float w0v = wavelet[st->it + it_off];
                     const float sv = (MODE == kBwd) ? -w0v : w0v;
-                    sxx += sv;
-                    syy += sv;
-                    szz += sv;
+                    sxx[d] += sv;
+                    syy[d] += sv;
+                    szz[d] += sv;
                 }
             }
-            const float l2m = l + 2.0f * mm;
-            sxx += dt * (l2m * Nx + l * Ny + l * Nz);
-            syy += dt * (l * Nx + l2m * Ny + l * Nz);
-            szz += dt * (l * Nx + l * Ny + l2m * Nz);
-            w.f[SXX][i0] = sxx;
-            w.f[SYY][i0] = syy;
-            w.f[SZZ][i0] = szz;
-            w.f[SXY][i0] = P[8 * cb + cc] + dt * mm * Sxy;
-            w.f[SXZ][i0] = P[9 * cb + cc] + dt * mm * Sxz;
-            w.f[SYZ][i0] = P[10 * cb + cc] + dt * mm * Syz;
-            if (MODE != kFwd) w.f[SAU][i0] = P[11 * cb + cc] + dt * (l + 2.0f * mm) * (Nx + Ny + Nz);
-            // advance the z window: the plane five above came in with this item
+            float o[7][2];
+            const float2 t8 = ld2(P, 8 * cb + cc), t9 = ld2(P, 9 * cb + cc), t10 = ld2(P, 10 * cb + cc);
+            const float sxy0[2] = {t8.x, t8.y}, sxz0[2] = {t9.x, t9.y}, syz0[2] = {t10.x, t10.y};
+            float sau0[2] = {0.f, 0.f};
+            if (MODE != kFwd) {
+                const float2 t11 = ld2(P, 11 * cb + cc);
+                sau0[0] = t11.x;
+                sau0[1] = t11.y;
+            }
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const float l2m = l[c] + 2.0f * mm[c];
+                o[0][c] = sxx[c] + dt * (l2m * Nx[c] + l[c] * Ny[c] + l[c] * Nz[c]);
+                o[1][c] = syy[c] + dt * (l[c] * Nx[c] + l2m * Ny[c] + l[c] * Nz[c]);
+                o[2][c] = szz[c] + dt * (l[c] * Nx[c] + l[c] * Ny[c] + l2m * Nz[c]);
+                o[3][c] = sxy0[c] + dt * mm[c] * Sxy[c];
+                o[4][c] = sxz0[c] + dt * mm[c] * Sxz[c];
+                o[5][c] = syz0[c] + dt * mm[c] * Syz[c];
+                o[6][c] = sau0[c] + dt * (l[c] + 2.0f * mm[c]) * (Nx[c] + Ny[c] + Nz[c]);
+            }
+            const int outf[7] = {SXX, SYY, SZZ, SXY, SXZ, SYZ, SAU};
+            const int nout = (MODE != kFwd) ? 7 : 6;
+#pragma unroll
+            for (int j = 0; j < 7; j++) {
+                if (j >= nout) break;
+                float *dst = w.f[outf[j]] + i0;
+                if (nval == 2) *reinterpret_cast<float2 *>(dst) = make_float2(o[j][0], o[j][1]);
+                else dst[0] = o[j][0];
+            }
+            // advance the z windows: the plane five above came in with this item
 #pragma unroll
             for (int f = 0; f < 3; f++) {
 #pragma unroll
                 for (int q = 0; q < 8; q++) rv[f][q] = rv[f][q + 1];
-                rv[f][8] = P[f * cb + cc];
+                rv[f][8] = ld2(P, f * cb + cc);
             }
         }
         __syncthreads();  // every thread is done with buffer b
@@ -1598,7 +1684,7 @@ int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     const int pxr = (g.px + 3) / 4 * 4;
     const int boxw = kZmPitch, boxh = kZmBoxH;
     // the tile must fit one CTA, and a row with its halo one box
-    if (g.px * kZmRows > kZmMaxThreads || pxr + 2 * kZmHalo > kZmPitch) return 0;
+    if ((g.px + 1) / 2 * kZmRows > kZmMaxThreads || pxr + 2 * kZmHalo > kZmPitch) return 0;
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -1664,7 +1750,7 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
         const int ytiles = (g.py + maps->rows - 1) / maps->rows;
         const long long items = (long long)ytiles * g.pz;
         const int grid = (int)std::min<long long>(maps->nsm, items);
-        const dim3 b(g.px * maps->rows);
+        const dim3 b((g.px + 1) / 2 * maps->rows);
         const size_t smem = zm3_smem();
         switch (mode) {
 #define JV_ZM3(M)                                                                                              \
