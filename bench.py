@@ -201,6 +201,47 @@ def cpu_sample(s, oracle, seconds_target=20.0, max_steps=200):
     return {"shots_per_h": 3600.0 / sec_per_shot, "gcells": cells / dt / 1e9, "steps": steps2, "seconds": dt}
 
 
+def serve_leg(jv, synth, n_req):
+    """Heterogeneous requests through jv_server: grids of 48..112 cells per
+    axis (+10 CPML), 400 steps, forward and RTM (the RTM requests model
+    their own traces first), each with its own model and a full receiver
+    plane; host buffers in and out.  Served with 4 slots against the same
+    requests one at a time (1 slot); requests/h and p50/p99 latency from
+    the server's own statistics (submission to completion)."""
+    sizes = [48, 64, 80, 96, 112]
+    surveys = {n: synth.scaled_cfg2(n, 400, pml=10, seed=30 + n) for n in sizes}
+    plan = [(surveys[sizes[i % len(sizes)]], jv.JOB_RTM if i % 3 else jv.JOB_FORWARD) for i in range(n_req)]
+
+    with jv.Server(slots=2) as srv:  # warm-up requests (module load, allocator pools), not counted
+        for rid, _ in [srv.submit_survey(k, sv) for sv, k in plan[:2]]:
+            srv.wait(rid, timeout=300.0)
+
+    def run(slots):
+        with jv.Server(slots=slots) as srv:
+            t0 = time.perf_counter()
+            subs = [srv.submit_survey(k, sv) for sv, k in plan]
+            for rid, _ in subs:
+                if srv.wait(rid, timeout=600.0) != 0:
+                    raise RuntimeError("served request failed")
+            dt = time.perf_counter() - t0
+            st = srv.stats()
+        return dt, st
+
+    t1, st1 = run(1)
+    t4, st4 = run(4)
+    cells = sum((sv.nx + 2 * sv.pml) * (sv.ny + 2 * sv.pml) * (sv.nz + 2 * sv.pml) * sv.nt * (3 if k else 1)
+                for sv, k in plan)
+    return {"requests": n_req, "unit": "requests/h",
+            "mix": f"grids {sizes}^3 +10 CPML, nt 400, 2/3 RTM (own modelling first), 1/3 forward",
+            "slots4": round(n_req / t4 * 3600.0, 1), "slots1": round(n_req / t1 * 3600.0, 1),
+            "speedup": round(t1 / t4, 3),
+            "p50_ms": {"slots4": round(st4["p50_ms"], 1), "slots1": round(st1["p50_ms"], 1)},
+            "p99_ms": {"slots4": round(st4["p99_ms"], 1), "slots1": round(st1["p99_ms"], 1)},
+            "gcell_updates_per_s": {"slots4": round(cells / t4 / 1e9, 2), "slots1": round(cells / t1 / 1e9, 2)},
+            "note": "latency counts from submission, all requests submitted at once; two warm-up requests "
+                    "on a server of their own are not counted"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -251,6 +292,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the request-server leg")
+    ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--ref-sample-steps", type=int, default=40)
     ap.add_argument("--variant", type=int, default=None, help="interior kernel variant (default: library default)")
     args = ap.parse_args()
@@ -399,6 +442,10 @@ def main():
                  "note": "plain: one jv_rtm_shot + jv_image_finalize per shot; batched: one jv_rtm_batch of the "
                          "shots, one finalize; served: the shots as queued RTM jobs, one finalize"}
 
+    serving = None
+    if world == 1 and not args.no_serve:
+        serving = serve_leg(jv, jv.synth, args.serve_requests)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -435,7 +482,7 @@ def main():
                    "rec_width": s.rec_width, "n_recv": nrec, "mode": "plain one-shot-per-call, graph time loop",
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "clocks": clk,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "serving": serving, "clocks": clk,
         "gpu_launches": launches * args.steps if launches else None,
         "gpu_launches_note": "kernels of the timed shots, counted from one instrumented shot (graph path)",
         "wall_s": round(wall, 3),

@@ -43,6 +43,8 @@ EXPORTS = (
     "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info", "jv_forward_noalloc",
     "jv_image_set", "jv_image_set_device", "jv_run_project_shard", "jv_read_argfile", "jv_rtm_batch",
     "jv_submit", "jv_poll", "jv_wait", "jv_cancel",
+    "jv_footprint", "jv_server_create", "jv_server_submit", "jv_server_poll", "jv_server_wait", "jv_server_cancel",
+    "jv_server_get_stats", "jv_server_close",
 )
 JOB_FORWARD, JOB_RTM = 0, 1
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELLED = 0, 1, 2, 3
@@ -72,6 +74,21 @@ class Options(C.Structure):
 class Job(C.Structure):
     _fields_ = [("kind", C.c_int), ("shot", C.c_int), ("obs", C.POINTER(C.c_float) * 3),
                 ("out", C.POINTER(C.c_float) * 3)]
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_int), ("grid", Grid), ("vp", C.POINTER(C.c_float)), ("vs", C.POINTER(C.c_float)),
+                ("rho", C.POINTER(C.c_float)), ("dt", C.c_float), ("fm", C.c_float), ("nt", C.c_int),
+                ("rec_width", C.c_int), ("shot_xyz", C.c_float * 3), ("n_recv", C.c_int),
+                ("recv_xyz", C.POINTER(C.c_float)), ("obs", C.POINTER(C.c_float) * 3),
+                ("out", C.POINTER(C.c_float) * 3), ("image", C.POINTER(C.c_double) * 5)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+                ("cancelled", C.c_longlong), ("running", C.c_longlong), ("queued", C.c_longlong),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t)]
 
 
 class ArgFileC(C.Structure):
@@ -145,6 +162,14 @@ def lib() -> C.CDLL:
     L.jv_poll.argtypes = [ctxp, C.c_longlong, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.jv_wait.argtypes = [ctxp, C.c_longlong, C.c_double, C.POINTER(C.c_int)]
     L.jv_cancel.argtypes = [ctxp, C.c_longlong]
+    L.jv_footprint.argtypes = [C.POINTER(Grid), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t)]
+    L.jv_server_create.argtypes = [C.c_int, C.c_int, C.c_size_t, C.POINTER(vp)]
+    L.jv_server_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_longlong)]
+    L.jv_server_poll.argtypes = [vp, C.c_longlong, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.jv_server_wait.argtypes = [vp, C.c_longlong, C.c_double, C.POINTER(C.c_int)]
+    L.jv_server_cancel.argtypes = [vp, C.c_longlong]
+    L.jv_server_get_stats.argtypes = [vp, C.POINTER(ServerStats)]
+    L.jv_server_close.argtypes = [vp]
     L.jv_run_project_shard.argtypes = [ctxp, C.c_int, C.c_int, REDUCE_FN, C.c_void_p]
     L.jv_read_argfile.argtypes = [C.c_char_p, C.POINTER(ArgFileC)]
     L.jv_forward_noalloc.argtypes = [C.POINTER(Grid), vp, vp, vp, C.c_float, C.c_float, C.c_int, fp, C.c_int, fp,
@@ -391,3 +416,114 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def footprint(nx, ny, nz, pml, nt, rec_width=1, kind=JOB_RTM, n_recv=0) -> int:
+    """Device bytes a context holds for one request of this size (jv_footprint)."""
+    g = Grid(nx, ny, nz, pml, 1.0, 1.0, 1.0)
+    b = C.c_size_t()
+    _check(lib().jv_footprint(C.byref(g), nt, rec_width, kind, n_recv, C.byref(b)))
+    return b.value
+
+
+class Server:
+    """jv_server: requests of their own size and model, admitted into
+    `slots` concurrent workers under an HBM budget (bytes; 0 = 90 % of the
+    free device memory)."""
+
+    def __init__(self, slots: int = 4, budget: int = 0, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().jv_server_create(device, slots, budget, C.byref(h)))
+        self._h = h
+        self._refs = {}
+
+    def submit(self, kind, nx, ny, nz, pml, dx, dy, dz, vp, vs, rho, dt, fm, nt, shot_xyz, recv_xyz,
+               rec_width=1, obs=None, out=None, image=None) -> int:
+        """Queues one request.  out (FORWARD) / obs (RTM) are 3 float32
+        arrays [n_kept][nt]; image (RTM) up to 5 float64 arrays of gridphy
+        (ip, pp, ps, sp, ss; None skips one).  The arrays are kept alive here
+        until the request has been waited for."""
+        r = Request()
+        r.kind = kind
+        r.grid = Grid(nx, ny, nz, pml, dx, dy, dz)
+        refs = []
+
+        def f32(a):
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            refs.append(a)
+            return _fptr(a)
+
+        r.vp, r.vs, r.rho = f32(vp), f32(vs), f32(rho)
+        r.dt, r.fm, r.nt, r.rec_width = dt, fm, nt, rec_width
+        for q in range(3):
+            r.shot_xyz[q] = float(shot_xyz[q])
+        rv = np.ascontiguousarray(recv_xyz, dtype=np.float32).reshape(-1, 3)
+        refs.append(rv)
+        r.n_recv = rv.shape[0]
+        r.recv_xyz = _fptr(rv)
+        for q in range(3):
+            if obs is not None:
+                r.obs[q] = f32(obs[q])
+            if out is not None and out[q] is not None:
+                if out[q].dtype != np.float32 or not out[q].flags.c_contiguous:
+                    raise JvError(JV_EINVAL, "request outputs must be C-contiguous float32 arrays")
+                refs.append(out[q])
+                r.out[q] = _fptr(out[q])
+        if image is not None:
+            for q in range(5):
+                if image[q] is not None:
+                    if image[q].dtype != np.float64 or not image[q].flags.c_contiguous:
+                        raise JvError(JV_EINVAL, "request images must be C-contiguous float64 arrays")
+                    refs.append(image[q])
+                    r.image[q] = image[q].ctypes.data_as(C.POINTER(C.c_double))
+        rid = C.c_longlong()
+        _check(lib().jv_server_submit(self._h, C.byref(r), C.byref(rid)))
+        self._refs[rid.value] = refs
+        return rid.value
+
+    def submit_survey(self, kind, s, shot: int = 0, obs=None):
+        """Queues shot `shot` of a synth.Survey-like object; returns (id,
+        outputs): the three trace arrays [n_recv][nt] of a FORWARD request,
+        or the five image arrays (ip, pp, ps, sp, ss; gridphy, float64) of an
+        RTM request, filled when the request is done."""
+        rv = np.ascontiguousarray(s.recvs, dtype=np.float32).reshape(-1, 3)
+        if kind == JOB_FORWARD:
+            outs = tuple(np.zeros((rv.shape[0], s.nt), np.float32) for _ in range(3))
+            rid = self.submit(kind, s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt,
+                              s.shots[shot], rv, rec_width=s.rec_width, out=outs)
+        else:
+            outs = tuple(np.zeros((s.nz, s.ny, s.nx), np.float64) for _ in range(5))
+            rid = self.submit(kind, s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt,
+                              s.shots[shot], rv, rec_width=s.rec_width, obs=obs, image=outs)
+        return rid, outs
+
+    def poll(self, rid: int):
+        st, res = C.c_int(), C.c_int()
+        _check(lib().jv_server_poll(self._h, rid, C.byref(st), C.byref(res)))
+        return st.value, res.value
+
+    def wait(self, rid: int, timeout: float = -1.0) -> int:
+        res = C.c_int()
+        _check(lib().jv_server_wait(self._h, rid, timeout, C.byref(res)))
+        self._refs.pop(rid, None)
+        return res.value
+
+    def cancel(self, rid: int) -> None:
+        _check(lib().jv_server_cancel(self._h, rid))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().jv_server_get_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            lib().jv_server_close(self._h)
+            self._h = None
+            self._refs.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -91,13 +91,21 @@ static Status bad(jv_status c, const std::string &m) {
 #define JV_CU(expr) JV_TRY(cu((expr), #expr))
 #define JV_K(expr) JV_TRY(cu((cudaError_t)(expr), #expr))
 
+// Device memory comes from the stream-ordered allocator on the context's
+// stream: neither allocating nor freeing waits for other contexts' work on
+// the device, so contexts run concurrently (a plain cudaFree would wait
+// for the whole device).  The stream is synchronised once the allocation
+// is made, so the memory is also usable from synchronous copies.
 Status Engine::alloc(void **p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) return Status{};
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = cudaMallocAsync(p, bytes, stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return bad(JV_ENOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        if (*p) cudaFreeAsync(*p, stream_);
+        *p = nullptr;
+        return bad(JV_ENOMEM, "allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
     }
     allocs_.push_back(*p);
     dev_bytes_ += bytes;
@@ -111,7 +119,9 @@ Engine::~Engine() {
     }
     for (auto &kv : graphs_) cudaGraphExecDestroy(kv.second);
     for (cudaEvent_t e : prof_pool_) cudaEventDestroy(e);
-    for (void *p : allocs_) cudaFree(p);
+    for (void *p : allocs_)
+        if (p) cudaFreeAsync(p, stream_);
+    if (stream_) cudaStreamSynchronize(stream_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -218,6 +228,71 @@ int upload_all_coefficients() {
     return upload_coefficients(list, dc2);
 }
 
+// VOWR face boxes (FD/fdtd3d_0_base_module/fdtd3d_base_5_wave_recon_meat.hpp:19-30;
+// face frames .jarvis_0_meta/.jarvis_3_operator/jarvis_1_mpicu_halo_store_operator_meat.hpp:129-134),
+// velocity fields first, with their offsets in the per-step record and their
+// first 256-cell block
+std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, long long *blocks) {
+    const int W[10][6] = {
+        {r - 1, r, r - 1, r, r, r - 1}, {r - 1, r, r, r - 1, r - 1, r}, {r, r - 1, r - 1, r, r - 1, r},
+        {0, 0, 0, 0, r - 1, r},         {0, 0, r - 1, r, 0, 0},         {r - 1, r, 0, 0, 0, 0},
+        {r - 1, r, r - 1, r, r - 1, r}, {0, 0, r, r - 1, r, r - 1},     {r, r - 1, 0, 0, r, r - 1},
+        {r, r - 1, r, r - 1, 0, 0}};
+    const int flds[10] = {VX, VY, VZ, SXX, SYY, SZZ, SAU, SXY, SXZ, SYZ};
+    const int m = g.m;
+    const int X0 = m, X1 = m + g.px, Y0 = m, Y1 = m + g.py, Z0 = m, Z1 = m + g.pz;
+    std::vector<SegDev> segs;
+    long long off = 0, blk = 0;
+    for (int f = 0; f < 10; f++)
+        for (int face = 0; face < 6; face++) {
+            int wd = W[f][face];
+            if (wd <= 0) continue;
+            int x0 = X0, x1 = X1, y0 = Y0, y1 = Y1, z0 = Z0, z1 = Z1;
+            switch (face) {
+            case 0: z0 = Z0 - wd; z1 = Z0; break;
+            case 1: z0 = Z1; z1 = Z1 + wd; break;
+            case 2: y0 = Y0 - wd; y1 = Y0; break;
+            case 3: y0 = Y1; y1 = Y1 + wd; break;
+            case 4: x0 = X0 - wd; x1 = X0; break;
+            default: x0 = X1; x1 = X1 + wd; break;
+            }
+            SegDev sg{};
+            sg.fld = flds[f];
+            sg.x0 = x0; sg.nxb = x1 - x0; sg.y0 = y0; sg.nyb = y1 - y0; sg.z0 = z0; sg.nzb = z1 - z0;
+            sg.off = off;
+            sg.nblk_first = blk;
+            long long cnt = (long long)sg.nxb * sg.nyb * sg.nzb;
+            off += cnt;
+            blk += (cnt + 255) / 256;
+            segs.push_back(sg);
+        }
+    *per_step = off;
+    *blocks = blk;
+    return segs;
+}
+
+size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm) {
+    size_t fe = 0;
+    const GridDev g = make_layout(grid, &fe);
+    long long psi = 0;
+    make_pml_slabs(g, 1, &psi);
+    const size_t nphy = (size_t)grid.nx * grid.ny * grid.nz;
+    size_t b = (4 * fe + 32) * sizeof(float);                 // model
+    b += (kNumFld * fe + 32) * sizeof(float);                 // forward wavefield
+    b += (size_t)psi * sizeof(float);                         // its memory variables
+    b += 5 * nphy * sizeof(double);                           // stacks
+    b += 16 * ((size_t)grid.nx + grid.ny + grid.nz + 2 * grid.pml * 3) + (1 << 20);  // tables, state, slack
+    if (rtm) {
+        long long per = 0, blk = 0;
+        vowr_segments(g, rec_width, &per, &blk);
+        b += (kNumFld * fe + 32) * sizeof(float) + (size_t)psi * sizeof(float);  // receiver wavefield
+        b += (size_t)per * (size_t)(nt > 1 ? nt - 1 : 0) * sizeof(float);          // boundary store
+        b += 5 * ((nphy + 63) / 64 * 64) * sizeof(float);                           // shot image
+        b += (size_t)blk * sizeof(int) + 64 * sizeof(SegDev);
+    }
+    return b;
+}
+
 // ------------------------------------------------------------ creation
 
 Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, const float *rho, float dt, float fm,
@@ -283,7 +358,6 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_K(upload_all_coefficients());
 
     // pitched gridext layout
-    const int m = grid_.pml;
     g_ = make_layout(grid_, &field_elems_);
     if (field_elems_ >= (size_t)1 << 31) return bad(JV_EINVAL, "gridext too large for 32-bit element offsets");
 
@@ -295,13 +369,13 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     vp_ = mb; rho_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
     const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
     float *tmp = nullptr;
-    JV_CU(cudaMalloc(&tmp, 3 * nphy * sizeof(float)));
+    JV_CU(cudaMallocAsync(&tmp, 3 * nphy * sizeof(float), stream_));
     cudaError_t e1 = cudaMemcpyAsync(tmp, vp, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
     cudaError_t e2 = cudaMemcpyAsync(tmp + nphy, vs, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
     cudaError_t e3 = cudaMemcpyAsync(tmp + 2 * nphy, rho, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
     int ek = k_model_prep(g_, tmp, tmp + nphy, tmp + 2 * nphy, vp_, rho_, lam_, mu_, stream_);
+    cudaFreeAsync(tmp, stream_);
     cudaError_t e4 = cudaStreamSynchronize(stream_);
-    cudaFree(tmp);
     JV_CU(e1); JV_CU(e2); JV_CU(e3); JV_K(ek); JV_CU(e4);
 
     // forward/backward wavefield (13 components, one arena)
@@ -346,41 +420,10 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     img_.ip = ib; img_.pp = ib + nphy; img_.ps = ib + 2 * nphy; img_.sp = ib + 3 * nphy; img_.ss = ib + 4 * nphy;
     JV_CU(cudaMemsetAsync(ib, 0, 5 * nphy * sizeof(double), stream_));
 
-    // VOWR face boxes (FD/fdtd3d_0_base_module/fdtd3d_base_5_wave_recon_meat.hpp:19-30;
-    // face frames .jarvis_0_meta/.jarvis_3_operator/jarvis_1_mpicu_halo_store_operator_meat.hpp:129-134)
+    // VOWR face boxes
     {
-        const int r = opt_.rec_width;
-        const int W[10][6] = {
-            {r - 1, r, r - 1, r, r, r - 1}, {r - 1, r, r, r - 1, r - 1, r}, {r, r - 1, r - 1, r, r - 1, r},
-            {0, 0, 0, 0, r - 1, r},         {0, 0, r - 1, r, 0, 0},         {r - 1, r, 0, 0, 0, 0},
-            {r - 1, r, r - 1, r, r - 1, r}, {0, 0, r, r - 1, r, r - 1},     {r, r - 1, 0, 0, r, r - 1},
-            {r, r - 1, r, r - 1, 0, 0}};
-        const int flds[10] = {VX, VY, VZ, SXX, SYY, SZZ, SAU, SXY, SXZ, SYZ};
-        const int X0 = m, X1 = m + g_.px, Y0 = m, Y1 = m + g_.py, Z0 = m, Z1 = m + g_.pz;
         long long off = 0, blk = 0;
-        for (int f = 0; f < 10; f++)
-            for (int face = 0; face < 6; face++) {
-                int wd = W[f][face];
-                if (wd <= 0) continue;
-                int x0 = X0, x1 = X1, y0 = Y0, y1 = Y1, z0 = Z0, z1 = Z1;
-                switch (face) {
-                case 0: z0 = Z0 - wd; z1 = Z0; break;
-                case 1: z0 = Z1; z1 = Z1 + wd; break;
-                case 2: y0 = Y0 - wd; y1 = Y0; break;
-                case 3: y0 = Y1; y1 = Y1 + wd; break;
-                case 4: x0 = X0 - wd; x1 = X0; break;
-                default: x0 = X1; x1 = X1 + wd; break;
-                }
-                SegDev sg{};
-                sg.fld = flds[f];
-                sg.x0 = x0; sg.nxb = x1 - x0; sg.y0 = y0; sg.nyb = y1 - y0; sg.z0 = z0; sg.nzb = z1 - z0;
-                sg.off = off;
-                sg.nblk_first = blk;
-                long long cnt = (long long)sg.nxb * sg.nyb * sg.nzb;
-                off += cnt;
-                blk += (cnt + 255) / 256;
-                segs_h_.push_back(sg);
-            }
+        segs_h_ = vowr_segments(g_, opt_.rec_width, &off, &blk);
         per_step_ = off;
         if (blk >= (1LL << 31) || per_step_ >= (1LL << 31)) return bad(JV_EINVAL, "boundary store too large");
         nslot_ = nt_ > 1 ? nt_ - 1 : 0;
@@ -428,7 +471,8 @@ Status Engine::set_geometry(int n_shot, const float *shot_xyz, int n_recv, const
     }
     nrec_ = (int)rec_h_.size();
     if (rec_d_) {
-        cudaFree(rec_d_);
+        cudaFreeAsync(rec_d_, stream_);
+        cudaStreamSynchronize(stream_);
         for (auto &a : allocs_)
             if (a == rec_d_) a = nullptr;
         rec_d_ = nullptr;

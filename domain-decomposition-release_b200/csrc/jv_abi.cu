@@ -90,9 +90,10 @@ struct jv_ctx {
         shutdown();
         if (eng) cudaSetDevice(eng->device());
         for (int q = 0; q < 2; q++) {
-            if (d_tr[q]) cudaFree(d_tr[q]);
+            if (d_tr[q]) cudaFreeAsync(d_tr[q], eng->stream());
             if (ev_copy[q]) cudaEventDestroy(ev_copy[q]);
         }
+        if (copy_stream) cudaStreamSynchronize(copy_stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
     }
 };
@@ -100,11 +101,13 @@ struct jv_ctx {
 static jv_status ensure_traces(jv_ctx *c, size_t elems, int which = 0) {
     if (c->d_tr_elems[which] >= elems) return JV_OK;
     cudaSetDevice(c->eng->device());
-    if (c->d_tr[which]) cudaFree(c->d_tr[which]);
+    cudaStream_t s = c->eng->stream();
+    if (c->d_tr[which]) cudaFreeAsync(c->d_tr[which], s);
     c->d_tr[which] = nullptr;
     c->d_tr_elems[which] = 0;
     if (elems == 0) return JV_OK;
-    cudaError_t e = cudaMalloc(&c->d_tr[which], elems * sizeof(float));
+    cudaError_t e = cudaMallocAsync(&c->d_tr[which], elems * sizeof(float), s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(JV_ENOMEM, std::string("trace buffer: ") + cudaGetErrorString(e));

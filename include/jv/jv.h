@@ -261,6 +261,51 @@ jv_status jv_wait(jv_ctx *c, long long id, double timeout_s, jv_status *result);
  * started runs to its end (JV_ESTATE). jv_close cancels the queued ones. */
 jv_status jv_cancel(jv_ctx *c, long long id);
 
+/* Requests and the server: a request is one shot of forward modelling or
+ * RTM on a model and grid of its own.  jv_server keeps a queue and `slots`
+ * worker threads; a worker takes the first queued request whose device
+ * footprint (jv_footprint) fits the memory still free under the server's
+ * budget, runs it on a context of its own and releases it, so requests of
+ * different sizes run concurrently on the GPU as slots and memory come
+ * free.  A request's result does not depend on what else runs.  The
+ * reference has no counterpart.  Host buffers named in a request must stay
+ * valid until it ends. */
+typedef struct jv_request {
+    int kind;                   /* JV_JOB_FORWARD or JV_JOB_RTM                      */
+    jv_grid grid;
+    const float *vp, *vs, *rho; /* host, gridphy                                      */
+    float dt, fm;
+    int nt;
+    int rec_width;              /* 0 -> 1                                            */
+    float shot_xyz[3];          /* metres, inside gridphy                            */
+    int n_recv;
+    const float *recv_xyz;      /* metres; points outside gridphy are dropped        */
+    const float *obs[3];        /* RTM: observed traces [n_kept][nt]; all NULL: the
+                                   request models them first                          */
+    float *out[3];              /* FORWARD: traces [n_kept][nt] (NULL skips one)     */
+    double *image[5];           /* RTM: this shot's FP64 stacks ip, pp, ps, sp, ss
+                                   (gridphy, NULL skips one)                         */
+} jv_request;
+typedef struct jv_server jv_server;
+typedef struct jv_server_stats {
+    long long submitted, completed, failed, cancelled, running, queued;
+    double p50_ms, p99_ms, mean_ms; /* submission to completion, over the latest 65536 completed */
+    size_t bytes_in_use, budget;
+} jv_server_stats;
+/* Device bytes a context holds for one request of this size with n_recv
+ * receivers (an estimate from the layout; the server's admission unit). */
+jv_status jv_footprint(const jv_grid *grid, int nt, int rec_width, int kind, int n_recv, size_t *bytes);
+/* hbm_budget 0: 90 % of the device's free memory now. */
+jv_status jv_server_create(int device, int slots, size_t hbm_budget, jv_server **out);
+/* JV_ENOMEM if the request alone exceeds the budget. */
+jv_status jv_server_submit(jv_server *s, const jv_request *r, long long *id);
+jv_status jv_server_poll(jv_server *s, long long id, int *state, jv_status *result);
+jv_status jv_server_wait(jv_server *s, long long id, double timeout_s, jv_status *result);
+jv_status jv_server_cancel(jv_server *s, long long id);
+jv_status jv_server_get_stats(jv_server *s, jv_server_stats *out);
+/* Cancels queued requests, waits for the running ones, frees the server. */
+jv_status jv_server_close(jv_server *s);
+
 /* Device time (ms) of the last jv_forward* / jv_rtm_shot* call, measured
  * with CUDA events around its kernels. */
 jv_status jv_last_timing(const jv_ctx *c, double *ms);
