@@ -176,11 +176,19 @@ def pml_bytes(s, name):
     return float(cells * per + axes * 3 * 8)
 
 
+# the full-gridext stress kernel (variant 4) does the work of two launches
+FUSED = {"stress_fz_fwd": ("stress_phy_fwd", "stress_pml"),
+         "stress_fz_rtmfwd": ("stress_phy_rtmfwd", "stress_pml_sau"),
+         "stress_fz_rev": ("stress_phy_rev", "stress_pml_sau")}
+
+
 def kernel_bytes(s, name):
     if name in BYTES_PER_CELL:
         return float(BYTES_PER_CELL[name] * s.n_phy)
     if name in ("vel_pml", "stress_pml", "stress_pml_sau"):
         return pml_bytes(s, name)
+    if name in FUSED:
+        return sum(kernel_bytes(s, k) for k in FUSED[name])
     return None
 
 

@@ -280,12 +280,13 @@ size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm) {
     size_t b = (4 * fe + 32) * sizeof(float);                 // model
     b += (kNumFld * fe + 32) * sizeof(float);                 // forward wavefield
     b += (size_t)psi * sizeof(float);                         // its memory variables
+    b += (size_t)fz_psi_floats(g) * sizeof(float);            // the full-gridext kernel's stress ones
     b += 5 * nphy * sizeof(double);                           // stacks
     b += 16 * ((size_t)grid.nx + grid.ny + grid.nz + 2 * grid.pml * 3) + (1 << 20);  // tables, state, slack
     if (rtm) {
         long long per = 0, blk = 0;
         vowr_segments(g, rec_width, &per, &blk);
-        b += (kNumFld * fe + 32) * sizeof(float) + (size_t)psi * sizeof(float);  // receiver wavefield
+        b += (kNumFld * fe + 32) * sizeof(float) + (size_t)(psi + fz_psi_floats(g)) * sizeof(float);  // receiver wavefield
         b += (size_t)per * (size_t)(nt > 1 ? nt - 1 : 0) * sizeof(float);          // boundary store
         b += 5 * ((nphy + 63) / 64 * 64) * sizeof(float);                           // shot image
         b += (size_t)blk * sizeof(int) + 64 * sizeof(SegDev);
@@ -314,7 +315,7 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread < 0 || opt.planes_per_thread > 2 || opt.pml_planes_per_thread < 0 ||
         opt.pml_planes_per_thread > 2)
         return bad(JV_EINVAL, "planes_per_thread and pml_planes_per_thread must be 0, 1 or 2");
-    if (opt.kernel_variant < 0 || opt.kernel_variant > 3) return bad(JV_EINVAL, "kernel_variant must be 0..3");
+    if (opt.kernel_variant < 0 || opt.kernel_variant > 4) return bad(JV_EINVAL, "kernel_variant must be 0..4");
     if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
         return bad(JV_EINVAL, "tile_gx * tile_gy must be <= 256");
     long long next = (long long)(grid.nx + 2 * grid.pml) * (grid.ny + 2 * grid.pml) * (grid.nz + 2 * grid.pml);
@@ -382,7 +383,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
     JV_CU(cudaMemsetAsync(p, 0, kGuard * sizeof(float), stream_));
     for (int f = 0; f < kNumFld; f++) F_.f[f] = (float *)p + kGuard + f * field_elems_;
-    if (kc_.variant == 3) {
+    if (kc_.variant >= 3) {
         JV_TRY(alloc(&p, sizeof(int)));
         zm_err_ = (int *)p;
         JV_CU(cudaMemsetAsync(zm_err_, 0, sizeof(int), stream_));
@@ -403,6 +404,12 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         }
         JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
         cpF_ = make_cpml((float *)p);
+    }
+    if (kc_.variant == 4) {
+        fz_psi_total_ = fz_psi_floats(g_);
+        JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
+        fzpsiF_ = (float *)p;
+        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, axis_d_, fzpsiF_, zm_err_, &fullF_));
     }
 
     // wavelet and step state
@@ -529,6 +536,9 @@ CpmlDev Engine::make_cpml(float *psi) const {
 
 Status Engine::zero_psi(const CpmlDev &c) {
     if (psi_total_ > 0) JV_CU(cudaMemsetAsync(c.psi, 0, (size_t)psi_total_ * sizeof(float), stream_));
+    // the axis-major stress memory variables of the full-gridext kernel
+    float *fz = c.psi == cpF_.psi ? fzpsiF_ : c.psi == cpR_.psi ? fzpsiR_ : nullptr;
+    if (fz) JV_CU(cudaMemsetAsync(fz, 0, (size_t)fz_psi_total_ * sizeof(float), stream_));
     return Status{};
 }
 
@@ -648,17 +658,29 @@ Status Engine::launch_step(int kind, int off, bool advance) {
     case kStepModel:
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, kc_, s));
-        JV_L("stress_phy_fwd", k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
+        if (fullF_.ok) {
+            JV_L("stress_fz_fwd", k_stress_full(kFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
+        } else {
+            JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, kc_, s));
+            JV_L("stress_phy_fwd",
+                 k_stress_phy(kFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
+        }
         JV_L("record", k_record(F_, rec_d_, nrec_, nt_, st_, off, s));
         if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
         JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
         JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, kc_, s));
-        JV_L("vowr_pack", k_vowr(g_, F_, vowr_, st_, off, 1, 0, s));
-        JV_L("stress_phy_rtmfwd", k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
+        if (fullF_.ok) {
+            // the boundary boxes lie in the absorbing layers: pack them after their update
+            JV_L("stress_fz_rtmfwd", k_stress_full(kRtmFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
+            JV_L("vowr_pack", k_vowr(g_, F_, vowr_, st_, off, 1, 0, s));
+        } else {
+            JV_L("stress_pml_sau", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 1, kc_, s));
+            JV_L("vowr_pack", k_vowr(g_, F_, vowr_, st_, off, 1, 0, s));
+            JV_L("stress_phy_rtmfwd",
+                 k_stress_phy(kRtmFwd, g_, F_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
+        }
         if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmRev:
@@ -672,8 +694,13 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
         JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
-        JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
-        JV_L("stress_phy_rev", k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsR_));
+        if (fullR_.ok) {
+            JV_L("stress_fz_rev", k_stress_full(kRev, g_, R_, dt, wavelet_, st_, off, fullR_, s));
+        } else {
+            JV_L("stress_pml_sau", k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
+            JV_L("stress_phy_rev",
+                 k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, off, kc_, s, &mapsR_));
+        }
         JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 1, s));
         if (advance) JV_L("step_advance", k_step_advance(st_, -1, s));
         break;
@@ -770,9 +797,14 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
         JV_CU(cudaMemsetAsync(p, 0, kGuard * sizeof(float), stream_));
         for (int f = 0; f < kNumFld; f++) R_.f[f] = (float *)p + kGuard + f * field_elems_;
-        if (kc_.variant == 3) JV_K(k_make_wave_maps(g_, R_, lam_, mu_, zm_err_, &mapsR_));
+        if (kc_.variant >= 3) JV_K(k_make_wave_maps(g_, R_, lam_, mu_, zm_err_, &mapsR_));
         JV_TRY(alloc(&p, (size_t)psi_total_ * sizeof(float)));
         cpR_ = make_cpml((float *)p);
+        if (kc_.variant == 4) {
+            JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
+            fzpsiR_ = (float *)p;
+            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, axis_d_, fzpsiR_, zm_err_, &fullR_));
+        }
     }
     if (!shot_img_.ip) {
         // five arrays at a pitch of whole 256-byte lines, so that every

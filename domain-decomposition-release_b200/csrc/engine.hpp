@@ -117,6 +117,9 @@ class Engine {
     GridDev g_{};
     KCfg kc_{};
     WaveMaps mapsF_{}, mapsR_{};  // TMA descriptors of the velocity fields (variant 3)
+    FullMaps fullF_{}, fullR_{};  // TMA descriptors of the full-gridext stress kernel (variant 4)
+    float *fzpsiF_ = nullptr, *fzpsiR_ = nullptr;  // its axis-major stress memory variables
+    long long fz_psi_total_ = 0;                   // floats of one of them
     int *zm_err_ = nullptr;       // device flag of variant 3's bounded waits
     Status check_zm_err();
     size_t field_elems_ = 0;  // elements per pitched field

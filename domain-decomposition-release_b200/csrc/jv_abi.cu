@@ -169,7 +169,7 @@ void jv_options_default(jv_options *o) {
     o->use_graphs = 1;
     o->graph_steps = 0;
     o->store_budget = 0;
-    o->kernel_variant = 3;
+    o->kernel_variant = 4;
     o->zchunk = 0;
 }
 

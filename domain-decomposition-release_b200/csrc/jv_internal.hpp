@@ -129,6 +129,47 @@ struct WaveMaps {
     int *err = nullptr;  // device flag: a bounded wait in the kernel ran out
 };
 
+// Geometry of the full-gridext stress kernel (variant 4).
+//  - XH, XC, corew: TMA x of the halo and core boxes, core box width;
+//    hxi, hxe: x pairs of a tile row in the physical range and in the two
+//    absorbing ranges; ytiles, nzi: 4-row tiles over y in [2, ny-2), planes
+//    z in [2, nz-2).
+//  - The stress memory variables of this kernel are axis-major: per axis
+//    three arrays over the cells that absorb on that axis, rows packed
+//    (x arrays [t][z-2][y-2][xc], pitch PX over xc = the W absorbing x
+//    columns; y arrays [t][z-2][yc][x-2] and z arrays [t][zc][y-2][x-2],
+//    pitch PY over x-2), so that a tile's memory variables arrive by TMA
+//    with its fields.  W = 2 (m - 2) absorbing indices per axis.
+//  - Runs: each tile's planes are cut into Q chunks of L planes (the last
+//    one padded with idle items); run r = chunk * ytiles + tile, and CTA b
+//    takes runs b, b + grid, ...  CTAs b and b+1 then march neighbouring
+//    tiles through the same planes together, so halo rows are shared in L2.
+struct FzGeo {
+    int XH, XC, corew;
+    int hxi, hxe;
+    int ytiles, nzi;
+    int PX, PY, W;
+    int Q, L, R;
+    float *psx, *psy, *psz;
+    const float4 *ax[3];
+};
+
+// floats of the axis-major stress memory variables of one wavefield
+long long fz_psi_floats(const GridDev &g);
+
+// TMA descriptors of the full-gridext stress kernel of one wavefield
+struct FullMaps {
+    FieldMap halo[3];             // vx vy vz
+    FieldMap core[kZmCore + 1];   // vx vy vz, lam, mu, vp, sxx syy szz sxy sxz syz, sau
+    FieldMap psi[3];              // the x, y and z memory-variable arrays (4-D: 3 arrays each)
+    bool ok = false;              // false: variant 4 is not available for this grid
+    FzGeo geo{};
+    int threads = 0;
+    int grid = 0;
+    size_t smem = 0;
+    int *err = nullptr;
+};
+
 // interior-kernel choice: variant 0 = one z plane per block, 1 = z-marching
 // over chunks of zchunk planes (0: the whole column)
 struct KCfg {
@@ -158,6 +199,16 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
 // or the driver entry point missing).  Returns a cudaError_t.
 int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
                      WaveMaps *maps);
+// The descriptors of the full-gridext stress kernel (variant 4); maps->ok
+// stays false when the grid does not suit it (odd pml_num or nx, a tile
+// row of more than 512 threads or a halo row wider than 256 floats, the
+// driver entry point missing).  Returns a cudaError_t.
+int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
+                     float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps);
+// Stress update of every updated cell of gridext, interior and absorbing
+// layers in one launch (modes kFwd, kRtmFwd, kRev).
+int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const float *wavelet, const StepState *st,
+                  int it_off, const FullMaps &maps, void *stream);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
               const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,

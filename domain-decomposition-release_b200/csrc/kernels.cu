@@ -1422,6 +1422,448 @@ __global__ void __launch_bounds__(256, MINB) stress_pml(GridDev g, CpmlDev P, Wa
     }
 }
 
+// ------------------------------------------------- full-gridext stress update
+//
+// Variant 4 of the stress update for the steps that carry absorbing
+// layers (forward modelling, the RTM forward pass and the receiver
+// wavefield): one persistent z-marching kernel over every updated cell of
+// gridext, [2, n-2) on each axis.  It merges the 8th-order interior update
+// (stress_zm3) and the 4th-order CPML update of the six slabs
+// (stress_pml), so each velocity value is brought on chip once per step
+// and the absorbing layers run behind the same TMA pipeline as the
+// interior.  Items are (4-row tile, plane) with y in [2, ny-2) and z in
+// [2, nz-2); a tile row is the whole updated x range.  Threads own x
+// pairs: the first 4*hxi threads the physical x range [m, m+px), the rest
+// the two absorbing x ranges [2, m) and [m+px, nx-2), so a warp takes one
+// branch except at the single warp where the two groups meet and in tiles
+// that straddle y = m or y = m+py.  Both m and px are even, which keeps
+// every region boundary on a pair boundary.  A cell is interior when x, y
+// and z are all in the physical range; it then takes the 8th-order update
+// of stress_phy (FD/fdtd3d_0_base_module/fdtd3d_base_3_kernel_device_meat.hpp)
+// and the explosive source.  Any other cell takes the CPML update of
+// stress_pml_group (4th order, memory variables on its absorbing axes,
+// FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_2_kernel_device_{x,y,z}_meat.hpp);
+// its memory variables are the axis-major arrays of FzGeo, brought in by
+// TMA with the fields and written back with plain stores.  The z windows hold
+// planes z-4 .. z+4; planes outside gridext read as zero (their taps have
+// zero weight wherever they are reached).
+
+constexpr int kFzCore = kZmCore + 1;  // vx vy vz (window feed), lam, mu, vp, sxx syy szz sxy sxz syz, sau
+constexpr int kFzStage = 3 * kZmHB + kFzCore * kZmCB;
+
+struct FzMaps {
+    CUtensorMap halo[3];
+    CUtensorMap core[kFzCore];
+    CUtensorMap psi[3];
+};
+
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int x, int y, int z, int w,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
+        : "memory");
+}
+
+// stage layout: halo planes, core tiles, then the three memory-variable
+// boxes (3 arrays x 4 rows each), every region 128-byte aligned
+__host__ __device__ constexpr int fz_round32(int n) { return (n + 31) / 32 * 32; }
+__host__ __device__ inline int fz_stage(const FzGeo &g) {
+    return kFzStage + fz_round32(12 * g.PX) + 2 * fz_round32(12 * g.PY);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kZmMaxThreads, 1)
+    stress_fz(GridDev g, const __grid_constant__ FzMaps maps, WaveDev w, float dt, const float *__restrict__ wavelet,
+              const StepState *__restrict__ st, int it_off, const __grid_constant__ FzGeo geo, int *err) {
+    static_assert(MODE != kBwd, "the source reconstruction carries no absorbing layers");
+    constexpr bool kSau = MODE != kFwd;
+    constexpr int NCT = kSau ? kFzCore : kFzCore - 1;  // sau is neither read nor written in forward modelling
+    extern __shared__ __align__(128) float sm[];
+    constexpr int hb = kZmHB, cb = kZmCB, boxw = kZmPitch;
+    const int stage = fz_stage(geo);
+    const int pxr = fz_round32(12 * geo.PX), pyr = fz_round32(12 * geo.PY);
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_abort;
+    // this CTA's runs: blockIdx.x, blockIdx.x + gridDim.x, ...; L items each
+    const int nrun = (geo.R - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int w0 = 0, w1 = nrun * geo.L;
+    if (nrun <= 0) return;
+    // item -> (tile, plane); planes past the last one are idle items
+    auto item_at = [&](int item, int &yt, int &z) {
+        const int j = item / geo.L, off = item - j * geo.L;
+        const int rr = (int)blockIdx.x + j * (int)gridDim.x;
+        const int q = rr / geo.ytiles;
+        yt = rr - q * geo.ytiles;
+        z = 2 + q * geo.L + off;
+    };
+    const int tid = threadIdx.x;
+    const int m = g.m;
+    const int ti = kZmRows * geo.hxi;
+    const bool xabs = tid >= ti;  // this thread's pair lies in an absorbing x range
+    int r, x;
+    if (!xabs) {
+        r = tid / geo.hxi;
+        x = m + 2 * (tid - r * geo.hxi);
+    } else {
+        const int e = tid - ti, half = geo.hxe / 2;
+        r = e / geo.hxe;
+        const int q = e - r * geo.hxe;
+        x = q < half ? 2 + 2 * q : m + g.px + 2 * (q - half);
+    }
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const uint32_t bytes_all = (uint32_t)(3 * hb + NCT * geo.corew * kZmRows) * 4u;
+    const uint32_t bytes_feed = (uint32_t)(3 * geo.corew * kZmRows) * 4u;
+    const uint32_t bytes_psx = (uint32_t)(12 * geo.PX) * 4u, bytes_psy = (uint32_t)(12 * geo.PY) * 4u;
+    auto issue = [&](int item, int b) {
+        int yt, z;
+        item_at(item, yt, z);
+        const uint32_t bar = b ? bar1 : bar0;
+        if (z >= g.nz - 2) {
+            mbar_expect(bar, 0);  // idle item: the phase completes with this arrival
+            return;
+        }
+        const int Y = 2 + yt * kZmRows;
+        float *base = sm + b * stage;
+        const bool feed = z + 5 < g.nz;  // the window's next plane; none past gridext
+        const bool zab = z < m || z >= m + g.pz;
+        const bool ylo = Y < m, yhi = Y + kZmRows - 1 >= m + g.py;  // the tile holds absorbing rows
+        mbar_expect(bar, (feed ? bytes_all : bytes_all - bytes_feed) + bytes_psx + (ylo || yhi ? bytes_psy : 0u) +
+                             (zab ? bytes_psy : 0u));
+        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], geo.XH, Y - kZmHalo, z, bar);
+        if (feed)
+            for (int f = 0; f < 3; f++)
+                tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], geo.XC, Y, z + 5, bar);
+        for (int f = 3; f < NCT; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], geo.XC, Y, z, bar);
+        float *ps = base + kFzStage;
+        tma_load_4d(smem_u32(ps), &maps.psi[0], 0, Y - 2, z - 2, 0, bar);
+        if (ylo || yhi)
+            tma_load_4d(smem_u32(ps + pxr), &maps.psi[1], 0, ylo ? Y - 2 : m - 2 + Y - (m + g.py), z - 2, 0, bar);
+        if (zab)
+            tma_load_4d(smem_u32(ps + pxr + pyr), &maps.psi[2], 0, Y - 2, z < m ? z - 2 : m - 2 + z - (m + g.pz), 0,
+                        bar);
+    };
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar1, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        issue(w0, 0);
+        if (w0 + 1 < w1) issue(w0 + 1, 1);
+    }
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    const int hcol = (int)g.xoff + x - geo.XH;  // the pair's first cell in a halo row (even)
+    const int ccol = (int)g.xoff + x - geo.XC;  // ... in a core row (even)
+    float2 rv[3][9];                           // z windows: planes z-4 .. z+4 of vx, vy, vz
+    const float *fv[3] = {w.f[VX], w.f[VY], w.f[VZ]};
+    int cur_yt = -1, cur_z = -2;
+    for (int k = w0; k < w1; k++) {
+        int yt, z;
+        item_at(k, yt, z);
+        const int y = 2 + yt * kZmRows + r;
+        const bool live = y < g.ny - 2 && z < g.nz - 2;
+        const int i0 = (int)g.xoff + x + sy * y + sz * z;  // even: float2-aligned
+        const int b = (k - w0) & 1;
+        const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
+        const float *base = sm + b * stage;
+        const int cc = r * geo.corew + ccol;
+        if (yt != cur_yt || z != cur_z + 1) {
+            // a new run of planes: fill the z windows from global memory
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+#pragma unroll
+                for (int q = 0; q < 9; q++) {
+                    const int zq = z + q - 4;
+                    rv[f][q] = (live && zq >= 0 && zq < g.nz)
+                                   ? __ldg(reinterpret_cast<const float2 *>(fv[f] + i0 + (q - 4) * sz))
+                                   : make_float2(0.f, 0.f);
+                }
+            }
+        }
+        cur_yt = yt;
+        cur_z = z;
+        if (!mbar_wait_bounded(b ? bar1 : bar0, parity)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+        }
+        if (live) {
+            const float *C = base + 3 * hb;  // core tiles
+            const int c0 = (r + kZmHalo) * boxw + hcol;
+            auto ld2 = [&](const float *F, int off) { return *reinterpret_cast<const float2 *>(F + off); };
+            // x window of a field around the pair: e[j] = f[x - 4 + j], j = 0..9
+            auto xwin2 = [&](const float *F, float *e) {
+#pragma unroll
+                for (int j = 0; j < 5; j++) {
+                    const float2 v = ld2(F, c0 - 4 + 2 * j);
+                    e[2 * j] = v.x;
+                    e[2 * j + 1] = v.y;
+                }
+            };
+            const bool zabs = z < m || z >= m + g.pz;
+            const bool yabs = y < m || y >= m + g.py;
+            const bool cpml = xabs || yabs || zabs;
+            float Nx[2], Ny[2], Nz[2], Sxy[2], Sxz[2], Syz[2];
+            float e[10];
+            if (!cpml) {
+                const float *cf = c_list[kPhyHalf];
+                // vx: Dm_x -> Nx, Dp_y -> Sxy, Dp_z -> Sxz
+                xwin2(base, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) t += cf[q] * (e[4 + c + q] - e[4 + c - q - 1]);
+                    Nx[c] = t * rdx;
+                }
+                {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float2 a = ld2(base, c0 + (q + 1) * boxw), bb = ld2(base, c0 - q * boxw);
+                        t.x += cf[q] * (a.x - bb.x);
+                        t.y += cf[q] * (a.y - bb.y);
+                    }
+                    Sxy[0] = t.x * rdy;
+                    Sxy[1] = t.y * rdy;
+                    t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        t.x += cf[q] * (rv[0][4 + q + 1].x - rv[0][4 - q].x);
+                        t.y += cf[q] * (rv[0][4 + q + 1].y - rv[0][4 - q].y);
+                    }
+                    Sxz[0] = t.x * rdz;
+                    Sxz[1] = t.y * rdz;
+                }
+                // vy: Dp_x -> Sxy, Dm_y -> Ny, Dp_z -> Syz
+                xwin2(base + hb, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) t += cf[q] * (e[4 + c + q + 1] - e[4 + c - q]);
+                    Sxy[c] += t * rdx;
+                }
+                {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float2 a = ld2(base + hb, c0 + q * boxw), bb = ld2(base + hb, c0 - (q + 1) * boxw);
+                        t.x += cf[q] * (a.x - bb.x);
+                        t.y += cf[q] * (a.y - bb.y);
+                    }
+                    Ny[0] = t.x * rdy;
+                    Ny[1] = t.y * rdy;
+                    t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        t.x += cf[q] * (rv[1][4 + q + 1].x - rv[1][4 - q].x);
+                        t.y += cf[q] * (rv[1][4 + q + 1].y - rv[1][4 - q].y);
+                    }
+                    Syz[0] = t.x * rdz;
+                    Syz[1] = t.y * rdz;
+                }
+                // vz: Dp_x -> Sxz, Dp_y -> Syz, Dm_z -> Nz
+                xwin2(base + 2 * hb, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) t += cf[q] * (e[4 + c + q + 1] - e[4 + c - q]);
+                    Sxz[c] += t * rdx;
+                }
+                {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float2 a = ld2(base + 2 * hb, c0 + (q + 1) * boxw),
+                                     bb = ld2(base + 2 * hb, c0 - q * boxw);
+                        t.x += cf[q] * (a.x - bb.x);
+                        t.y += cf[q] * (a.y - bb.y);
+                    }
+                    Syz[0] += t.x * rdy;
+                    Syz[1] += t.y * rdy;
+                    t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        t.x += cf[q] * (rv[2][4 + q].x - rv[2][4 - q - 1].x);
+                        t.y += cf[q] * (rv[2][4 + q].y - rv[2][4 - q - 1].y);
+                    }
+                    Nz[0] = t.x * rdz;
+                    Nz[1] = t.y * rdz;
+                }
+            } else {
+                // 4th-order differences of the absorbing layers, then the
+                // memory variables of the absorbing axes
+                const float k0 = c_dc2[0], k1 = c_dc2[1];
+                float d[9][2];  // vx_x vy_x vz_x | vy_y vx_y vz_y | vz_z vx_z vy_z
+                xwin2(base, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) d[0][c] = (k0 * (e[4 + c] - e[3 + c]) + k1 * (e[5 + c] - e[2 + c])) * rdx;
+                xwin2(base + hb, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) d[1][c] = (k0 * (e[5 + c] - e[4 + c]) + k1 * (e[6 + c] - e[3 + c])) * rdx;
+                xwin2(base + 2 * hb, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) d[2][c] = (k0 * (e[5 + c] - e[4 + c]) + k1 * (e[6 + c] - e[3 + c])) * rdx;
+                {
+                    // Dm_y vy
+                    const float *F = base + hb;
+                    const float2 a = ld2(F, c0), bb = ld2(F, c0 - boxw), cq = ld2(F, c0 + boxw),
+                                 dq = ld2(F, c0 - 2 * boxw);
+                    d[3][0] = (k0 * (a.x - bb.x) + k1 * (cq.x - dq.x)) * rdy;
+                    d[3][1] = (k0 * (a.y - bb.y) + k1 * (cq.y - dq.y)) * rdy;
+                }
+#pragma unroll
+                for (int f = 0; f < 3; f += 2) {
+                    // Dp_y vx -> d[4], Dp_y vz -> d[5]
+                    const float *F = base + f * hb;
+                    const float2 a = ld2(F, c0 + boxw), bb = ld2(F, c0), cq = ld2(F, c0 + 2 * boxw),
+                                 dq = ld2(F, c0 - boxw);
+                    d[4 + f / 2][0] = (k0 * (a.x - bb.x) + k1 * (cq.x - dq.x)) * rdy;
+                    d[4 + f / 2][1] = (k0 * (a.y - bb.y) + k1 * (cq.y - dq.y)) * rdy;
+                }
+                // Dm_z vz -> d[6]; Dp_z vx -> d[7], vy -> d[8]
+                d[6][0] = (k0 * (rv[2][4].x - rv[2][3].x) + k1 * (rv[2][5].x - rv[2][2].x)) * rdz;
+                d[6][1] = (k0 * (rv[2][4].y - rv[2][3].y) + k1 * (rv[2][5].y - rv[2][2].y)) * rdz;
+#pragma unroll
+                for (int f = 0; f < 2; f++) {
+                    d[7 + f][0] = (k0 * (rv[f][5].x - rv[f][4].x) + k1 * (rv[f][6].x - rv[f][3].x)) * rdz;
+                    d[7 + f][1] = (k0 * (rv[f][5].y - rv[f][4].y) + k1 * (rv[f][6].y - rv[f][3].y)) * rdz;
+                }
+                // memory variables: this tile's boxes in shared memory, the
+                // axis-major arrays in global memory
+                const float *PS = base + kFzStage;
+                const int zi = z - 2, yi = y - 2, xi = x - 2;
+                const float2 vp2 = ld2(C, 5 * cb + cc);
+                const float vpc[2] = {vp2.x, vp2.y};
+                float A[2], B[2], Ah[2], Bh[2];
+                auto upd = [&](const float *sp, float *gp, const float *BB, const float *AA, float *dd) {
+                    float2 v = *reinterpret_cast<const float2 *>(sp);
+                    v.x = BB[0] * v.x + AA[0] * dd[0];
+                    v.y = BB[1] * v.y + AA[1] * dd[1];
+                    *reinterpret_cast<float2 *>(gp) = v;
+                    dd[0] += v.x;
+                    dd[1] += v.y;
+                };
+                if (xabs) {
+                    const int xc = x < m ? x - 2 : m - 2 + x - (m + g.px);
+                    const long long a0 = ((long long)zi * (g.ny - 4) + yi) * geo.PX + xc;
+                    const long long as = (long long)(g.nz - 4) * (g.ny - 4) * geo.PX;
+                    const int s0 = r * geo.PX + xc, ss = 4 * geo.PX;
+#pragma unroll
+                    for (int c = 0; c < 2; c++) cpml_coef(vpc[c], __ldg(&geo.ax[0][x + c]), dt, A[c], B[c], Ah[c], Bh[c]);
+                    upd(PS + s0, geo.psx + a0, B, A, d[0]);
+                    upd(PS + s0 + ss, geo.psx + a0 + as, Bh, Ah, d[1]);
+                    upd(PS + s0 + 2 * ss, geo.psx + a0 + 2 * as, Bh, Ah, d[2]);
+                }
+                if (yabs) {
+                    const int yc = y < m ? y - 2 : m - 2 + y - (m + g.py);
+                    const long long a0 = ((long long)zi * geo.W + yc) * geo.PY + xi;
+                    const long long as = (long long)(g.nz - 4) * geo.W * geo.PY;
+                    const int s0 = fz_round32(12 * geo.PX) + r * geo.PY + xi, ss = 4 * geo.PY;
+                    const float4 ty = __ldg(&geo.ax[1][y]);
+#pragma unroll
+                    for (int c = 0; c < 2; c++) cpml_coef(vpc[c], ty, dt, A[c], B[c], Ah[c], Bh[c]);
+                    upd(PS + s0, geo.psy + a0, B, A, d[3]);
+                    upd(PS + s0 + ss, geo.psy + a0 + as, Bh, Ah, d[4]);
+                    upd(PS + s0 + 2 * ss, geo.psy + a0 + 2 * as, Bh, Ah, d[5]);
+                }
+                if (zabs) {
+                    const int zc = z < m ? z - 2 : m - 2 + z - (m + g.pz);
+                    const long long a0 = ((long long)zc * (g.ny - 4) + yi) * geo.PY + xi;
+                    const long long as = (long long)geo.W * (g.ny - 4) * geo.PY;
+                    const int s0 = fz_round32(12 * geo.PX) + fz_round32(12 * geo.PY) + r * geo.PY + xi,
+                              ss = 4 * geo.PY;
+                    const float4 tz = __ldg(&geo.ax[2][z]);
+#pragma unroll
+                    for (int c = 0; c < 2; c++) cpml_coef(vpc[c], tz, dt, A[c], B[c], Ah[c], Bh[c]);
+                    upd(PS + s0, geo.psz + a0, B, A, d[6]);
+                    upd(PS + s0 + ss, geo.psz + a0 + as, Bh, Ah, d[7]);
+                    upd(PS + s0 + 2 * ss, geo.psz + a0 + 2 * as, Bh, Ah, d[8]);
+                }
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    Nx[c] = d[0][c];
+                    Ny[c] = d[3][c];
+                    Nz[c] = d[6][c];
+                    Sxy[c] = d[1][c] + d[4][c];
+                    Sxz[c] = d[2][c] + d[7][c];
+                    Syz[c] = d[5][c] + d[8][c];
+                }
+            }
+            const float2 l2 = ld2(C, 3 * cb + cc), m2 = ld2(C, 4 * cb + cc);
+            const float l[2] = {l2.x, l2.y}, mm[2] = {m2.x, m2.y};
+            const float2 s0 = ld2(C, 6 * cb + cc), s1 = ld2(C, 7 * cb + cc), s2 = ld2(C, 8 * cb + cc);
+            float sxx[2] = {s0.x, s0.y}, syy[2] = {s1.x, s1.y}, szz[2] = {s2.x, s2.y};
+            if (MODE != kRev && !cpml) {
+                // explosive source (physical cells), applied before the stress update of step it
+                const long long dd = st->src - (long long)i0;
+                if (dd >= 0 && dd < 2) {
+                    const float sv = wavelet[st->it + it_off];
+                    sxx[dd] += sv;
+                    syy[dd] += sv;
+                    szz[dd] += sv;
+                }
+            }
+            const float2 t9 = ld2(C, 9 * cb + cc), t10 = ld2(C, 10 * cb + cc), t11 = ld2(C, 11 * cb + cc);
+            const float sxy0[2] = {t9.x, t9.y}, sxz0[2] = {t10.x, t10.y}, syz0[2] = {t11.x, t11.y};
+            float sau0[2] = {0.f, 0.f};
+            if (kSau) {
+                const float2 t12 = ld2(C, 12 * cb + cc);
+                sau0[0] = t12.x;
+                sau0[1] = t12.y;
+            }
+            float o[7][2];
+#pragma unroll
+            for (int c = 0; c < 2; c++) {
+                const float l2m = l[c] + 2.0f * mm[c];
+                o[0][c] = sxx[c] + dt * (l2m * Nx[c] + l[c] * Ny[c] + l[c] * Nz[c]);
+                o[1][c] = syy[c] + dt * (l[c] * Nx[c] + l2m * Ny[c] + l[c] * Nz[c]);
+                o[2][c] = szz[c] + dt * (l[c] * Nx[c] + l[c] * Ny[c] + l2m * Nz[c]);
+                o[3][c] = sxy0[c] + dt * mm[c] * Sxy[c];
+                o[4][c] = sxz0[c] + dt * mm[c] * Sxz[c];
+                o[5][c] = syz0[c] + dt * mm[c] * Syz[c];
+                o[6][c] = sau0[c] + dt * l2m * (Nx[c] + Ny[c] + Nz[c]);
+            }
+            const int outf[7] = {SXX, SYY, SZZ, SXY, SXZ, SYZ, SAU};
+#pragma unroll
+            for (int j = 0; j < 7; j++) {
+                if (j == 6 && !kSau) break;
+                *reinterpret_cast<float2 *>(w.f[outf[j]] + i0) = make_float2(o[j][0], o[j][1]);
+            }
+            // advance the z windows: the plane five above came in with this item
+            const bool fed = z + 5 < g.nz;
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+#pragma unroll
+                for (int q = 0; q < 8; q++) rv[f][q] = rv[f][q + 1];
+                rv[f][8] = fed ? ld2(C, f * cb + cc) : make_float2(0.f, 0.f);
+            }
+        }
+        __syncthreads();  // every thread is done with buffer b
+        if (s_abort) {
+            if (tid == 0) {
+                mbar_wait_bounded(b ? bar1 : bar0, parity);
+                if (k + 1 < w1) {
+                    const int k1 = k + 1 - w0;
+                    mbar_wait_bounded((k1 & 1) ? bar1 : bar0, (uint32_t)((k1 >> 1) & 1));
+                }
+            }
+            __syncthreads();
+            return;
+        }
+        if (tid == 0 && k + 2 < w1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(k + 2, b);
+        }
+    }
+}
+
 // ------------------------------------------------------------ receivers
 
 __global__ void record(WaveDev w, const long long *__restrict__ rec, int nrec, int nt,
@@ -1636,7 +2078,7 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
     cudaStream_t s = (cudaStream_t)stream;
     WaveDev rv = rev ? *rev : WaveDev{};
     ImageDev im = img ? *img : ImageDev{};
-    if (kc.variant == 2 || kc.variant == 3) {
+    if (kc.variant >= 2) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
         if (kc.zp == 2) {
@@ -1738,11 +2180,151 @@ int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     return 0;
 }
 
+long long fz_psi_floats(const GridDev &g) {
+    const int W = 2 * (g.m - 2), PX = (W + 3) / 4 * 4, PY = (g.nx - 4 + 3) / 4 * 4;
+    const long long ny = g.ny - 4, nz = g.nz - 4;
+    return 3LL * PX * ny * nz + 3LL * PY * W * nz + 3LL * PY * ny * W;
+}
+
+int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
+                     float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps) {
+    maps->ok = false;
+    const int m = g.m, xoff = (int)g.xoff;
+    if ((m & 1) || (g.px & 1) || !psi) return 0;
+    FzGeo geo{};
+    geo.hxi = g.px / 2;
+    geo.hxe = m - 2;
+    const int threads = kZmRows * (geo.hxi + geo.hxe);
+    geo.XC = (xoff + 2) / 4 * 4;
+    geo.XH = geo.XC - kZmHalo;
+    geo.corew = (xoff + g.nx - 2 - geo.XC + 3) / 4 * 4;
+    geo.ytiles = (g.ny - 4 + kZmRows - 1) / kZmRows;
+    geo.nzi = g.nz - 4;
+    geo.W = 2 * (m - 2);
+    geo.PX = (geo.W + 3) / 4 * 4;
+    geo.PY = (g.nx - 4 + 3) / 4 * 4;
+    // one tile per CTA; a row's x window inside the 256-float halo box; the
+    // memory-variable boxes no wider than 256
+    if (threads > kZmMaxThreads || xoff + g.nx + 2 - geo.XH > kZmPitch || geo.corew > kZmPitch ||
+        geo.PY > kZmPitch)
+        return 0;
+    int dev = 0, nsm = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return (int)e;
+    const size_t smem = (size_t)2 * fz_stage(geo) * sizeof(float);
+    if (smem + 1024 > (size_t)smem_max) return 0;
+    // runs: the chunking with the shortest longest-CTA time (a run's first
+    // plane costs about a window refill more)
+    long long best = -1;
+    for (int Q = 1; Q <= 64 && Q <= geo.nzi; Q++) {
+        const int L = (geo.nzi + Q - 1) / Q, R = geo.ytiles * Q;
+        const int G = std::min(nsm, R);
+        const long long cost = (long long)((R + G - 1) / G) * (L + 6);
+        if (best < 0 || cost < best) {
+            best = cost;
+            geo.Q = Q;
+            geo.L = L;
+            geo.R = R;
+        }
+    }
+    geo.psx = psi;
+    geo.psy = psi + 3LL * geo.PX * (g.ny - 4) * (g.nz - 4);
+    geo.psz = geo.psy + 3LL * geo.PY * geo.W * (g.nz - 4);
+    for (int a = 0; a < 3; a++) geo.ax[a] = ax[a];
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return 0;
+        encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    // a tensor of rank 3 or 4 over float32, packed except for its strides
+    auto make = [&](const float *base, int rank, const cuuint64_t *dims, const cuuint32_t *box, FieldMap *out) {
+        CUtensorMap tm;
+        cuuint64_t strides[3];
+        cuuint64_t acc = dims[0];
+        for (int d = 1; d < rank; d++) {
+            strides[d - 1] = acc * sizeof(float);
+            acc *= dims[d];
+        }
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        CUresult r = encode(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, (void *)base, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+        std::memcpy(out->bytes, &tm, sizeof(tm));
+        return true;
+    };
+    // the pitched gridext arrays as 3-D tensors (sy, ny, nz)
+    const cuuint64_t fd[3] = {(cuuint64_t)g.sy, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+    const cuuint32_t hbox[3] = {(cuuint32_t)kZmPitch, (cuuint32_t)kZmBoxH, 1};
+    const cuuint32_t cbox[3] = {(cuuint32_t)geo.corew, (cuuint32_t)kZmRows, 1};
+    const int vel[3] = {VX, VY, VZ};
+    for (int f = 0; f < 3; f++)
+        if (!make(w.f[vel[f]], 3, fd, hbox, &maps->halo[f]) || !make(w.f[vel[f]], 3, fd, cbox, &maps->core[f]))
+            return 0;
+    const float *pts[kFzCore - 3] = {lam, mu, vp, w.f[SXX], w.f[SYY], w.f[SZZ], w.f[SXY], w.f[SXZ], w.f[SYZ],
+                                     w.f[SAU]};
+    for (int f = 0; f < kFzCore - 3; f++)
+        if (!make(pts[f], 3, fd, cbox, &maps->core[3 + f])) return 0;
+    // the memory variables: 4-D (row, rows, planes, 3 arrays), boxes of 4 rows of one plane
+    const cuuint64_t ny = (cuuint64_t)(g.ny - 4), nz = (cuuint64_t)(g.nz - 4), W = (cuuint64_t)geo.W;
+    const cuuint64_t dx4[4] = {(cuuint64_t)geo.PX, ny, nz, 3}, dy4[4] = {(cuuint64_t)geo.PY, W, nz, 3},
+                     dz4[4] = {(cuuint64_t)geo.PY, ny, W, 3};
+    const cuuint32_t bx4[4] = {(cuuint32_t)geo.PX, (cuuint32_t)kZmRows, 1, 3},
+                     by4[4] = {(cuuint32_t)geo.PY, (cuuint32_t)kZmRows, 1, 3};
+    if (!make(geo.psx, 4, dx4, bx4, &maps->psi[0]) || !make(geo.psy, 4, dy4, by4, &maps->psi[1]) ||
+        !make(geo.psz, 4, dz4, by4, &maps->psi[2]))
+        return 0;
+    // The attribute belongs to the kernel, not to this context: contexts of
+    // other grids launch the same kernel with other stage sizes, possibly
+    // at the same time.  Every caller sets the same value, the device's
+    // limit, and each launch asks for its own size below it.
+    const int smem_attr = smem_max - 1024;
+    e = cudaFuncSetAttribute(stress_fz<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress_fz<kRtmFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress_fz<kRev>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
+    if (e != cudaSuccess) return (int)e;
+    maps->geo = geo;
+    maps->threads = threads;
+    maps->grid = std::min(nsm, geo.R);
+    maps->smem = smem;
+    maps->err = err_flag;
+    maps->ok = true;
+    return 0;
+}
+
+int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const float *wavelet, const StepState *st,
+                  int it_off, const FullMaps &maps, void *stream) {
+    if (!maps.ok) return (int)cudaErrorInvalidValue;
+    FzMaps fm;
+    static_assert(sizeof(FzMaps) == sizeof(maps.halo) + sizeof(maps.core) + sizeof(maps.psi), "descriptor layout");
+    std::memcpy(fm.halo, maps.halo, sizeof(maps.halo));
+    std::memcpy(fm.core, maps.core, sizeof(maps.core));
+    std::memcpy(fm.psi, maps.psi, sizeof(maps.psi));
+    cudaStream_t s = (cudaStream_t)stream;
+    const dim3 grid(maps.grid), block(maps.threads);
+    switch (mode) {
+    case kFwd: stress_fz<kFwd><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err); break;
+    case kRtmFwd:
+        stress_fz<kRtmFwd><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err);
+        break;
+    case kRev: stress_fz<kRev><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err); break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    return cerr();
+}
+
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt, int rec_w,
                  const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream,
                  const WaveMaps *maps) {
     cudaStream_t s = (cudaStream_t)stream;
-    if (kc.variant == 3 && maps && maps->ok) {
+    if ((kc.variant == 3 || kc.variant == 4) && maps && maps->ok) {
         ZmMaps zm;
         static_assert(sizeof(ZmMaps) == sizeof(maps->halo) + sizeof(maps->core), "descriptor layout");
         std::memcpy(zm.halo, maps->halo, sizeof(maps->halo));
@@ -1764,7 +2346,7 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
         }
         return cerr();
     }
-    if (kc.variant == 2 || kc.variant == 3) {
+    if (kc.variant >= 2) {
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
         if (kc.zp == 2) {

@@ -75,8 +75,10 @@ typedef struct jv_options {
     int use_graphs;     /* capture the time loop in CUDA graphs (default on)     */
     int graph_steps;    /* time steps per captured graph (0 -> library default)  */
     size_t store_budget;/* max bytes of HBM for the boundary store (0 -> auto)   */
-    int kernel_variant; /* interior kernels: 0 one plane per block, 1 z-marching, 2 x-vectorised,
-                           3 (default) as 2 with a TMA-fed z-marching stress update */
+    int kernel_variant; /* stencil kernels: 0 one plane per block, 1 z-marching, 2 x-vectorised,
+                           3 as 2 with a TMA-fed z-marching stress update, 4 (default) as 3
+                           with the absorbing layers' stress update in the same TMA kernel
+                           (even pml_num and nx; other grids run variant 3's kernels) */
     int zchunk;         /* z planes per block for variant 1 (0 -> auto)          */
     int tile_gx;        /* variant 2: 4-cell x groups per block (0 -> auto)      */
     int tile_gy;        /* variant 2: rows per block (0 -> auto)                 */

@@ -58,6 +58,7 @@ def _create(**kw):
     (dict(pml_min_blocks=2), "min_blocks"),
     (dict(tile_gx=200, tile_gy=2), "tile_gx"),
     (dict(planes_per_thread=3), "planes_per_thread"),
+    (dict(kernel_variant=5), "kernel_variant"),
 ])
 def test_invalid_problems_rejected_without_device(kw, msg):
     with pytest.raises(jv.JvError) as e:

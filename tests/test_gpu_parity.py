@@ -33,7 +33,9 @@ SMALL = [
 ]
 
 
-VARIANTS = [0, 1, 2, 3]  # interior kernels: one plane per block, z-marching, x-vectorised, + TMA z-march stress
+# interior kernels: one plane per block, z-marching, x-vectorised, + TMA z-marching stress, + the stress update
+# of the absorbing layers in the same TMA kernel (variant 4; even pml_num and nx, else variant 3's kernels)
+VARIANTS = [0, 1, 2, 3, 4]
 
 
 @pytest.mark.parametrize("kw", SMALL)
@@ -195,3 +197,74 @@ def test_launch_options_do_not_change_results(synth, kw):
         assert rel_l2(a, b) <= 1e-6
     for k in i0:
         assert rel_l2(i0[k], i1[k]) <= 2e-5, k
+
+
+# grids on which variant 4's full-gridext stress kernel runs (even pml_num and
+# nx): region boundaries at every tile-row offset, the smallest pml, sources
+# and receivers next to the absorbing layers
+FULL = [
+    dict(n=(26, 14, 16), pml=8, nt=120, seed=31, shot_idx=[(1, 2, 1)]),
+    dict(n=(40, 12, 10), pml=10, nt=110, seed=32, nrec=40),
+    dict(n=(12, 30, 22), pml=4, nt=130, seed=33, shot_idx=[(10, 27, 20)]),
+    dict(n=(18, 9, 27), pml=6, nt=100, seed=34, shot_idx=[(9, 4, 13)]),
+]
+
+
+def _kernels(ctx):
+    return set(ctx.profile())
+
+
+@pytest.mark.parametrize("kw", FULL)
+def test_full_stress_kernel_forward_vs_oracle(oracle, synth, kw):
+    s = synth.small_case(**kw)
+    ref = oracle.forward(_problem(oracle, s))
+    with jv.Context.from_survey(s, kernel_variant=4) as ctx:
+        tr = ctx.forward(0)
+        ctx.set_profiling(True)
+        ctx.forward(0)
+        names = _kernels(ctx)
+    assert "stress_fz_fwd" in names and "stress_pml" not in names, names
+    for a, b in zip(tr, ref):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
+
+
+@pytest.mark.parametrize("kw", FULL[:2])
+@pytest.mark.parametrize("w", [1, 4])
+def test_full_stress_kernel_rtm_vs_oracle(oracle, synth, kw, w):
+    s = synth.small_case(**dict(kw, rec_width=w))
+    p = _problem(oracle, s, w)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    obs32 = [o.astype(np.float32) for o in obs]
+    with jv.Context.from_survey(s, kernel_variant=4) as ctx:
+        ctx.set_profiling(True)
+        ctx.rtm_shot(0, obs32)
+        names = _kernels(ctx)
+        raw = ctx.images()
+    assert {"stress_fz_rtmfwd", "stress_fz_rev"} <= names and "stress_pml_sau" not in names, names
+    for k in ("ip", "pp", "ps", "sp", "ss"):
+        assert np.all(np.isfinite(raw[k]))
+        assert rel_l2(raw[k], ref[k]) <= 5e-5, (w, k, rel_l2(raw[k], ref[k]))
+
+
+def test_full_stress_kernel_vs_oracle_at_size(oracle, synth):
+    """Variant 4 against the oracle on a grid with several tiles per CTA and
+    runs of planes that start inside a column, as accurate as variant 3's
+    split kernels on the same problem."""
+    s = synth.scaled_cfg2(44, 110, pml=10)
+    p = _problem(oracle, s)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    obs32 = [o.astype(np.float32) for o in obs]
+    err = {}
+    for v in (3, 4):
+        with jv.Context.from_survey(s, kernel_variant=v) as ctx:
+            tr = ctx.forward(0)
+            ctx.rtm_shot(0, obs32)
+            im = ctx.images()
+        err[v] = ([rel_l2(a, b) for a, b in zip(tr, obs)], {k: rel_l2(im[k], ref[k]) for k in im})
+    for e in err[4][0]:
+        assert e <= 2e-5, err
+    for k, e in err[4][1].items():
+        assert e <= max(5e-5, 1.5 * err[3][1][k]), (k, err)

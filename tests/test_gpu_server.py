@@ -63,6 +63,22 @@ def test_mixed_requests_match_each_run_alone():
     assert 0 < st["p50_ms"] <= st["p99_ms"] and st["mean_ms"] > 0
 
 
+def test_concurrent_grids_of_different_stage_sizes():
+    """Requests whose full-gridext stress kernel needs different shared
+    memory (other x widths and absorbing widths) running side by side."""
+    cases = [synth.small_case(n=(22, 20, 16), pml=6, nt=60, seed=41),
+             synth.small_case(n=(60, 14, 12), pml=8, nt=60, seed=42),
+             synth.small_case(n=(96, 10, 10), pml=10, nt=60, seed=43)]
+    plan = [(c, k) for c in cases for k in (jv.JOB_FORWARD, jv.JOB_RTM)] * 2
+    want = {(id(c), k): _alone(c, k) for c, k in plan[:6]}
+    with jv.Server(slots=6, budget=1 << 32) as srv:
+        subs = [srv.submit_survey(k, c) for c, k in plan]
+        for rid, _ in subs:
+            assert srv.wait(rid, timeout=180.0) == jv.JV_OK
+    for (c, k), (_, got) in zip(plan, subs):
+        _check_same(k, got, want[(id(c), k)])
+
+
 def test_budget_holds_while_requests_run():
     s = _cases()[0]
     one = jv.footprint(s.nx, s.ny, s.nz, s.pml, s.nt, s.rec_width, jv.JOB_RTM, n_recv=len(s.recvs))
