@@ -140,6 +140,7 @@ BYTES_PER_CELL = {
     "stress_phy_rev": 4 * (3 + 2 + 7) + 4 * 7,
     "stress_phy_rtmfwd": 4 * (3 + 2 + 7) + 4 * 7,
     "stress_phy_fwd": 4 * (3 + 2 + 6) + 4 * 6,
+    "velp_rev": 4 * (1 + 1 + 3) + 4 * 3,
 }
 
 
@@ -176,10 +177,13 @@ def pml_bytes(s, name):
     return float(cells * per + axes * 3 * 8)
 
 
-# the full-gridext stress kernel (variant 4) does the work of two launches
+# the full-gridext kernels (variant 4) do the work of two launches
 FUSED = {"stress_fz_fwd": ("stress_phy_fwd", "stress_pml"),
          "stress_fz_rtmfwd": ("stress_phy_rtmfwd", "stress_pml_sau"),
-         "stress_fz_rev": ("stress_phy_rev", "stress_pml_sau")}
+         "stress_fz_rev": ("stress_phy_rev", "stress_pml_sau"),
+         "vel_fz_fwd": ("vel_phy_fwd", "vel_pml"),
+         "vel_fz_rtmfwd": ("vel_phy_rtmfwd", "vel_pml"),
+         "vel_fz_rev": ("vel_phy_fwd", "vel_pml")}  # the receiver side's P-wave part is velp_rev
 
 
 def kernel_bytes(s, name):

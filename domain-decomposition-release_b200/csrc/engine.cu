@@ -280,13 +280,13 @@ size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm) {
     size_t b = (4 * fe + 32) * sizeof(float);                 // model
     b += (kNumFld * fe + 32) * sizeof(float);                 // forward wavefield
     b += (size_t)psi * sizeof(float);                         // its memory variables
-    b += (size_t)fz_psi_floats(g) * sizeof(float);            // the full-gridext kernel's stress ones
+    b += (size_t)2 * fz_psi_floats(g) * sizeof(float);        // the full-gridext kernels' ones
     b += 5 * nphy * sizeof(double);                           // stacks
     b += 16 * ((size_t)grid.nx + grid.ny + grid.nz + 2 * grid.pml * 3) + (1 << 20);  // tables, state, slack
     if (rtm) {
         long long per = 0, blk = 0;
         vowr_segments(g, rec_width, &per, &blk);
-        b += (kNumFld * fe + 32) * sizeof(float) + (size_t)(psi + fz_psi_floats(g)) * sizeof(float);  // receiver wavefield
+        b += (kNumFld * fe + 32) * sizeof(float) + (size_t)(psi + 2 * fz_psi_floats(g)) * sizeof(float);  // receiver wavefield
         b += (size_t)per * (size_t)(nt > 1 ? nt - 1 : 0) * sizeof(float);          // boundary store
         b += 5 * ((nphy + 63) / 64 * 64) * sizeof(float);                           // shot image
         b += (size_t)blk * sizeof(int) + 64 * sizeof(SegDev);
@@ -406,10 +406,10 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         cpF_ = make_cpml((float *)p);
     }
     if (kc_.variant == 4) {
-        fz_psi_total_ = fz_psi_floats(g_);
+        fz_psi_total_ = 2 * fz_psi_floats(g_);  // velocity and stress sets
         JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
         fzpsiF_ = (float *)p;
-        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, axis_d_, fzpsiF_, zm_err_, &fullF_));
+        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, &fullF_));
     }
 
     // wavelet and step state
@@ -656,8 +656,12 @@ Status Engine::launch_step(int kind, int off, bool advance) {
     const int rw = opt_.rec_width;
     switch (kind) {
     case kStepModel:
-        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
-        JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        if (fullF_.ok) {
+            JV_L("vel_fz_fwd", k_vel_full(g_, F_, dt, fullF_, s));
+        } else {
+            JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
+            JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        }
         if (fullF_.ok) {
             JV_L("stress_fz_fwd", k_stress_full(kFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
         } else {
@@ -669,8 +673,12 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
-        JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
-        JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        if (fullF_.ok) {
+            JV_L("vel_fz_rtmfwd", k_vel_full(g_, F_, dt, fullF_, s));
+        } else {
+            JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
+            JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        }
         if (fullF_.ok) {
             // the boundary boxes lie in the absorbing layers: pack them after their update
             JV_L("stress_fz_rtmfwd", k_stress_full(kRtmFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
@@ -688,8 +696,13 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // injection + reverse velocity, stress boundary layers of step it-1
         JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, off, s));
         JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
-        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
-        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        if (fullR_.ok) {
+            JV_L("vel_fz_rev", k_vel_full(g_, R_, dt, fullR_, s));
+            JV_L("velp_rev", k_velp(g_, R_, rho_, dt, s));
+        } else {
+            JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
+            JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        }
         JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
@@ -803,7 +816,7 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         if (kc_.variant == 4) {
             JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
             fzpsiR_ = (float *)p;
-            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, axis_d_, fzpsiR_, zm_err_, &fullR_));
+            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, rho_, axis_d_, fzpsiR_, zm_err_, &fullR_));
         }
     }
     if (!shot_img_.ip) {

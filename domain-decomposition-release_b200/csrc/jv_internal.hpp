@@ -154,7 +154,8 @@ struct FzGeo {
     const float4 *ax[3];
 };
 
-// floats of the axis-major stress memory variables of one wavefield
+// floats of one set (3 axes x 3 arrays) of axis-major memory variables; a
+// wavefield holds two, the velocity set first, then the stress set
 long long fz_psi_floats(const GridDev &g);
 
 // TMA descriptors of the full-gridext stress kernel of one wavefield
@@ -162,11 +163,14 @@ struct FullMaps {
     FieldMap halo[3];             // vx vy vz
     FieldMap core[kZmCore + 1];   // vx vy vz, lam, mu, vp, sxx syy szz sxy sxz syz, sau
     FieldMap psi[3];              // the x, y and z memory-variable arrays (4-D: 3 arrays each)
+    // the velocity kernel's: halo planes sxy syy syz, bands sxx sxz, core
+    // tiles rho vp vx vy vz, window feed sxz syz szz, memory variables
+    FieldMap vhalo[3], vband[2], vcore[5], vfeed[3], vpsi[3];
     bool ok = false;              // false: variant 4 is not available for this grid
-    FzGeo geo{};
+    FzGeo geo{}, vgeo{};          // stress and velocity kernels (their memory-variable sets differ)
     int threads = 0;
     int grid = 0;
-    size_t smem = 0;
+    size_t smem = 0, vsmem = 0;
     int *err = nullptr;
 };
 
@@ -204,11 +208,15 @@ int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const
 // row of more than 512 threads or a halo row wider than 256 floats, the
 // driver entry point missing).  Returns a cudaError_t.
 int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
-                     float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps);
+                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps);
 // Stress update of every updated cell of gridext, interior and absorbing
 // layers in one launch (modes kFwd, kRtmFwd, kRev).
 int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const float *wavelet, const StepState *st,
                   int it_off, const FullMaps &maps, void *stream);
+// Velocity update of every updated cell of gridext (variant 4; vx, vy, vz)
+int k_vel_full(const GridDev &g, const WaveDev &w, float dt, const FullMaps &maps, void *stream);
+// P-wave velocities (vxp, vyp, vzp) of the physical cells, receiver wavefield
+int k_velp(const GridDev &g, const WaveDev &w, const float *rho, float dt, void *stream);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
               const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,

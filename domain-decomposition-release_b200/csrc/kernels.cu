@@ -1864,6 +1864,418 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     }
 }
 
+// --------------------------------------------- full-gridext velocity update
+//
+// Variant 4 of the velocity update for the steps that carry absorbing
+// layers: vel_phy's 8th-order update of the physical cells
+// (FD/fdtd3d_0_base_module/fdtd3d_base_3_kernel_device_meat.hpp) and
+// vel_pml_group's 4th-order CPML update of the others in one persistent
+// z-marching kernel, with the tiling, thread layout, run schedule and
+// axis-major memory variables of stress_fz.  Per item TMA brings halo
+// planes (12 rows) of sxy, syy, syz; 4-row bands with the x halo of sxx
+// and sxz; the core tiles of rho, vp, vx, vy, vz; the window feed of sxz,
+// syz, szz five planes ahead; the memory-variable boxes.  The z windows
+// hold sxz, syz, szz.  The P-wave velocities of the receiver wavefield are
+// updated by velp_v4 beside it.
+
+constexpr int kFvStage = 3 * kZmHB + 10 * kZmCB;  // halo planes, 2 bands, 5 core tiles, 3 feed tiles
+
+struct FvMaps {
+    CUtensorMap halo[3];  // sxy syy syz
+    CUtensorMap band[2];  // sxx sxz
+    CUtensorMap core[5];  // rho vp vx vy vz
+    CUtensorMap feed[3];  // sxz syz szz (core boxes)
+    CUtensorMap psi[3];
+};
+
+__host__ __device__ inline int fv_stage(const FzGeo &g) {
+    return kFvStage + fz_round32(12 * g.PX) + 2 * fz_round32(12 * g.PY);
+}
+
+__global__ void __launch_bounds__(kZmMaxThreads, 1)
+    vel_fz(GridDev g, const __grid_constant__ FvMaps maps, WaveDev w, float dt, const __grid_constant__ FzGeo geo,
+           int *err) {
+    extern __shared__ __align__(128) float sm[];
+    constexpr int hb = kZmHB, cb = kZmCB, boxw = kZmPitch;
+    const int stage = fv_stage(geo);
+    const int pxr = fz_round32(12 * geo.PX), pyr = fz_round32(12 * geo.PY);
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int s_abort;
+    const int nrun = (geo.R - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int w0 = 0, w1 = nrun * geo.L;
+    if (nrun <= 0) return;
+    auto item_at = [&](int item, int &yt, int &z) {
+        const int j = item / geo.L, off = item - j * geo.L;
+        const int rr = (int)blockIdx.x + j * (int)gridDim.x;
+        const int q = rr / geo.ytiles;
+        yt = rr - q * geo.ytiles;
+        z = 2 + q * geo.L + off;
+    };
+    const int tid = threadIdx.x;
+    const int m = g.m;
+    const int ti = kZmRows * geo.hxi;
+    const bool xabs = tid >= ti;
+    int r, x;
+    if (!xabs) {
+        r = tid / geo.hxi;
+        x = m + 2 * (tid - r * geo.hxi);
+    } else {
+        const int e = tid - ti, half = geo.hxe / 2;
+        r = e / geo.hxe;
+        const int q = e - r * geo.hxe;
+        x = q < half ? 2 + 2 * q : m + g.px + 2 * (q - half);
+    }
+    const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+    const uint32_t bytes_feed = (uint32_t)(3 * geo.corew * kZmRows) * 4u;
+    const uint32_t bytes_all = (uint32_t)(3 * hb + 2 * cb + 5 * geo.corew * kZmRows) * 4u + bytes_feed;
+    const uint32_t bytes_psx = (uint32_t)(12 * geo.PX) * 4u, bytes_psy = (uint32_t)(12 * geo.PY) * 4u;
+    auto issue = [&](int item, int b) {
+        int yt, z;
+        item_at(item, yt, z);
+        const uint32_t bar = b ? bar1 : bar0;
+        if (z >= g.nz - 2) {
+            mbar_expect(bar, 0);
+            return;
+        }
+        const int Y = 2 + yt * kZmRows;
+        float *base = sm + b * stage;
+        const bool feed = z + 5 < g.nz;
+        const bool zab = z < m || z >= m + g.pz;
+        const bool ylo = Y < m, yhi = Y + kZmRows - 1 >= m + g.py;
+        mbar_expect(bar, (feed ? bytes_all : bytes_all - bytes_feed) + bytes_psx + (ylo || yhi ? bytes_psy : 0u) +
+                             (zab ? bytes_psy : 0u));
+        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], geo.XH, Y - kZmHalo, z, bar);
+        for (int f = 0; f < 2; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.band[f], geo.XH, Y, z, bar);
+        for (int f = 0; f < 5; f++)
+            tma_load_3d(smem_u32(base + 3 * hb + (2 + f) * cb), &maps.core[f], geo.XC, Y, z, bar);
+        if (feed)
+            for (int f = 0; f < 3; f++)
+                tma_load_3d(smem_u32(base + 3 * hb + (7 + f) * cb), &maps.feed[f], geo.XC, Y, z + 5, bar);
+        float *ps = base + kFvStage;
+        tma_load_4d(smem_u32(ps), &maps.psi[0], 0, Y - 2, z - 2, 0, bar);
+        if (ylo || yhi)
+            tma_load_4d(smem_u32(ps + pxr), &maps.psi[1], 0, ylo ? Y - 2 : m - 2 + Y - (m + g.py), z - 2, 0, bar);
+        if (zab)
+            tma_load_4d(smem_u32(ps + pxr + pyr), &maps.psi[2], 0, Y - 2, z < m ? z - 2 : m - 2 + z - (m + g.pz), 0,
+                        bar);
+    };
+    if (tid == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar1, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        issue(w0, 0);
+        if (w0 + 1 < w1) issue(w0 + 1, 1);
+    }
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    const int hcol = (int)g.xoff + x - geo.XH;
+    const int ccol = (int)g.xoff + x - geo.XC;
+    float2 rv[3][9];  // z windows: planes z-4 .. z+4 of sxz, syz, szz
+    const float *fv[3] = {w.f[SXZ], w.f[SYZ], w.f[SZZ]};
+    int cur_yt = -1, cur_z = -2;
+    for (int k = w0; k < w1; k++) {
+        int yt, z;
+        item_at(k, yt, z);
+        const int y = 2 + yt * kZmRows + r;
+        const bool live = y < g.ny - 2 && z < g.nz - 2;
+        const int i0 = (int)g.xoff + x + sy * y + sz * z;
+        const int b = (k - w0) & 1;
+        const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
+        const float *base = sm + b * stage;
+        const int cc = r * geo.corew + ccol;
+        if (yt != cur_yt || z != cur_z + 1) {
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+#pragma unroll
+                for (int q = 0; q < 9; q++) {
+                    const int zq = z + q - 4;
+                    rv[f][q] = (live && zq >= 0 && zq < g.nz)
+                                   ? __ldg(reinterpret_cast<const float2 *>(fv[f] + i0 + (q - 4) * sz))
+                                   : make_float2(0.f, 0.f);
+                }
+            }
+        }
+        cur_yt = yt;
+        cur_z = z;
+        if (!mbar_wait_bounded(b ? bar1 : bar0, parity)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+        }
+        if (live) {
+            const float *H = base;                  // halo planes: sxy, syy, syz
+            const float *BD = base + 3 * hb;         // bands: sxx, sxz
+            const float *C = base + 3 * hb + 2 * cb; // core: rho, vp, vx, vy, vz
+            const float *FD = base + 3 * hb + 7 * cb;
+            const int c0 = (r + kZmHalo) * boxw + hcol;  // a halo plane
+            const int b0 = r * boxw + hcol;              // a band
+            auto ld2 = [&](const float *F, int off) { return *reinterpret_cast<const float2 *>(F + off); };
+            auto xwin2 = [&](const float *F, int at, float *e) {
+#pragma unroll
+                for (int j = 0; j < 5; j++) {
+                    const float2 v = ld2(F, at - 4 + 2 * j);
+                    e[2 * j] = v.x;
+                    e[2 * j + 1] = v.y;
+                }
+            };
+            const bool zabs = z < m || z >= m + g.pz;
+            const bool yabs = y < m || y >= m + g.py;
+            const bool cpml = xabs || yabs || zabs;
+            float Dx[2], Dy[2], Dz[2];
+            float e[10];
+            if (!cpml) {
+                const float *cf = c_list[kPhyHalf];
+                // vx: Dp_x sxx + Dm_y sxy + Dm_z sxz
+                xwin2(BD, b0, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) t += cf[q] * (e[4 + c + q + 1] - e[4 + c - q]);
+                    Dx[c] = t * rdx;
+                }
+                {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float2 a = ld2(H, c0 + q * boxw), bb = ld2(H, c0 - (q + 1) * boxw);
+                        t.x += cf[q] * (a.x - bb.x);
+                        t.y += cf[q] * (a.y - bb.y);
+                    }
+                    Dx[0] += t.x * rdy;
+                    Dx[1] += t.y * rdy;
+                    t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        t.x += cf[q] * (rv[0][4 + q].x - rv[0][4 - q - 1].x);
+                        t.y += cf[q] * (rv[0][4 + q].y - rv[0][4 - q - 1].y);
+                    }
+                    Dx[0] += t.x * rdz;
+                    Dx[1] += t.y * rdz;
+                }
+                // vy: Dm_x sxy + Dp_y syy + Dm_z syz
+                xwin2(H, c0, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) t += cf[q] * (e[4 + c + q] - e[4 + c - q - 1]);
+                    Dy[c] = t * rdx;
+                }
+                {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float2 a = ld2(H + hb, c0 + (q + 1) * boxw), bb = ld2(H + hb, c0 - q * boxw);
+                        t.x += cf[q] * (a.x - bb.x);
+                        t.y += cf[q] * (a.y - bb.y);
+                    }
+                    Dy[0] += t.x * rdy;
+                    Dy[1] += t.y * rdy;
+                    t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        t.x += cf[q] * (rv[1][4 + q].x - rv[1][4 - q - 1].x);
+                        t.y += cf[q] * (rv[1][4 + q].y - rv[1][4 - q - 1].y);
+                    }
+                    Dy[0] += t.x * rdz;
+                    Dy[1] += t.y * rdz;
+                }
+                // vz: Dm_x sxz + Dm_y syz + Dp_z szz
+                xwin2(BD + cb, b0, e);
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    float t = 0.f;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) t += cf[q] * (e[4 + c + q] - e[4 + c - q - 1]);
+                    Dz[c] = t * rdx;
+                }
+                {
+                    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float2 a = ld2(H + 2 * hb, c0 + q * boxw), bb = ld2(H + 2 * hb, c0 - (q + 1) * boxw);
+                        t.x += cf[q] * (a.x - bb.x);
+                        t.y += cf[q] * (a.y - bb.y);
+                    }
+                    Dz[0] += t.x * rdy;
+                    Dz[1] += t.y * rdy;
+                    t = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        t.x += cf[q] * (rv[2][4 + q + 1].x - rv[2][4 - q].x);
+                        t.y += cf[q] * (rv[2][4 + q + 1].y - rv[2][4 - q].y);
+                    }
+                    Dz[0] += t.x * rdz;
+                    Dz[1] += t.y * rdz;
+                }
+            } else {
+                const float k0 = c_dc2[0], k1 = c_dc2[1];
+                // sxx_x syx_x szx_x | sxy_y syy_y szy_y | sxz_z syz_z szz_z
+                float d[9][2];
+                xwin2(BD, b0, e);  // sxx: Dp_x
+#pragma unroll
+                for (int c = 0; c < 2; c++) d[0][c] = (k0 * (e[5 + c] - e[4 + c]) + k1 * (e[6 + c] - e[3 + c])) * rdx;
+                xwin2(H, c0, e);  // sxy: Dm_x
+#pragma unroll
+                for (int c = 0; c < 2; c++) d[1][c] = (k0 * (e[4 + c] - e[3 + c]) + k1 * (e[5 + c] - e[2 + c])) * rdx;
+                xwin2(BD + cb, b0, e);  // sxz: Dm_x
+#pragma unroll
+                for (int c = 0; c < 2; c++) d[2][c] = (k0 * (e[4 + c] - e[3 + c]) + k1 * (e[5 + c] - e[2 + c])) * rdx;
+#pragma unroll
+                for (int f = 0; f < 3; f += 2) {
+                    // Dm_y sxy -> d[3], Dm_y syz -> d[5]
+                    const float *F = H + f * hb;
+                    const float2 a = ld2(F, c0), bb = ld2(F, c0 - boxw), cq = ld2(F, c0 + boxw),
+                                 dq = ld2(F, c0 - 2 * boxw);
+                    d[3 + f][0] = (k0 * (a.x - bb.x) + k1 * (cq.x - dq.x)) * rdy;
+                    d[3 + f][1] = (k0 * (a.y - bb.y) + k1 * (cq.y - dq.y)) * rdy;
+                }
+                {
+                    // Dp_y syy -> d[4]
+                    const float *F = H + hb;
+                    const float2 a = ld2(F, c0 + boxw), bb = ld2(F, c0), cq = ld2(F, c0 + 2 * boxw),
+                                 dq = ld2(F, c0 - boxw);
+                    d[4][0] = (k0 * (a.x - bb.x) + k1 * (cq.x - dq.x)) * rdy;
+                    d[4][1] = (k0 * (a.y - bb.y) + k1 * (cq.y - dq.y)) * rdy;
+                }
+                // Dm_z sxz -> d[6], syz -> d[7]; Dp_z szz -> d[8]
+#pragma unroll
+                for (int f = 0; f < 2; f++) {
+                    d[6 + f][0] = (k0 * (rv[f][4].x - rv[f][3].x) + k1 * (rv[f][5].x - rv[f][2].x)) * rdz;
+                    d[6 + f][1] = (k0 * (rv[f][4].y - rv[f][3].y) + k1 * (rv[f][5].y - rv[f][2].y)) * rdz;
+                }
+                d[8][0] = (k0 * (rv[2][5].x - rv[2][4].x) + k1 * (rv[2][6].x - rv[2][3].x)) * rdz;
+                d[8][1] = (k0 * (rv[2][5].y - rv[2][4].y) + k1 * (rv[2][6].y - rv[2][3].y)) * rdz;
+                const float *PS = base + kFvStage;
+                const int zi = z - 2, yi = y - 2, xi = x - 2;
+                const float2 vp2 = ld2(C, cb + cc);
+                const float vpc[2] = {vp2.x, vp2.y};
+                float A[2], B[2], Ah[2], Bh[2];
+                auto upd = [&](const float *sp, float *gp, const float *BB, const float *AA, float *dd) {
+                    float2 v = *reinterpret_cast<const float2 *>(sp);
+                    v.x = BB[0] * v.x + AA[0] * dd[0];
+                    v.y = BB[1] * v.y + AA[1] * dd[1];
+                    *reinterpret_cast<float2 *>(gp) = v;
+                    dd[0] += v.x;
+                    dd[1] += v.y;
+                };
+                if (xabs) {
+                    const int xc = x < m ? x - 2 : m - 2 + x - (m + g.px);
+                    const long long a0 = ((long long)zi * (g.ny - 4) + yi) * geo.PX + xc;
+                    const long long as = (long long)(g.nz - 4) * (g.ny - 4) * geo.PX;
+                    const int s0 = r * geo.PX + xc, ss = 4 * geo.PX;
+#pragma unroll
+                    for (int c = 0; c < 2; c++) cpml_coef(vpc[c], __ldg(&geo.ax[0][x + c]), dt, A[c], B[c], Ah[c], Bh[c]);
+                    upd(PS + s0, geo.psx + a0, Bh, Ah, d[0]);
+                    upd(PS + s0 + ss, geo.psx + a0 + as, B, A, d[1]);
+                    upd(PS + s0 + 2 * ss, geo.psx + a0 + 2 * as, B, A, d[2]);
+                }
+                if (yabs) {
+                    const int yc = y < m ? y - 2 : m - 2 + y - (m + g.py);
+                    const long long a0 = ((long long)zi * geo.W + yc) * geo.PY + xi;
+                    const long long as = (long long)(g.nz - 4) * geo.W * geo.PY;
+                    const int s0 = pxr + r * geo.PY + xi, ss = 4 * geo.PY;
+                    const float4 ty = __ldg(&geo.ax[1][y]);
+#pragma unroll
+                    for (int c = 0; c < 2; c++) cpml_coef(vpc[c], ty, dt, A[c], B[c], Ah[c], Bh[c]);
+                    upd(PS + s0, geo.psy + a0, B, A, d[3]);
+                    upd(PS + s0 + ss, geo.psy + a0 + as, Bh, Ah, d[4]);
+                    upd(PS + s0 + 2 * ss, geo.psy + a0 + 2 * as, B, A, d[5]);
+                }
+                if (zabs) {
+                    const int zc = z < m ? z - 2 : m - 2 + z - (m + g.pz);
+                    const long long a0 = ((long long)zc * (g.ny - 4) + yi) * geo.PY + xi;
+                    const long long as = (long long)geo.W * (g.ny - 4) * geo.PY;
+                    const int s0 = pxr + pyr + r * geo.PY + xi, ss = 4 * geo.PY;
+                    const float4 tz = __ldg(&geo.ax[2][z]);
+#pragma unroll
+                    for (int c = 0; c < 2; c++) cpml_coef(vpc[c], tz, dt, A[c], B[c], Ah[c], Bh[c]);
+                    upd(PS + s0, geo.psz + a0, B, A, d[6]);
+                    upd(PS + s0 + ss, geo.psz + a0 + as, B, A, d[7]);
+                    upd(PS + s0 + 2 * ss, geo.psz + a0 + 2 * as, Bh, Ah, d[8]);
+                }
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    Dx[c] = d[0][c] + d[3][c] + d[6][c];
+                    Dy[c] = d[1][c] + d[4][c] + d[7][c];
+                    Dz[c] = d[2][c] + d[5][c] + d[8][c];
+                }
+            }
+            const float2 rh = ld2(C, cc);
+            const float dtr[2] = {dt / rh.x, dt / rh.y};
+            const float2 v0 = ld2(C, 2 * cb + cc), v1 = ld2(C, 3 * cb + cc), v2 = ld2(C, 4 * cb + cc);
+            *reinterpret_cast<float2 *>(w.f[VX] + i0) = make_float2(v0.x + dtr[0] * Dx[0], v0.y + dtr[1] * Dx[1]);
+            *reinterpret_cast<float2 *>(w.f[VY] + i0) = make_float2(v1.x + dtr[0] * Dy[0], v1.y + dtr[1] * Dy[1]);
+            *reinterpret_cast<float2 *>(w.f[VZ] + i0) = make_float2(v2.x + dtr[0] * Dz[0], v2.y + dtr[1] * Dz[1]);
+            const bool fed = z + 5 < g.nz;
+#pragma unroll
+            for (int f = 0; f < 3; f++) {
+#pragma unroll
+                for (int q = 0; q < 8; q++) rv[f][q] = rv[f][q + 1];
+                rv[f][8] = fed ? ld2(FD, f * cb + cc) : make_float2(0.f, 0.f);
+            }
+        }
+        __syncthreads();
+        if (s_abort) {
+            if (tid == 0) {
+                mbar_wait_bounded(b ? bar1 : bar0, parity);
+                if (k + 1 < w1) {
+                    const int k1 = k + 1 - w0;
+                    mbar_wait_bounded((k1 & 1) ? bar1 : bar0, (uint32_t)((k1 >> 1) & 1));
+                }
+            }
+            __syncthreads();
+            return;
+        }
+        if (tid == 0 && k + 2 < w1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(k + 2, b);
+        }
+    }
+}
+
+// P-wave velocities of the receiver wavefield (REV mode of vel_group4's
+// P part: Dp of sau on every axis, physical cells), for variant 4 where
+// vel_fz updates vx, vy, vz.
+__global__ void __launch_bounds__(256, 4) velp_v4(GridDev g, WaveDev w, const float *__restrict__ rho, float dt) {
+    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
+    const int pk = blockIdx.z;
+    if (pi0 >= g.px || pj >= g.py || pk >= g.pz) return;
+    const int nvalid = min(4, g.px - pi0);
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    const int i0 = (int)g.xoff + (pi0 + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
+    const float *cx[4];
+    xcoefs<kRev>(pi0, g.px, 0, cx);
+    const float *c = c_list[kPhyHalf];
+    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
+    float dtr[4], t[4], win[12], p[4];
+    {
+        const float4 r4 = ld4(rho, i0);
+        dtr[0] = dt / r4.x; dtr[1] = dt / r4.y; dtr[2] = dt / r4.z; dtr[3] = dt / r4.w;
+    }
+    xwin(w.f[SAU], i0, win);
+    xdp(win, cx, t);
+    f4a(p, ldw4(w.f[VXP], i0));
+#pragma unroll
+    for (int q = 0; q < 4; q++) p[q] += dtr[q] * (t[q] * rdx);
+    st4(w.f[VXP], i0, p, nvalid);
+    sdp(w.f[SAU], i0, sy, c, t);
+    f4a(p, ldw4(w.f[VYP], i0));
+#pragma unroll
+    for (int q = 0; q < 4; q++) p[q] += dtr[q] * (t[q] * rdy);
+    st4(w.f[VYP], i0, p, nvalid);
+    sdp(w.f[SAU], i0, sz, c, t);
+    f4a(p, ldw4(w.f[VZP], i0));
+#pragma unroll
+    for (int q = 0; q < 4; q++) p[q] += dtr[q] * (t[q] * rdz);
+    st4(w.f[VZP], i0, p, nvalid);
+}
+
 // ------------------------------------------------------------ receivers
 
 __global__ void record(WaveDev w, const long long *__restrict__ rec, int nrec, int nt,
@@ -2187,7 +2599,7 @@ long long fz_psi_floats(const GridDev &g) {
 }
 
 int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
-                     float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps) {
+                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps) {
     maps->ok = false;
     const int m = g.m, xoff = (int)g.xoff;
     if ((m & 1) || (g.px & 1) || !psi) return 0;
@@ -2215,6 +2627,8 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     if (e != cudaSuccess) return (int)e;
     const size_t smem = (size_t)2 * fz_stage(geo) * sizeof(float);
     if (smem + 1024 > (size_t)smem_max) return 0;
+    const size_t vsmem = (size_t)2 * fv_stage(geo) * sizeof(float);
+    if (vsmem + 1024 > (size_t)smem_max) return 0;
     // runs: the chunking with the shortest longest-CTA time (a run's first
     // plane costs about a window refill more)
     long long best = -1;
@@ -2229,10 +2643,15 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
             geo.R = R;
         }
     }
-    geo.psx = psi;
-    geo.psy = psi + 3LL * geo.PX * (g.ny - 4) * (g.nz - 4);
-    geo.psz = geo.psy + 3LL * geo.PY * geo.W * (g.nz - 4);
     for (int a = 0; a < 3; a++) geo.ax[a] = ax[a];
+    FzGeo vgeo = geo;
+    // memory variables: the velocity set, then the stress set
+    vgeo.psx = psi;
+    vgeo.psy = vgeo.psx + 3LL * geo.PX * (g.ny - 4) * (g.nz - 4);
+    vgeo.psz = vgeo.psy + 3LL * geo.PY * geo.W * (g.nz - 4);
+    geo.psx = psi + fz_psi_floats(g);
+    geo.psy = geo.psx + (vgeo.psy - vgeo.psx);
+    geo.psz = geo.psx + (vgeo.psz - vgeo.psx);
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -2279,24 +2698,64 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     if (!make(geo.psx, 4, dx4, bx4, &maps->psi[0]) || !make(geo.psy, 4, dy4, by4, &maps->psi[1]) ||
         !make(geo.psz, 4, dz4, by4, &maps->psi[2]))
         return 0;
+    if (!make(vgeo.psx, 4, dx4, bx4, &maps->vpsi[0]) || !make(vgeo.psy, 4, dy4, by4, &maps->vpsi[1]) ||
+        !make(vgeo.psz, 4, dz4, by4, &maps->vpsi[2]))
+        return 0;
+    // the velocity kernel's field boxes
+    const cuuint32_t bbox[3] = {(cuuint32_t)kZmPitch, (cuuint32_t)kZmRows, 1};
+    const int vh[3] = {SXY, SYY, SYZ}, vb[2] = {SXX, SXZ}, vf[3] = {SXZ, SYZ, SZZ};
+    const float *vc[5] = {rho, vp, w.f[VX], w.f[VY], w.f[VZ]};
+    for (int f = 0; f < 3; f++)
+        if (!make(w.f[vh[f]], 3, fd, hbox, &maps->vhalo[f]) || !make(w.f[vf[f]], 3, fd, cbox, &maps->vfeed[f]))
+            return 0;
+    for (int f = 0; f < 2; f++)
+        if (!make(w.f[vb[f]], 3, fd, bbox, &maps->vband[f])) return 0;
+    for (int f = 0; f < 5; f++)
+        if (!make(vc[f], 3, fd, cbox, &maps->vcore[f])) return 0;
     // The attribute belongs to the kernel, not to this context: contexts of
     // other grids launch the same kernel with other stage sizes, possibly
     // at the same time.  Every caller sets the same value, the device's
     // limit, and each launch asks for its own size below it.
     const int smem_attr = smem_max - 1024;
-    e = cudaFuncSetAttribute(stress_fz<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
+    e = cudaFuncSetAttribute(vel_fz, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(stress_fz<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(stress_fz<kRtmFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(stress_fz<kRev>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
     if (e != cudaSuccess) return (int)e;
     maps->geo = geo;
+    maps->vgeo = vgeo;
     maps->threads = threads;
     maps->grid = std::min(nsm, geo.R);
     maps->smem = smem;
+    maps->vsmem = vsmem;
     maps->err = err_flag;
     maps->ok = true;
     return 0;
+}
+
+int k_vel_full(const GridDev &g, const WaveDev &w, float dt, const FullMaps &maps, void *stream) {
+    if (!maps.ok) return (int)cudaErrorInvalidValue;
+    FvMaps fm;
+    static_assert(sizeof(FvMaps) == sizeof(maps.vhalo) + sizeof(maps.vband) + sizeof(maps.vcore) +
+                                        sizeof(maps.vfeed) + sizeof(maps.vpsi),
+                  "descriptor layout");
+    std::memcpy(fm.halo, maps.vhalo, sizeof(maps.vhalo));
+    std::memcpy(fm.band, maps.vband, sizeof(maps.vband));
+    std::memcpy(fm.core, maps.vcore, sizeof(maps.vcore));
+    std::memcpy(fm.feed, maps.vfeed, sizeof(maps.vfeed));
+    std::memcpy(fm.psi, maps.vpsi, sizeof(maps.vpsi));
+    vel_fz<<<maps.grid, maps.threads, maps.vsmem, (cudaStream_t)stream>>>(g, fm, w, dt, maps.vgeo, maps.err);
+    return cerr();
+}
+
+int k_velp(const GridDev &g, const WaveDev &w, const float *rho, float dt, void *stream) {
+    const int ngx = (g.px + 3) / 4;
+    const int nb = (ngx + 63) / 64, gx = (ngx + nb - 1) / nb, gy = std::max(1, 256 / gx);
+    const dim3 b(gx, gy), gr((ngx + gx - 1) / gx, (g.py + gy - 1) / gy, g.pz);
+    velp_v4<<<gr, b, 0, (cudaStream_t)stream>>>(g, w, rho, dt);
+    return cerr();
 }
 
 int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const float *wavelet, const StepState *st,

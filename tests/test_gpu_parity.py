@@ -199,7 +199,7 @@ def test_launch_options_do_not_change_results(synth, kw):
         assert rel_l2(i0[k], i1[k]) <= 2e-5, k
 
 
-# grids on which variant 4's full-gridext stress kernel runs (even pml_num and
+# grids on which variant 4's full-gridext stress and velocity kernels run (even pml_num and
 # nx): region boundaries at every tile-row offset, the smallest pml, sources
 # and receivers next to the absorbing layers
 FULL = [
@@ -223,7 +223,7 @@ def test_full_stress_kernel_forward_vs_oracle(oracle, synth, kw):
         ctx.set_profiling(True)
         ctx.forward(0)
         names = _kernels(ctx)
-    assert "stress_fz_fwd" in names and "stress_pml" not in names, names
+    assert {"stress_fz_fwd", "vel_fz_fwd"} <= names and not {"stress_pml", "vel_pml"} & names, names
     for a, b in zip(tr, ref):
         assert np.all(np.isfinite(a))
         assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
@@ -242,7 +242,8 @@ def test_full_stress_kernel_rtm_vs_oracle(oracle, synth, kw, w):
         ctx.rtm_shot(0, obs32)
         names = _kernels(ctx)
         raw = ctx.images()
-    assert {"stress_fz_rtmfwd", "stress_fz_rev"} <= names and "stress_pml_sau" not in names, names
+    assert {"stress_fz_rtmfwd", "stress_fz_rev", "vel_fz_rtmfwd", "vel_fz_rev", "velp_rev"} <= names, names
+    assert not {"stress_pml_sau", "vel_pml"} & names, names
     for k in ("ip", "pp", "ps", "sp", "ss"):
         assert np.all(np.isfinite(raw[k]))
         assert rel_l2(raw[k], ref[k]) <= 5e-5, (w, k, rel_l2(raw[k], ref[k]))
