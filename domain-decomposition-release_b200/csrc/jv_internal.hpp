@@ -132,7 +132,8 @@ struct WaveMaps {
 // Geometry of the full-gridext stress kernel (variant 4).
 //  - XH, XC, corew: TMA x of the halo and core boxes, core box width;
 //    hxi, hxe: x pairs of a tile row in the physical range and in the two
-//    absorbing ranges; ytiles, nzi: 4-row tiles over y in [2, ny-2), planes
+//    absorbing ranges; tpad: 4 hxi rounded up to whole warps, the first
+//    thread of the absorbing pairs; ytiles, nzi: 4-row tiles over y in [2, ny-2), planes
 //    z in [2, nz-2).
 //  - The stress memory variables of this kernel are axis-major: per axis
 //    three arrays over the cells that absorb on that axis, rows packed
@@ -146,7 +147,7 @@ struct WaveMaps {
 //    tiles through the same planes together, so halo rows are shared in L2.
 struct FzGeo {
     int XH, XC, corew;
-    int hxi, hxe;
+    int hxi, hxe, tpad;
     int ytiles, nzi;
     int PX, PY, W;
     int Q, L, R;

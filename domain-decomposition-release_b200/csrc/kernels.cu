@@ -1500,14 +1500,17 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     };
     const int tid = threadIdx.x;
     const int m = g.m;
+    // threads [0, 4 hxi): physical x pairs; up to tpad (a warp multiple):
+    // idle; from tpad: absorbing x pairs -- no warp mixes the two updates
     const int ti = kZmRows * geo.hxi;
-    const bool xabs = tid >= ti;  // this thread's pair lies in an absorbing x range
+    const bool xabs = tid >= geo.tpad;  // this thread's pair lies in an absorbing x range
+    const bool idle = tid >= ti && !xabs;
     int r, x;
     if (!xabs) {
-        r = tid / geo.hxi;
-        x = m + 2 * (tid - r * geo.hxi);
+        r = idle ? 0 : tid / geo.hxi;
+        x = m + 2 * (idle ? 0 : tid - r * geo.hxi);
     } else {
-        const int e = tid - ti, half = geo.hxe / 2;
+        const int e = tid - geo.tpad, half = geo.hxe / 2;
         r = e / geo.hxe;
         const int q = e - r * geo.hxe;
         x = q < half ? 2 + 2 * q : m + g.px + 2 * (q - half);
@@ -1566,7 +1569,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
         int yt, z;
         item_at(k, yt, z);
         const int y = 2 + yt * kZmRows + r;
-        const bool live = y < g.ny - 2 && z < g.nz - 2;
+        const bool live = !idle && y < g.ny - 2 && z < g.nz - 2;
         const int i0 = (int)g.xoff + x + sy * y + sz * z;  // even: float2-aligned
         const int b = (k - w0) & 1;
         const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
@@ -1913,14 +1916,17 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     };
     const int tid = threadIdx.x;
     const int m = g.m;
+    // threads [0, 4 hxi): physical x pairs; up to tpad (a warp multiple):
+    // idle; from tpad: absorbing x pairs -- no warp mixes the two updates
     const int ti = kZmRows * geo.hxi;
-    const bool xabs = tid >= ti;
+    const bool xabs = tid >= geo.tpad;  // this thread's pair lies in an absorbing x range
+    const bool idle = tid >= ti && !xabs;
     int r, x;
     if (!xabs) {
-        r = tid / geo.hxi;
-        x = m + 2 * (tid - r * geo.hxi);
+        r = idle ? 0 : tid / geo.hxi;
+        x = m + 2 * (idle ? 0 : tid - r * geo.hxi);
     } else {
-        const int e = tid - ti, half = geo.hxe / 2;
+        const int e = tid - geo.tpad, half = geo.hxe / 2;
         r = e / geo.hxe;
         const int q = e - r * geo.hxe;
         x = q < half ? 2 + 2 * q : m + g.px + 2 * (q - half);
@@ -1981,7 +1987,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
         int yt, z;
         item_at(k, yt, z);
         const int y = 2 + yt * kZmRows + r;
-        const bool live = y < g.ny - 2 && z < g.nz - 2;
+        const bool live = !idle && y < g.ny - 2 && z < g.nz - 2;
         const int i0 = (int)g.xoff + x + sy * y + sz * z;
         const int b = (k - w0) & 1;
         const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
@@ -2606,7 +2612,8 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     FzGeo geo{};
     geo.hxi = g.px / 2;
     geo.hxe = m - 2;
-    const int threads = kZmRows * (geo.hxi + geo.hxe);
+    geo.tpad = (kZmRows * geo.hxi + 31) / 32 * 32;
+    const int threads = geo.tpad + kZmRows * geo.hxe;
     geo.XC = (xoff + 2) / 4 * 4;
     geo.XH = geo.XC - kZmHalo;
     geo.corew = (xoff + g.nx - 2 - geo.XC + 3) / 4 * 4;
