@@ -308,6 +308,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--ref-sample-steps", type=int, default=40)
     ap.add_argument("--variant", type=int, default=None, help="interior kernel variant (default: library default)")
+    ap.add_argument("--store", default="fp32", choices=["fp32", "bf16", "fp16"],
+                    help="boundary-store precision (wavefields are FP32 in every case)")
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
@@ -329,6 +331,8 @@ def main():
     jv = importlib.import_module("domain-decomposition-release_b200")
     s = survey(args, jv.synth)
     kopts = {} if args.variant is None else {"kernel_variant": args.variant}
+    if args.store != "fp32":
+        kopts["precision"] = {"bf16": jv.JV_BF16, "fp16": jv.JV_FP16}[args.store]
     ctx = jv.Context.from_survey(s, device=local, **kopts)
     info = ctx.info()
     nrec, nt = info.n_recv, info.nt
@@ -493,6 +497,7 @@ def main():
         "config": {"workload": s.name, "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt,
                    "rec_width": s.rec_width, "n_recv": nrec, "mode": "plain one-shot-per-call, graph time loop",
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
+                   "boundary_store": args.store,
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "serving": serving, "clocks": clk,
         "gpu_launches": launches * args.steps if launches else None,

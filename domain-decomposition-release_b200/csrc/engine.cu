@@ -308,7 +308,8 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (!vp || !vs || !rho) return bad(JV_EINVAL, "model arrays must not be NULL");
     int rw = opt.rec_width == 0 ? 1 : opt.rec_width;
     if (rw < 1 || rw > kPhyHalf || rw > grid.pml) return bad(JV_EINVAL, "rec_width must be in 1..4 and <= pml_num");
-    if (opt.precision != JV_FP32) return bad(JV_ENOTSUP, "only FP32 wavefield storage is built");
+    if (opt.precision != JV_FP32 && opt.precision != JV_BF16 && opt.precision != JV_FP16)
+        return bad(JV_EINVAL, "precision must be JV_FP32, JV_BF16 or JV_FP16");
     if ((opt.min_blocks != 0 && opt.min_blocks != 3 && opt.min_blocks != 4) ||
         (opt.pml_min_blocks != 0 && opt.pml_min_blocks != 3 && opt.pml_min_blocks != 4))
         return bad(JV_EINVAL, "min_blocks and pml_min_blocks must be 0, 3 or 4");
@@ -437,6 +438,8 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         vowr_ = VowrDev{};
         vowr_.per_step = per_step_;
         vowr_.nslot = nslot_;
+        vowr_.prec = opt_.precision;
+        vowr_.nseg = (int)segs_h_.size();
         vowr_.all_blocks = (int)blk;
         std::vector<int> blk_seg((size_t)blk);
         for (size_t q = 0; q < segs_h_.size(); q++) {
@@ -830,8 +833,10 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         shot_img_.ss = b + 4 * pitch;
         shot_img_pitch_ = pitch;
     }
-    if (!store_ && per_step_ > 0 && nslot_ > 0) {
-        size_t bytes = (size_t)per_step_ * nslot_ * sizeof(float);
+    if (!store_ && !vowr_.store16 && per_step_ > 0 && nslot_ > 0) {
+        const bool s16 = vowr_.prec != JV_FP32;
+        size_t bytes = (size_t)per_step_ * nslot_ * (s16 ? sizeof(uint16_t) : sizeof(float));
+        if (s16) bytes += (size_t)vowr_.nseg * (nslot_ + 2) * sizeof(float);
         size_t freeb = 0, totalb = 0;
         JV_CU(cudaMemGetInfo(&freeb, &totalb));
         size_t budget = opt_.store_budget ? opt_.store_budget : (freeb > (2ULL << 30) ? freeb - (2ULL << 30) : 0);
@@ -839,9 +844,21 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
             return bad(JV_ENOTSUP, "boundary store of " + std::to_string(bytes) +
                                        " bytes does not fit the device budget; host streaming is not built");
         void *p;
-        JV_TRY(alloc(&p, bytes));
-        store_ = (float *)p;
-        vowr_.store = store_;
+        if (s16) {
+            // 16-bit records, then one FP32 scale per box and step, then the
+            // two rows of largest magnitudes
+            const size_t nrec = (size_t)per_step_ * nslot_;
+            JV_TRY(alloc(&p, round_up((long long)(nrec * sizeof(uint16_t)), 256) +
+                                 (size_t)vowr_.nseg * (nslot_ + 2) * sizeof(float)));
+            vowr_.store16 = (uint16_t *)p;
+            vowr_.scales = (float *)((char *)p + round_up((long long)(nrec * sizeof(uint16_t)), 256));
+            vowr_.amax = (unsigned *)(vowr_.scales + (size_t)vowr_.nseg * nslot_);
+            JV_CU(cudaMemsetAsync(vowr_.amax, 0, 2 * (size_t)vowr_.nseg * sizeof(unsigned), stream_));
+        } else {
+            JV_TRY(alloc(&p, bytes));
+            store_ = (float *)p;
+            vowr_.store = store_;
+        }
     }
     const float *obs[3] = {d_ox, d_oy, d_oz};
     JV_CU(cudaEventRecord(ev0_, stream_));
@@ -954,7 +971,7 @@ void Engine::info(jv_info *i) const {
     i->precision = opt_.precision;
     i->n_ext = (long long)g_.nx * g_.ny * g_.nz;
     i->n_phy = (long long)g_.px * g_.py * g_.pz;
-    i->store_bytes_per_step = (size_t)per_step_ * sizeof(float);
+    i->store_bytes_per_step = (size_t)per_step_ * (opt_.precision == JV_FP32 ? sizeof(float) : sizeof(uint16_t));
     i->device_bytes = dev_bytes_;
     i->store_on_device = 1;
 }

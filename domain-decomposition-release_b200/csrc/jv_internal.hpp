@@ -88,13 +88,24 @@ struct SegDev {          // one VOWR face box
 // The VOWR boundary store and its face boxes.  Boxes of the velocity
 // fields come first; each box is cut into blocks of 256 cells and
 // blk_seg maps a block to its box.
+// boundary-store precision (the values of jv_precision)
+constexpr int kStoreF32 = 0, kStoreBF16 = 1, kStoreFP16 = 2;
+
 struct VowrDev {
     const SegDev *segs;
     const int *blk_seg;
     int vel_blocks, all_blocks;
-    long long per_step;  // floats of one step's record
+    long long per_step;  // values of one step's record
     int nslot;           // records in the store
-    float *store;
+    float *store;        // FP32 records (prec == JV_FP32)
+    // 16-bit records (prec == JV_BF16 / JV_FP16): value / scale, one FP32
+    // scale per face box and step (scales[slot * nseg + box]) = the box's
+    // largest magnitude; amax[2][nseg] collects it, by step parity
+    int prec;
+    int nseg;
+    uint16_t *store16;
+    float *scales;
+    unsigned *amax;
 };
 
 // Per-step state in device memory, read by the kernels of a captured
@@ -229,6 +240,10 @@ int k_inject_rec(const WaveDev &w, const long long *rec, int nrec, int nt, const
                  void *stream);
 // pack (1) or unpack (0) record st->it + slot_shift; which: 0 all fields,
 // 1 the velocity fields, 2 the stress fields
+// Packs (pack = 1) or unpacks the face boxes of step st->it + slot_shift;
+// which = 0 all boxes, 1 velocity boxes, 2 stress boxes.  With a 16-bit
+// store, packing is two launches: the boxes' largest magnitudes, then the
+// scaled values.
 int k_vowr(const GridDev &g, const WaveDev &w, const VowrDev &v, const StepState *st, int slot_shift, int pack,
            int which, void *stream);
 int k_step_advance(StepState *st, int delta, void *stream);

@@ -14,6 +14,8 @@
 //   imaging             RTM/rtm3d_0_image_module/rtm3d_iamge_kernel.hpp:6-51,118-135,184-200
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -2335,6 +2337,65 @@ __global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, VowrDev v, con
     else w.f[S.fld][i] = *rec;
 }
 
+// 16-bit boundary store.  Pass 1: each box's largest magnitude in this
+// step (amax[parity][box], atomic max of the float bits, non-negative);
+// the other parity's row, last read by the previous step's pass 2, is
+// cleared for the next step.
+__global__ void __launch_bounds__(256) vowr_amax(GridDev g, WaveDev w, VowrDev v, const StepState *__restrict__ st,
+                                                 int slot_shift) {
+    const int slot = st->it + slot_shift;
+    if (slot < 0 || slot >= v.nslot) return;
+    unsigned *cur = v.amax + (slot & 1) * v.nseg, *nxt = v.amax + ((slot + 1) & 1) * v.nseg;
+    if (blockIdx.x == 0)
+        for (int q = threadIdx.x; q < v.nseg; q += blockDim.x) nxt[q] = 0u;
+    const int b = (int)blockIdx.x;
+    const int sg = v.blk_seg[b];
+    const SegDev &S = v.segs[sg];
+    const int e = (b - (int)S.nblk_first) * 256 + (int)threadIdx.x;
+    float a = 0.f;
+    if (e < S.nxb * S.nyb * S.nzb) {
+        const int t = e / S.nxb;
+        const int x = S.x0 + (e - t * S.nxb);
+        const int z = t / S.nyb;
+        const int y = S.y0 + (t - z * S.nyb);
+        a = fabsf(w.f[S.fld][(int)g.xoff + x + (int)g.sy * y + (int)g.sz * (S.z0 + z)]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+    if ((threadIdx.x & 31) == 0 && a > 0.f) atomicMax(cur + sg, __float_as_uint(a));
+}
+
+// Pass 2 (pack) and the unpack of a 16-bit store: value = q * scale.
+template <int PREC>
+__global__ void __launch_bounds__(256) vowr16(GridDev g, WaveDev w, VowrDev v, const StepState *__restrict__ st,
+                                              int slot_shift, int pack, int b0) {
+    const int slot = st->it + slot_shift;
+    if (slot < 0 || slot >= v.nslot) return;
+    const int b = b0 + (int)blockIdx.x;
+    const int sg = v.blk_seg[b];
+    const SegDev &S = v.segs[sg];
+    const int e = (b - (int)S.nblk_first) * 256 + (int)threadIdx.x;
+    if (e >= S.nxb * S.nyb * S.nzb) return;
+    const int t = e / S.nxb;
+    const int x = S.x0 + (e - t * S.nxb);
+    const int z = t / S.nyb;
+    const int y = S.y0 + (t - z * S.nyb);
+    const int i = (int)g.xoff + x + (int)g.sy * y + (int)g.sz * (S.z0 + z);
+    uint16_t *rec = v.store16 + (long long)slot * v.per_step + S.off + e;
+    float *scale = v.scales + (long long)slot * v.nseg + sg;
+    if (pack) {
+        const float s = __uint_as_float(v.amax[(slot & 1) * v.nseg + sg]);
+        if (e == 0) *scale = s;
+        const float q = s > 0.f ? w.f[S.fld][i] / s : 0.f;
+        if (PREC == kStoreBF16) *rec = __bfloat16_as_ushort(__float2bfloat16_rn(q));
+        else *rec = __half_as_ushort(__float2half_rn(q));
+    } else {
+        const float q = PREC == kStoreBF16 ? __bfloat162float(__ushort_as_bfloat16(*rec))
+                                        : __half2float(__ushort_as_half(*rec));
+        w.f[S.fld][i] = q * *scale;
+    }
+}
+
 __global__ void step_advance(StepState *st, int delta) { st->it += delta; }
 
 __global__ void count_nonfinite_f(const float *p, size_t n, unsigned long long *out) {
@@ -2907,7 +2968,17 @@ int k_vowr(const GridDev &g, const WaveDev &w, const VowrDev &v, const StepState
     const int b0 = which == 2 ? v.vel_blocks : 0;
     const int b1 = which == 1 ? v.vel_blocks : v.all_blocks;
     if (b1 <= b0) return 0;
-    vowr<<<(unsigned)(b1 - b0), 256, 0, (cudaStream_t)stream>>>(g, w, v, st, slot_shift, pack, b0);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (v.prec == kStoreF32) {
+        vowr<<<(unsigned)(b1 - b0), 256, 0, s>>>(g, w, v, st, slot_shift, pack, b0);
+        return cerr();
+    }
+    if (pack) {
+        if (b0 != 0 || b1 != v.all_blocks) return (int)cudaErrorInvalidValue;  // a step's boxes pack together
+        vowr_amax<<<(unsigned)v.all_blocks, 256, 0, s>>>(g, w, v, st, slot_shift);
+    }
+    if (v.prec == kStoreBF16) vowr16<kStoreBF16><<<(unsigned)(b1 - b0), 256, 0, s>>>(g, w, v, st, slot_shift, pack, b0);
+    else vowr16<kStoreFP16><<<(unsigned)(b1 - b0), 256, 0, s>>>(g, w, v, st, slot_shift, pack, b0);
     return cerr();
 }
 

@@ -61,7 +61,10 @@ typedef struct jv_grid {
     float dx, dy, dz;
 } jv_grid;
 
-/* Wavefield storage precision (all arithmetic is FP32). */
+/* Storage precision of the VOWR boundary store: JV_BF16 / JV_FP16 keep each
+ * stored value as value/scale in 16 bits, with one FP32 scale per face box
+ * and time step (the box's largest magnitude). Wavefields stay FP32, and all
+ * arithmetic is FP32. */
 typedef enum jv_precision { JV_FP32 = 0, JV_BF16 = 1, JV_FP16 = 2 } jv_precision;
 
 /* Boundary-store placement for VOWR. */

@@ -269,3 +269,30 @@ def test_full_stress_kernel_vs_oracle_at_size(oracle, synth):
         assert e <= 2e-5, err
     for k, e in err[4][1].items():
         assert e <= max(5e-5, 1.5 * err[3][1][k]), (k, err)
+
+
+@pytest.mark.parametrize("prec,img_tol", [(jv.JV_FP16, 5e-5), (jv.JV_BF16, 1e-4)])
+@pytest.mark.parametrize("w", [1, 4])
+def test_16bit_boundary_store_vs_oracle(oracle, synth, prec, img_tol, w):
+    """The VOWR boundary store in 16 bits with one FP32 scale per face box and
+    step: the images against the FP64 oracle, next to the FP32 store's.
+    Tolerances, relative L2: FP16 5e-5 and BF16 1e-4.  Measured on this case:
+    0.9-1.2e-5 (FP16) and 1.4-1.9e-5 (BF16), against 0.7-1.0e-5 with the FP32
+    store.  The replayed values only seed the rim of the reconstruction, so
+    their 11 and 8 mantissa bits cost little."""
+    s = synth.small_case(n=(22, 18, 21), pml=6, nt=140, seed=21, rec_width=w, anomaly=(0.1, 3.0),
+                         shot_idx=[(11, 9, 3)])
+    p = _problem(oracle, s, w)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    obs32 = [o.astype(np.float32) for o in obs]
+    err = {}
+    for pr in (jv.JV_FP32, prec):
+        with jv.Context.from_survey(s, precision=pr) as ctx:
+            assert ctx.info().precision == pr
+            ctx.rtm_shot(0, obs32)
+            raw = ctx.images()
+        err[pr] = {k: rel_l2(raw[k], ref[k]) for k in raw}
+    print("image rel-L2 vs FP64 oracle, FP32 store:", err[jv.JV_FP32], "16-bit store:", err[prec])
+    for k, e in err[prec].items():
+        assert np.isfinite(e) and e <= img_tol, (k, err)
