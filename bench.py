@@ -243,15 +243,42 @@ def serve_leg(jv, synth, n_req):
     t4, st4 = run(4)
     cells = sum((sv.nx + 2 * sv.pml) * (sv.ny + 2 * sv.pml) * (sv.nz + 2 * sv.pml) * sv.nt * (3 if k else 1)
                 for sv, k in plan)
+
+    # a Poisson stream: requests arrive (seeded exponential gaps) while
+    # others run, at half and at 0.9 of the 4-slot capacity just measured
+    def poisson(rate, seed):
+        rng = np.random.default_rng(seed)
+        with jv.Server(slots=4) as srv:
+            t0 = time.perf_counter()
+            due = 0.0
+            subs = []
+            for sv, k in plan:
+                due += rng.exponential(1.0 / rate)
+                pause = t0 + due - time.perf_counter()
+                if pause > 0:
+                    time.sleep(pause)
+                subs.append(srv.submit_survey(k, sv))
+            for rid, _ in subs:
+                if srv.wait(rid, timeout=600.0) != 0:
+                    raise RuntimeError("served request failed")
+            dt = time.perf_counter() - t0
+            st = srv.stats()
+        return {"offered_per_s": round(rate, 2), "achieved_per_s": round(n_req / dt, 2),
+                "p50_ms": round(st["p50_ms"], 1), "p99_ms": round(st["p99_ms"], 1)}
+
+    cap = n_req / t4
+    stream = [poisson(f * cap, 40 + i) for i, f in enumerate((0.5, 0.9))]
     return {"requests": n_req, "unit": "requests/h",
+            "poisson_4slots": stream,
             "mix": f"grids {sizes}^3 +10 CPML, nt 400, 2/3 RTM (own modelling first), 1/3 forward",
             "slots4": round(n_req / t4 * 3600.0, 1), "slots1": round(n_req / t1 * 3600.0, 1),
             "speedup": round(t1 / t4, 3),
             "p50_ms": {"slots4": round(st4["p50_ms"], 1), "slots1": round(st1["p50_ms"], 1)},
             "p99_ms": {"slots4": round(st4["p99_ms"], 1), "slots1": round(st1["p99_ms"], 1)},
             "gcell_updates_per_s": {"slots4": round(cells / t4 / 1e9, 2), "slots1": round(cells / t1 / 1e9, 2)},
-            "note": "latency counts from submission, all requests submitted at once; two warm-up requests "
-                    "on a server of their own are not counted"}
+            "note": "latency counts from submission; slots4/slots1: all requests submitted at once; "
+                    "poisson_4slots: seeded exponential arrival gaps at 0.5 and 0.9 of the slots4 rate; two "
+                    "warm-up requests on a server of their own are not counted"}
 
 
 def run_reference(args):

@@ -141,26 +141,31 @@ struct WaveMaps {
 };
 
 // Geometry of the full-gridext stress kernel (variant 4).
-//  - XH, XC, corew: TMA x of the halo and core boxes, core box width;
-//    hxi, hxe: x pairs of a tile row in the physical range and in the two
-//    absorbing ranges; tpad: 4 hxi rounded up to whole warps, the first
-//    thread of the absorbing pairs; ytiles, nzi: 4-row tiles over y in [2, ny-2), planes
-//    z in [2, nz-2).
+//  - x tiles: tile xt holds the physical x pairs [xt TPP, (xt+1) TPP) of the
+//    hxi = px/2, the first also the low absorbing strip [2, m), the last the
+//    high one [m+px, nx-2) (one tile: both); hxe: absorbing pairs a tile
+//    row carries (m-2 with one tile, else (m-2)/2); tpad: 4 TPP rounded up
+//    to whole warps, the first thread of the absorbing pairs; corew: the
+//    core box width (the widest tile's).  ytiles, nzi: 4-row tiles over y in
+//    [2, ny-2), planes z in [2, nz-2).
 //  - The stress memory variables of this kernel are axis-major: per axis
 //    three arrays over the cells that absorb on that axis, rows packed
 //    (x arrays [t][z-2][y-2][xc], pitch PX over xc = the W absorbing x
 //    columns; y arrays [t][z-2][yc][x-2] and z arrays [t][zc][y-2][x-2],
 //    pitch PY over x-2), so that a tile's memory variables arrive by TMA
-//    with its fields.  W = 2 (m - 2) absorbing indices per axis.
+//    with its fields (y and z boxes PB wide, from the tile's first cell
+//    rounded down to 16 bytes).  W = 2 (m - 2) absorbing indices per axis.
 //  - Runs: each tile's planes are cut into Q chunks of L planes (the last
-//    one padded with idle items); run r = chunk * ytiles + tile, and CTA b
-//    takes runs b, b + grid, ...  CTAs b and b+1 then march neighbouring
-//    tiles through the same planes together, so halo rows are shared in L2.
+//    one padded with idle items); run r = chunk * (NTX ytiles) + tile, tile
+//    = yt NTX + xt, and CTA b takes runs b, b + grid, ...  Neighbouring CTAs
+//    then march neighbouring tiles through the same planes together, so
+//    halo rows are shared in L2.
 struct FzGeo {
-    int XH, XC, corew;
+    int corew;
     int hxi, hxe, tpad;
+    int NTX, TPP;       // x tiles; physical x pairs per tile
     int ytiles, nzi;
-    int PX, PY, W;
+    int PX, PY, PB, W;  // PB: width of a y/z memory-variable box
     int Q, L, R;
     float *psx, *psy, *psz;
     const float4 *ax[3];

@@ -1472,10 +1472,65 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map
 // boxes (3 arrays x 4 rows each), every region 128-byte aligned
 __host__ __device__ constexpr int fz_round32(int n) { return (n + 31) / 32 * 32; }
 __host__ __device__ inline int fz_stage(const FzGeo &g) {
-    return kFzStage + fz_round32(12 * g.PX) + 2 * fz_round32(12 * g.PY);
+    return kFzStage + fz_round32(12 * g.PX) + 2 * fz_round32(12 * g.PB);
 }
 
-template <int MODE>
+// x tiles of the full-gridext kernels: the first cell of tile xt
+__host__ __device__ inline int fz_xlo(const GridDev &g, const FzGeo &q, int xt) {
+    return xt == 0 ? 2 : g.m + 2 * xt * q.TPP;
+}
+// ... and one past its last
+__host__ __device__ inline int fz_xhi(const GridDev &g, const FzGeo &q, int xt) {
+    return xt == q.NTX - 1 ? g.nx - 2 : g.m + 2 * (xt + 1) * q.TPP;
+}
+
+// The pair of a thread in an x tile.  FzLane holds the tile-invariant part
+// (computed once per thread); fz_lane gives, for tile xt, the row r, the
+// first cell x, whether it absorbs in x, and live = false when the thread
+// has no pair there.  Threads [0, 4 TPP): physical pairs; up to tpad (a
+// warp multiple): none; from tpad: absorbing pairs -- no warp mixes the
+// two updates.
+struct FzLane {
+    int r, k;   // row; pair within the tile's physical pairs, or absorbing pair index
+    bool phys;
+};
+__device__ __forceinline__ FzLane fz_lane0(const FzGeo &q, int tid) {
+    FzLane L;
+    L.phys = tid < q.tpad;
+    if (L.phys) {
+        L.r = tid / q.TPP;
+        L.k = tid - L.r * q.TPP;
+    } else {
+        const int e = tid - q.tpad;
+        L.r = e / q.hxe;
+        L.k = e - L.r * q.hxe;
+    }
+    return L;
+}
+__device__ __forceinline__ void fz_lane(const GridDev &g, const FzGeo &q, const FzLane &L, int xt, int &r, int &x,
+                                        bool &xabs, bool &live) {
+    const int m = g.m;
+    if (L.phys) {
+        xabs = false;
+        const int gp = xt * q.TPP + L.k;
+        live = L.r < kZmRows && gp < q.hxi;
+        r = live ? L.r : 0;
+        x = m + 2 * (live ? gp : 0);
+    } else {
+        xabs = true;
+        r = L.r;
+        if (q.NTX == 1) {
+            const int half = q.hxe / 2;
+            x = L.k < half ? 2 + 2 * L.k : m + g.px + 2 * (L.k - half);
+            live = true;
+        } else {
+            live = xt == 0 || xt == q.NTX - 1;
+            x = xt == 0 ? 2 + 2 * L.k : m + g.px + 2 * L.k;
+        }
+    }
+}
+
+template <int MODE, bool XT>
 __global__ void __launch_bounds__(kZmMaxThreads, 1)
     stress_fz(GridDev g, const __grid_constant__ FzMaps maps, WaveDev w, float dt, const float *__restrict__ wavelet,
               const StepState *__restrict__ st, int it_off, const __grid_constant__ FzGeo geo, int *err) {
@@ -1485,45 +1540,38 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     extern __shared__ __align__(128) float sm[];
     constexpr int hb = kZmHB, cb = kZmCB, boxw = kZmPitch;
     const int stage = fz_stage(geo);
-    const int pxr = fz_round32(12 * geo.PX), pyr = fz_round32(12 * geo.PY);
+    const int pxr = fz_round32(12 * geo.PX), pyr = fz_round32(12 * geo.PB);
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_abort;
     // this CTA's runs: blockIdx.x, blockIdx.x + gridDim.x, ...; L items each
     const int nrun = (geo.R - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     const int w0 = 0, w1 = nrun * geo.L;
     if (nrun <= 0) return;
-    // item -> (tile, plane); planes past the last one are idle items
-    auto item_at = [&](int item, int &yt, int &z) {
+    // item -> (x tile, y tile, plane); planes past the last one are idle items
+    const int ntile = geo.NTX * geo.ytiles;
+    auto item_at = [&](int item, int &xt, int &yt, int &z) {
         const int j = item / geo.L, off = item - j * geo.L;
         const int rr = (int)blockIdx.x + j * (int)gridDim.x;
-        const int q = rr / geo.ytiles;
-        yt = rr - q * geo.ytiles;
+        const int q = rr / ntile, t = rr - q * ntile;
+        if (!XT) {  // one x tile: every tile quantity is loop-invariant
+            yt = t;
+            xt = 0;
+        } else {
+            yt = t / geo.NTX;
+            xt = t - yt * geo.NTX;
+        }
         z = 2 + q * geo.L + off;
     };
     const int tid = threadIdx.x;
     const int m = g.m;
-    // threads [0, 4 hxi): physical x pairs; up to tpad (a warp multiple):
-    // idle; from tpad: absorbing x pairs -- no warp mixes the two updates
-    const int ti = kZmRows * geo.hxi;
-    const bool xabs = tid >= geo.tpad;  // this thread's pair lies in an absorbing x range
-    const bool idle = tid >= ti && !xabs;
-    int r, x;
-    if (!xabs) {
-        r = idle ? 0 : tid / geo.hxi;
-        x = m + 2 * (idle ? 0 : tid - r * geo.hxi);
-    } else {
-        const int e = tid - geo.tpad, half = geo.hxe / 2;
-        r = e / geo.hxe;
-        const int q = e - r * geo.hxe;
-        x = q < half ? 2 + 2 * q : m + g.px + 2 * (q - half);
-    }
+    const FzLane ln = fz_lane0(geo, tid);
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     const uint32_t bytes_all = (uint32_t)(3 * hb + NCT * geo.corew * kZmRows) * 4u;
     const uint32_t bytes_feed = (uint32_t)(3 * geo.corew * kZmRows) * 4u;
-    const uint32_t bytes_psx = (uint32_t)(12 * geo.PX) * 4u, bytes_psy = (uint32_t)(12 * geo.PY) * 4u;
+    const uint32_t bytes_psx = (uint32_t)(12 * geo.PX) * 4u, bytes_psy = (uint32_t)(12 * geo.PB) * 4u;
     auto issue = [&](int item, int b) {
-        int yt, z;
-        item_at(item, yt, z);
+        int xt, yt, z;
+        item_at(item, xt, yt, z);
         const uint32_t bar = b ? bar1 : bar0;
         if (z >= g.nz - 2) {
             mbar_expect(bar, 0);  // idle item: the phase completes with this arrival
@@ -1534,19 +1582,22 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
         const bool feed = z + 5 < g.nz;  // the window's next plane; none past gridext
         const bool zab = z < m || z >= m + g.pz;
         const bool ylo = Y < m, yhi = Y + kZmRows - 1 >= m + g.py;  // the tile holds absorbing rows
-        mbar_expect(bar, (feed ? bytes_all : bytes_all - bytes_feed) + bytes_psx + (ylo || yhi ? bytes_psy : 0u) +
-                             (zab ? bytes_psy : 0u));
-        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], geo.XH, Y - kZmHalo, z, bar);
+        const bool xab = !XT || xt == 0 || xt == geo.NTX - 1;      // ... or absorbing columns
+        const int xlo = fz_xlo(g, geo, xt);
+        const int XC = ((int)g.xoff + xlo) & ~3, XH = XC - kZmHalo, xb0 = (xlo - 2) & ~3;
+        mbar_expect(bar, (feed ? bytes_all : bytes_all - bytes_feed) + (xab ? bytes_psx : 0u) +
+                             (ylo || yhi ? bytes_psy : 0u) + (zab ? bytes_psy : 0u));
+        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], XH, Y - kZmHalo, z, bar);
         if (feed)
             for (int f = 0; f < 3; f++)
-                tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], geo.XC, Y, z + 5, bar);
-        for (int f = 3; f < NCT; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], geo.XC, Y, z, bar);
+                tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], XC, Y, z + 5, bar);
+        for (int f = 3; f < NCT; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.core[f], XC, Y, z, bar);
         float *ps = base + kFzStage;
-        tma_load_4d(smem_u32(ps), &maps.psi[0], 0, Y - 2, z - 2, 0, bar);
+        if (xab) tma_load_4d(smem_u32(ps), &maps.psi[0], 0, Y - 2, z - 2, 0, bar);
         if (ylo || yhi)
-            tma_load_4d(smem_u32(ps + pxr), &maps.psi[1], 0, ylo ? Y - 2 : m - 2 + Y - (m + g.py), z - 2, 0, bar);
+            tma_load_4d(smem_u32(ps + pxr), &maps.psi[1], xb0, ylo ? Y - 2 : m - 2 + Y - (m + g.py), z - 2, 0, bar);
         if (zab)
-            tma_load_4d(smem_u32(ps + pxr + pyr), &maps.psi[2], 0, Y - 2, z < m ? z - 2 : m - 2 + z - (m + g.pz), 0,
+            tma_load_4d(smem_u32(ps + pxr + pyr), &maps.psi[2], xb0, Y - 2, z < m ? z - 2 : m - 2 + z - (m + g.pz), 0,
                         bar);
     };
     if (tid == 0) {
@@ -1562,22 +1613,37 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     }
     const int sy = (int)g.sy, sz = (int)g.sz;
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    const int hcol = (int)g.xoff + x - geo.XH;  // the pair's first cell in a halo row (even)
-    const int ccol = (int)g.xoff + x - geo.XC;  // ... in a core row (even)
     float2 rv[3][9];                           // z windows: planes z-4 .. z+4 of vx, vy, vz
     const float *fv[3] = {w.f[VX], w.f[VY], w.f[VZ]};
-    int cur_yt = -1, cur_z = -2;
+    // with one x tile the pair and the boxes are the same for every item
+    int r1, x1, XC1, xb1;
+    bool xabs1, lane1;
+    fz_lane(g, geo, ln, 0, r1, x1, xabs1, lane1);
+    XC1 = ((int)g.xoff + 2) & ~3;
+    xb1 = 0;
+    int cur_t = -1, cur_z = -2;
     for (int k = w0; k < w1; k++) {
-        int yt, z;
-        item_at(k, yt, z);
+        int xt, yt, z;
+        item_at(k, xt, yt, z);
+        int r = r1, x = x1, XC = XC1, xb0 = xb1;
+        bool xabs = xabs1, lane = lane1;
+        if (XT) {
+            fz_lane(g, geo, ln, xt, r, x, xabs, lane);
+            const int xlo = fz_xlo(g, geo, xt);
+            XC = ((int)g.xoff + xlo) & ~3;
+            xb0 = (xlo - 2) & ~3;
+        }
+        const int hcol = (int)g.xoff + x - (XC - kZmHalo);  // the pair's first cell in a halo row (even)
+        const int ccol = (int)g.xoff + x - XC;              // ... in a core row (even)
         const int y = 2 + yt * kZmRows + r;
-        const bool live = !idle && y < g.ny - 2 && z < g.nz - 2;
+        const bool live = lane && y < g.ny - 2 && z < g.nz - 2;
         const int i0 = (int)g.xoff + x + sy * y + sz * z;  // even: float2-aligned
         const int b = (k - w0) & 1;
         const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
         const float *base = sm + b * stage;
         const int cc = r * geo.corew + ccol;
-        if (yt != cur_yt || z != cur_z + 1) {
+        const int t = yt * geo.NTX + xt;
+        if (t != cur_t || z != cur_z + 1) {
             // a new run of planes: fill the z windows from global memory
 #pragma unroll
             for (int f = 0; f < 3; f++) {
@@ -1590,7 +1656,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                 }
             }
         }
-        cur_yt = yt;
+        cur_t = t;
         cur_z = z;
         if (!mbar_wait_bounded(b ? bar1 : bar0, parity)) {
             s_abort = 1;
@@ -1770,7 +1836,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                     const int yc = y < m ? y - 2 : m - 2 + y - (m + g.py);
                     const long long a0 = ((long long)zi * geo.W + yc) * geo.PY + xi;
                     const long long as = (long long)(g.nz - 4) * geo.W * geo.PY;
-                    const int s0 = fz_round32(12 * geo.PX) + r * geo.PY + xi, ss = 4 * geo.PY;
+                    const int s0 = pxr + r * geo.PB + (xi - xb0), ss = 4 * geo.PB;
                     const float4 ty = __ldg(&geo.ax[1][y]);
 #pragma unroll
                     for (int c = 0; c < 2; c++) cpml_coef(vpc[c], ty, dt, A[c], B[c], Ah[c], Bh[c]);
@@ -1782,8 +1848,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                     const int zc = z < m ? z - 2 : m - 2 + z - (m + g.pz);
                     const long long a0 = ((long long)zc * (g.ny - 4) + yi) * geo.PY + xi;
                     const long long as = (long long)geo.W * (g.ny - 4) * geo.PY;
-                    const int s0 = fz_round32(12 * geo.PX) + fz_round32(12 * geo.PY) + r * geo.PY + xi,
-                              ss = 4 * geo.PY;
+                    const int s0 = pxr + pyr + r * geo.PB + (xi - xb0), ss = 4 * geo.PB;
                     const float4 tz = __ldg(&geo.ax[2][z]);
 #pragma unroll
                     for (int c = 0; c < 2; c++) cpml_coef(vpc[c], tz, dt, A[c], B[c], Ah[c], Bh[c]);
@@ -1894,52 +1959,46 @@ struct FvMaps {
 };
 
 __host__ __device__ inline int fv_stage(const FzGeo &g) {
-    return kFvStage + fz_round32(12 * g.PX) + 2 * fz_round32(12 * g.PY);
+    return kFvStage + fz_round32(12 * g.PX) + 2 * fz_round32(12 * g.PB);
 }
 
+template <bool XT>
 __global__ void __launch_bounds__(kZmMaxThreads, 1)
     vel_fz(GridDev g, const __grid_constant__ FvMaps maps, WaveDev w, float dt, const __grid_constant__ FzGeo geo,
            int *err) {
     extern __shared__ __align__(128) float sm[];
     constexpr int hb = kZmHB, cb = kZmCB, boxw = kZmPitch;
     const int stage = fv_stage(geo);
-    const int pxr = fz_round32(12 * geo.PX), pyr = fz_round32(12 * geo.PY);
+    const int pxr = fz_round32(12 * geo.PX), pyr = fz_round32(12 * geo.PB);
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_abort;
     const int nrun = (geo.R - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     const int w0 = 0, w1 = nrun * geo.L;
     if (nrun <= 0) return;
-    auto item_at = [&](int item, int &yt, int &z) {
+    const int ntile = geo.NTX * geo.ytiles;
+    auto item_at = [&](int item, int &xt, int &yt, int &z) {
         const int j = item / geo.L, off = item - j * geo.L;
         const int rr = (int)blockIdx.x + j * (int)gridDim.x;
-        const int q = rr / geo.ytiles;
-        yt = rr - q * geo.ytiles;
+        const int q = rr / ntile, t = rr - q * ntile;
+        if (!XT) {  // one x tile: every tile quantity is loop-invariant
+            yt = t;
+            xt = 0;
+        } else {
+            yt = t / geo.NTX;
+            xt = t - yt * geo.NTX;
+        }
         z = 2 + q * geo.L + off;
     };
     const int tid = threadIdx.x;
     const int m = g.m;
-    // threads [0, 4 hxi): physical x pairs; up to tpad (a warp multiple):
-    // idle; from tpad: absorbing x pairs -- no warp mixes the two updates
-    const int ti = kZmRows * geo.hxi;
-    const bool xabs = tid >= geo.tpad;  // this thread's pair lies in an absorbing x range
-    const bool idle = tid >= ti && !xabs;
-    int r, x;
-    if (!xabs) {
-        r = idle ? 0 : tid / geo.hxi;
-        x = m + 2 * (idle ? 0 : tid - r * geo.hxi);
-    } else {
-        const int e = tid - geo.tpad, half = geo.hxe / 2;
-        r = e / geo.hxe;
-        const int q = e - r * geo.hxe;
-        x = q < half ? 2 + 2 * q : m + g.px + 2 * (q - half);
-    }
+    const FzLane ln = fz_lane0(geo, tid);
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     const uint32_t bytes_feed = (uint32_t)(3 * geo.corew * kZmRows) * 4u;
     const uint32_t bytes_all = (uint32_t)(3 * hb + 2 * cb + 5 * geo.corew * kZmRows) * 4u + bytes_feed;
-    const uint32_t bytes_psx = (uint32_t)(12 * geo.PX) * 4u, bytes_psy = (uint32_t)(12 * geo.PY) * 4u;
+    const uint32_t bytes_psx = (uint32_t)(12 * geo.PX) * 4u, bytes_psy = (uint32_t)(12 * geo.PB) * 4u;
     auto issue = [&](int item, int b) {
-        int yt, z;
-        item_at(item, yt, z);
+        int xt, yt, z;
+        item_at(item, xt, yt, z);
         const uint32_t bar = b ? bar1 : bar0;
         if (z >= g.nz - 2) {
             mbar_expect(bar, 0);
@@ -1950,21 +2009,23 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
         const bool feed = z + 5 < g.nz;
         const bool zab = z < m || z >= m + g.pz;
         const bool ylo = Y < m, yhi = Y + kZmRows - 1 >= m + g.py;
-        mbar_expect(bar, (feed ? bytes_all : bytes_all - bytes_feed) + bytes_psx + (ylo || yhi ? bytes_psy : 0u) +
-                             (zab ? bytes_psy : 0u));
-        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], geo.XH, Y - kZmHalo, z, bar);
-        for (int f = 0; f < 2; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.band[f], geo.XH, Y, z, bar);
-        for (int f = 0; f < 5; f++)
-            tma_load_3d(smem_u32(base + 3 * hb + (2 + f) * cb), &maps.core[f], geo.XC, Y, z, bar);
+        const bool xab = !XT || xt == 0 || xt == geo.NTX - 1;
+        const int xlo = fz_xlo(g, geo, xt);
+        const int XC = ((int)g.xoff + xlo) & ~3, XH = XC - kZmHalo, xb0 = (xlo - 2) & ~3;
+        mbar_expect(bar, (feed ? bytes_all : bytes_all - bytes_feed) + (xab ? bytes_psx : 0u) +
+                             (ylo || yhi ? bytes_psy : 0u) + (zab ? bytes_psy : 0u));
+        for (int f = 0; f < 3; f++) tma_load_3d(smem_u32(base + f * hb), &maps.halo[f], XH, Y - kZmHalo, z, bar);
+        for (int f = 0; f < 2; f++) tma_load_3d(smem_u32(base + 3 * hb + f * cb), &maps.band[f], XH, Y, z, bar);
+        for (int f = 0; f < 5; f++) tma_load_3d(smem_u32(base + 3 * hb + (2 + f) * cb), &maps.core[f], XC, Y, z, bar);
         if (feed)
             for (int f = 0; f < 3; f++)
-                tma_load_3d(smem_u32(base + 3 * hb + (7 + f) * cb), &maps.feed[f], geo.XC, Y, z + 5, bar);
+                tma_load_3d(smem_u32(base + 3 * hb + (7 + f) * cb), &maps.feed[f], XC, Y, z + 5, bar);
         float *ps = base + kFvStage;
-        tma_load_4d(smem_u32(ps), &maps.psi[0], 0, Y - 2, z - 2, 0, bar);
+        if (xab) tma_load_4d(smem_u32(ps), &maps.psi[0], 0, Y - 2, z - 2, 0, bar);
         if (ylo || yhi)
-            tma_load_4d(smem_u32(ps + pxr), &maps.psi[1], 0, ylo ? Y - 2 : m - 2 + Y - (m + g.py), z - 2, 0, bar);
+            tma_load_4d(smem_u32(ps + pxr), &maps.psi[1], xb0, ylo ? Y - 2 : m - 2 + Y - (m + g.py), z - 2, 0, bar);
         if (zab)
-            tma_load_4d(smem_u32(ps + pxr + pyr), &maps.psi[2], 0, Y - 2, z < m ? z - 2 : m - 2 + z - (m + g.pz), 0,
+            tma_load_4d(smem_u32(ps + pxr + pyr), &maps.psi[2], xb0, Y - 2, z < m ? z - 2 : m - 2 + z - (m + g.pz), 0,
                         bar);
     };
     if (tid == 0) {
@@ -1980,22 +2041,37 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     }
     const int sy = (int)g.sy, sz = (int)g.sz;
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    const int hcol = (int)g.xoff + x - geo.XH;
-    const int ccol = (int)g.xoff + x - geo.XC;
     float2 rv[3][9];  // z windows: planes z-4 .. z+4 of sxz, syz, szz
     const float *fv[3] = {w.f[SXZ], w.f[SYZ], w.f[SZZ]};
-    int cur_yt = -1, cur_z = -2;
+    // with one x tile the pair and the boxes are the same for every item
+    int r1, x1, XC1, xb1;
+    bool xabs1, lane1;
+    fz_lane(g, geo, ln, 0, r1, x1, xabs1, lane1);
+    XC1 = ((int)g.xoff + 2) & ~3;
+    xb1 = 0;
+    int cur_t = -1, cur_z = -2;
     for (int k = w0; k < w1; k++) {
-        int yt, z;
-        item_at(k, yt, z);
+        int xt, yt, z;
+        item_at(k, xt, yt, z);
+        int r = r1, x = x1, XC = XC1, xb0 = xb1;
+        bool xabs = xabs1, lane = lane1;
+        if (XT) {
+            fz_lane(g, geo, ln, xt, r, x, xabs, lane);
+            const int xlo = fz_xlo(g, geo, xt);
+            XC = ((int)g.xoff + xlo) & ~3;
+            xb0 = (xlo - 2) & ~3;
+        }
+        const int hcol = (int)g.xoff + x - (XC - kZmHalo);
+        const int ccol = (int)g.xoff + x - XC;
+        const int t = yt * geo.NTX + xt;
         const int y = 2 + yt * kZmRows + r;
-        const bool live = !idle && y < g.ny - 2 && z < g.nz - 2;
+        const bool live = lane && y < g.ny - 2 && z < g.nz - 2;
         const int i0 = (int)g.xoff + x + sy * y + sz * z;
         const int b = (k - w0) & 1;
         const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
         const float *base = sm + b * stage;
         const int cc = r * geo.corew + ccol;
-        if (yt != cur_yt || z != cur_z + 1) {
+        if (t != cur_t || z != cur_z + 1) {
 #pragma unroll
             for (int f = 0; f < 3; f++) {
 #pragma unroll
@@ -2007,7 +2083,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                 }
             }
         }
-        cur_yt = yt;
+        cur_t = t;
         cur_z = z;
         if (!mbar_wait_bounded(b ? bar1 : bar0, parity)) {
             s_abort = 1;
@@ -2186,7 +2262,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                     const int yc = y < m ? y - 2 : m - 2 + y - (m + g.py);
                     const long long a0 = ((long long)zi * geo.W + yc) * geo.PY + xi;
                     const long long as = (long long)(g.nz - 4) * geo.W * geo.PY;
-                    const int s0 = pxr + r * geo.PY + xi, ss = 4 * geo.PY;
+                    const int s0 = pxr + r * geo.PB + (xi - xb0), ss = 4 * geo.PB;
                     const float4 ty = __ldg(&geo.ax[1][y]);
 #pragma unroll
                     for (int c = 0; c < 2; c++) cpml_coef(vpc[c], ty, dt, A[c], B[c], Ah[c], Bh[c]);
@@ -2198,7 +2274,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                     const int zc = z < m ? z - 2 : m - 2 + z - (m + g.pz);
                     const long long a0 = ((long long)zc * (g.ny - 4) + yi) * geo.PY + xi;
                     const long long as = (long long)geo.W * (g.ny - 4) * geo.PY;
-                    const int s0 = pxr + pyr + r * geo.PY + xi, ss = 4 * geo.PY;
+                    const int s0 = pxr + pyr + r * geo.PB + (xi - xb0), ss = 4 * geo.PB;
                     const float4 tz = __ldg(&geo.ax[2][z]);
 #pragma unroll
                     for (int c = 0; c < 2; c++) cpml_coef(vpc[c], tz, dt, A[c], B[c], Ah[c], Bh[c]);
@@ -2672,22 +2748,34 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     if ((m & 1) || (g.px & 1) || !psi) return 0;
     FzGeo geo{};
     geo.hxi = g.px / 2;
-    geo.hxe = m - 2;
-    geo.tpad = (kZmRows * geo.hxi + 31) / 32 * 32;
-    const int threads = geo.tpad + kZmRows * geo.hxe;
-    geo.XC = (xoff + 2) / 4 * 4;
-    geo.XH = geo.XC - kZmHalo;
-    geo.corew = (xoff + g.nx - 2 - geo.XC + 3) / 4 * 4;
     geo.ytiles = (g.ny - 4 + kZmRows - 1) / kZmRows;
     geo.nzi = g.nz - 4;
     geo.W = 2 * (m - 2);
     geo.PX = (geo.W + 3) / 4 * 4;
     geo.PY = (g.nx - 4 + 3) / 4 * 4;
-    // one tile per CTA; a row's x window inside the 256-float halo box; the
-    // memory-variable boxes no wider than 256
-    if (threads > kZmMaxThreads || xoff + g.nx + 2 - geo.XH > kZmPitch || geo.corew > kZmPitch ||
-        geo.PY > kZmPitch)
-        return 0;
+    // x tiles: the fewest for which a tile fits one CTA, each tile row with
+    // its x halo fits the 256-float halo box, and the core and
+    // memory-variable boxes are at most 256 wide
+    int threads = 0;
+    for (geo.NTX = 1; geo.NTX <= 64; geo.NTX++) {
+        geo.TPP = (geo.hxi + geo.NTX - 1) / geo.NTX;
+        geo.hxe = geo.NTX == 1 ? m - 2 : (m - 2) / 2;
+        geo.tpad = (kZmRows * geo.TPP + 31) / 32 * 32;
+        threads = geo.tpad + kZmRows * geo.hxe;
+        bool fits = threads <= kZmMaxThreads && (geo.NTX - 1) * geo.TPP < geo.hxi;
+        geo.corew = 0;
+        geo.PB = 0;
+        for (int t = 0; t < geo.NTX && fits; t++) {
+            const int xlo = fz_xlo(g, geo, t), xhi = fz_xhi(g, geo, t);
+            const int XC = (xoff + xlo) & ~3, XH = XC - kZmHalo, xb0 = (xlo - 2) & ~3;
+            geo.corew = std::max(geo.corew, (xoff + xhi - XC + 3) / 4 * 4);
+            geo.PB = std::max(geo.PB, (xhi - 2 - xb0 + 3) / 4 * 4);
+            fits = xoff + xhi + 4 - XH <= kZmPitch;
+        }
+        if (fits && geo.corew <= kZmPitch && geo.PB <= kZmPitch) break;
+        if (geo.TPP <= 16) return 0;
+    }
+    if (geo.NTX > 64) return 0;
     int dev = 0, nsm = 0, smem_max = 0;
     cudaGetDevice(&dev);
     cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -2701,7 +2789,7 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     // plane costs about a window refill more)
     long long best = -1;
     for (int Q = 1; Q <= 64 && Q <= geo.nzi; Q++) {
-        const int L = (geo.nzi + Q - 1) / Q, R = geo.ytiles * Q;
+        const int L = (geo.nzi + Q - 1) / Q, R = geo.NTX * geo.ytiles * Q;
         const int G = std::min(nsm, R);
         const long long cost = (long long)((R + G - 1) / G) * (L + 6);
         if (best < 0 || cost < best) {
@@ -2762,7 +2850,7 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     const cuuint64_t dx4[4] = {(cuuint64_t)geo.PX, ny, nz, 3}, dy4[4] = {(cuuint64_t)geo.PY, W, nz, 3},
                      dz4[4] = {(cuuint64_t)geo.PY, ny, W, 3};
     const cuuint32_t bx4[4] = {(cuuint32_t)geo.PX, (cuuint32_t)kZmRows, 1, 3},
-                     by4[4] = {(cuuint32_t)geo.PY, (cuuint32_t)kZmRows, 1, 3};
+                     by4[4] = {(cuuint32_t)geo.PB, (cuuint32_t)kZmRows, 1, 3};
     if (!make(geo.psx, 4, dx4, bx4, &maps->psi[0]) || !make(geo.psy, 4, dy4, by4, &maps->psi[1]) ||
         !make(geo.psz, 4, dz4, by4, &maps->psi[2]))
         return 0;
@@ -2785,12 +2873,13 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     // at the same time.  Every caller sets the same value, the device's
     // limit, and each launch asks for its own size below it.
     const int smem_attr = smem_max - 1024;
-    e = cudaFuncSetAttribute(vel_fz, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stress_fz<kFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(stress_fz<kRtmFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(stress_fz<kRev>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
+    const void *fns[8] = {(const void *)vel_fz<false>,          (const void *)vel_fz<true>,
+                          (const void *)stress_fz<kFwd, false>,    (const void *)stress_fz<kFwd, true>,
+                          (const void *)stress_fz<kRtmFwd, false>, (const void *)stress_fz<kRtmFwd, true>,
+                          (const void *)stress_fz<kRev, false>,    (const void *)stress_fz<kRev, true>};
+    e = cudaSuccess;
+    for (int f = 0; f < 8 && e == cudaSuccess; f++)
+        e = cudaFuncSetAttribute(fns[f], cudaFuncAttributeMaxDynamicSharedMemorySize, smem_attr);
     if (e != cudaSuccess) return (int)e;
     maps->geo = geo;
     maps->vgeo = vgeo;
@@ -2814,7 +2903,8 @@ int k_vel_full(const GridDev &g, const WaveDev &w, float dt, const FullMaps &map
     std::memcpy(fm.core, maps.vcore, sizeof(maps.vcore));
     std::memcpy(fm.feed, maps.vfeed, sizeof(maps.vfeed));
     std::memcpy(fm.psi, maps.vpsi, sizeof(maps.vpsi));
-    vel_fz<<<maps.grid, maps.threads, maps.vsmem, (cudaStream_t)stream>>>(g, fm, w, dt, maps.vgeo, maps.err);
+    if (maps.geo.NTX > 1) vel_fz<true><<<maps.grid, maps.threads, maps.vsmem, (cudaStream_t)stream>>>(g, fm, w, dt, maps.vgeo, maps.err);
+    else vel_fz<false><<<maps.grid, maps.threads, maps.vsmem, (cudaStream_t)stream>>>(g, fm, w, dt, maps.vgeo, maps.err);
     return cerr();
 }
 
@@ -2836,14 +2926,17 @@ int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const 
     std::memcpy(fm.psi, maps.psi, sizeof(maps.psi));
     cudaStream_t s = (cudaStream_t)stream;
     const dim3 grid(maps.grid), block(maps.threads);
+    const bool xt = maps.geo.NTX > 1;
+#define JV_FZ(M)                                                                                                 \
+    if (xt) stress_fz<M, true><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err); \
+    else stress_fz<M, false><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err)
     switch (mode) {
-    case kFwd: stress_fz<kFwd><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err); break;
-    case kRtmFwd:
-        stress_fz<kRtmFwd><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err);
-        break;
-    case kRev: stress_fz<kRev><<<grid, block, maps.smem, s>>>(g, fm, w, dt, wavelet, st, it_off, maps.geo, maps.err); break;
+    case kFwd: JV_FZ(kFwd); break;
+    case kRtmFwd: JV_FZ(kRtmFwd); break;
+    case kRev: JV_FZ(kRev); break;
     default: return (int)cudaErrorInvalidValue;
     }
+#undef JV_FZ
     return cerr();
 }
 

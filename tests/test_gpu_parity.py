@@ -296,3 +296,41 @@ def test_16bit_boundary_store_vs_oracle(oracle, synth, prec, img_tol, w):
     print("image rel-L2 vs FP64 oracle, FP32 store:", err[jv.JV_FP32], "16-bit store:", err[prec])
     for k, e in err[prec].items():
         assert np.isfinite(e) and e <= img_tol, (k, err)
+
+
+# grids wide enough that variant 4 cuts the x range into tiles (2-3 x tiles;
+# the absorbing strips ride with the first and last tile)
+WIDE = [
+    dict(n=(260, 10, 12), pml=8, nt=90, seed=51, shot_idx=[(3, 5, 6)], nrec=30),
+    dict(n=(300, 9, 10), pml=10, nt=80, seed=52, shot_idx=[(296, 4, 5)]),
+    dict(n=(510, 8, 9), pml=4, nt=70, seed=53, shot_idx=[(255, 4, 4)], nrec=20),
+]
+
+
+@pytest.mark.parametrize("kw", WIDE)
+def test_full_kernels_x_tiles_forward_vs_oracle(oracle, synth, kw):
+    s = synth.small_case(**kw)
+    ref = oracle.forward(_problem(oracle, s))
+    with jv.Context.from_survey(s) as ctx:
+        ctx.set_profiling(True)
+        tr = ctx.forward(0)
+        names = _kernels(ctx)
+    assert {"stress_fz_fwd", "vel_fz_fwd"} <= names, names
+    for a, b in zip(tr, ref):
+        assert np.all(np.isfinite(a))
+        assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
+
+
+def test_full_kernels_x_tiles_rtm_vs_oracle(oracle, synth):
+    s = synth.small_case(**dict(WIDE[0], rec_width=2, anomaly=(0.1, 3.0)))
+    p = _problem(oracle, s, 2)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    with jv.Context.from_survey(s) as ctx:
+        ctx.set_profiling(True)
+        ctx.rtm_shot(0, [o.astype(np.float32) for o in obs])
+        names = _kernels(ctx)
+        raw = ctx.images()
+    assert {"stress_fz_rtmfwd", "stress_fz_rev", "vel_fz_rtmfwd", "vel_fz_rev"} <= names, names
+    for k in ("ip", "pp", "ps", "sp", "ss"):
+        assert rel_l2(raw[k], ref[k]) <= 5e-5, (k, rel_l2(raw[k], ref[k]))
