@@ -140,7 +140,6 @@ BYTES_PER_CELL = {
     "stress_phy_rev": 4 * (3 + 2 + 7) + 4 * 7,
     "stress_phy_rtmfwd": 4 * (3 + 2 + 7) + 4 * 7,
     "stress_phy_fwd": 4 * (3 + 2 + 6) + 4 * 6,
-    "velp_rev": 4 * (1 + 1 + 3) + 4 * 3,
 }
 
 
@@ -182,8 +181,7 @@ FUSED = {"stress_fz_fwd": ("stress_phy_fwd", "stress_pml"),
          "stress_fz_rtmfwd": ("stress_phy_rtmfwd", "stress_pml_sau"),
          "stress_fz_rev": ("stress_phy_rev", "stress_pml_sau"),
          "vel_fz_fwd": ("vel_phy_fwd", "vel_pml"),
-         "vel_fz_rtmfwd": ("vel_phy_rtmfwd", "vel_pml"),
-         "vel_fz_rev": ("vel_phy_fwd", "vel_pml")}  # the receiver side's P-wave part is velp_rev
+         "vel_fz_rtmfwd": ("vel_phy_rtmfwd", "vel_pml")}
 
 
 def kernel_bytes(s, name):

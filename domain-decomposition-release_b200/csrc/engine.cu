@@ -411,6 +411,9 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
         fzpsiF_ = (float *)p;
         JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, &fullF_));
+        // the fused velocity update runs on one-tile grids, where it measured
+        // faster than the split kernels; x-tiled grids keep the split ones
+        vel_full_ = fullF_.ok && fullF_.geo.NTX == 1;
     }
 
     // wavelet and step state
@@ -659,7 +662,7 @@ Status Engine::launch_step(int kind, int off, bool advance) {
     const int rw = opt_.rec_width;
     switch (kind) {
     case kStepModel:
-        if (fullF_.ok) {
+        if (vel_full_) {
             JV_L("vel_fz_fwd", k_vel_full(g_, F_, dt, fullF_, s));
         } else {
             JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
@@ -676,7 +679,7 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         if (advance) JV_L("step_advance", k_step_advance(st_, +1, s));
         break;
     case kStepRtmFwd:
-        if (fullF_.ok) {
+        if (vel_full_) {
             JV_L("vel_fz_rtmfwd", k_vel_full(g_, F_, dt, fullF_, s));
         } else {
             JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
@@ -699,13 +702,11 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // injection + reverse velocity, stress boundary layers of step it-1
         JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, off, s));
         JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
-        if (fullR_.ok) {
-            JV_L("vel_fz_rev", k_vel_full(g_, R_, dt, fullR_, s));
-            JV_L("velp_rev", k_velp(g_, R_, rho_, dt, s));
-        } else {
-            JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
-            JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        }
+        // the receiver side's velocity update keeps the split kernels: with
+        // its P-wave velocities it measured no faster fused (cfg2), slower
+        // on x-tiled grids
+        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
+        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1

@@ -120,6 +120,7 @@ class Engine {
     FullMaps fullF_{}, fullR_{};  // TMA descriptors of the full-gridext stress kernel (variant 4)
     float *fzpsiF_ = nullptr, *fzpsiR_ = nullptr;  // its axis-major stress memory variables
     long long fz_psi_total_ = 0;                   // floats of one of them
+    bool vel_full_ = false;                        // the forward passes' velocity update runs in vel_fz
     int *zm_err_ = nullptr;       // device flag of variant 3's bounded waits
     Status check_zm_err();
     size_t field_elems_ = 0;  // elements per pitched field

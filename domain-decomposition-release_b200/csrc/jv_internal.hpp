@@ -232,8 +232,6 @@ int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const 
                   int it_off, const FullMaps &maps, void *stream);
 // Velocity update of every updated cell of gridext (variant 4; vx, vy, vz)
 int k_vel_full(const GridDev &g, const WaveDev &w, float dt, const FullMaps &maps, void *stream);
-// P-wave velocities (vxp, vyp, vzp) of the physical cells, receiver wavefield
-int k_velp(const GridDev &g, const WaveDev &w, const float *rho, float dt, void *stream);
 int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
               const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,

@@ -1945,8 +1945,10 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
 // planes (12 rows) of sxy, syy, syz; 4-row bands with the x halo of sxx
 // and sxz; the core tiles of rho, vp, vx, vy, vz; the window feed of sxz,
 // syz, szz five planes ahead; the memory-variable boxes.  The z windows
-// hold sxz, syz, szz.  The P-wave velocities of the receiver wavefield are
-// updated by velp_v4 beside it.
+// hold sxz, syz, szz.  It serves the passes without P-wave velocities
+// (forward modelling, the RTM forward pass) on grids of one x tile; the
+// receiver wavefield and x-tiled grids keep vel_phy_v4 + vel_pml, which
+// measured as fast or faster there.
 
 constexpr int kFvStage = 3 * kZmHB + 10 * kZmCB;  // halo planes, 2 bands, 5 core tiles, 3 feed tiles
 
@@ -2322,43 +2324,6 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     }
 }
 
-// P-wave velocities of the receiver wavefield (REV mode of vel_group4's
-// P part: Dp of sau on every axis, physical cells), for variant 4 where
-// vel_fz updates vx, vy, vz.
-__global__ void __launch_bounds__(256, 4) velp_v4(GridDev g, WaveDev w, const float *__restrict__ rho, float dt) {
-    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
-    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
-    const int pk = blockIdx.z;
-    if (pi0 >= g.px || pj >= g.py || pk >= g.pz) return;
-    const int nvalid = min(4, g.px - pi0);
-    const int sy = (int)g.sy, sz = (int)g.sz;
-    const int i0 = (int)g.xoff + (pi0 + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
-    const float *cx[4];
-    xcoefs<kRev>(pi0, g.px, 0, cx);
-    const float *c = c_list[kPhyHalf];
-    const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    float dtr[4], t[4], win[12], p[4];
-    {
-        const float4 r4 = ld4(rho, i0);
-        dtr[0] = dt / r4.x; dtr[1] = dt / r4.y; dtr[2] = dt / r4.z; dtr[3] = dt / r4.w;
-    }
-    xwin(w.f[SAU], i0, win);
-    xdp(win, cx, t);
-    f4a(p, ldw4(w.f[VXP], i0));
-#pragma unroll
-    for (int q = 0; q < 4; q++) p[q] += dtr[q] * (t[q] * rdx);
-    st4(w.f[VXP], i0, p, nvalid);
-    sdp(w.f[SAU], i0, sy, c, t);
-    f4a(p, ldw4(w.f[VYP], i0));
-#pragma unroll
-    for (int q = 0; q < 4; q++) p[q] += dtr[q] * (t[q] * rdy);
-    st4(w.f[VYP], i0, p, nvalid);
-    sdp(w.f[SAU], i0, sz, c, t);
-    f4a(p, ldw4(w.f[VZP], i0));
-#pragma unroll
-    for (int q = 0; q < 4; q++) p[q] += dtr[q] * (t[q] * rdz);
-    st4(w.f[VZP], i0, p, nvalid);
-}
 
 // ------------------------------------------------------------ receivers
 
@@ -2905,14 +2870,6 @@ int k_vel_full(const GridDev &g, const WaveDev &w, float dt, const FullMaps &map
     std::memcpy(fm.psi, maps.vpsi, sizeof(maps.vpsi));
     if (maps.geo.NTX > 1) vel_fz<true><<<maps.grid, maps.threads, maps.vsmem, (cudaStream_t)stream>>>(g, fm, w, dt, maps.vgeo, maps.err);
     else vel_fz<false><<<maps.grid, maps.threads, maps.vsmem, (cudaStream_t)stream>>>(g, fm, w, dt, maps.vgeo, maps.err);
-    return cerr();
-}
-
-int k_velp(const GridDev &g, const WaveDev &w, const float *rho, float dt, void *stream) {
-    const int ngx = (g.px + 3) / 4;
-    const int nb = (ngx + 63) / 64, gx = (ngx + nb - 1) / nb, gy = std::max(1, 256 / gx);
-    const dim3 b(gx, gy), gr((ngx + gx - 1) / gx, (g.py + gy - 1) / gy, g.pz);
-    velp_v4<<<gr, b, 0, (cudaStream_t)stream>>>(g, w, rho, dt);
     return cerr();
 }
 
