@@ -279,6 +279,46 @@ def serve_leg(jv, synth, n_req):
                     "warm-up requests on a server of their own are not counted"}
 
 
+def extra_configs(jv, synth, torch, device):
+    """The other configurations, one short measurement each (not the
+    headline): cfg1 plain forward modelling in full, and the large cfg3
+    grid's RTM shot with the FP16 boundary store, cut to a few time steps."""
+    out = {}
+    s = synth.cfg1()
+    with jv.Context.from_survey(s, device=device) as ctx:
+        i = ctx.info()
+        tr = torch.empty((3, max(i.n_recv, 1), i.nt), dtype=torch.float32, device=f"cuda:{device}")
+        ptrs = [tr[q].data_ptr() for q in range(3)]
+        ctx.forward_device(0, ptrs)  # warm-up (graph capture)
+        ms = []
+        for _ in range(3):
+            ctx.forward_device(0, ptrs)
+            ms.append(ctx.last_ms())
+        t = min(ms) / 1000.0
+        out["cfg1_forward"] = {"grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt, "n_recv": i.n_recv,
+                               "ms_per_shot": round(1000 * t, 2), "shots_per_h": round(3600.0 / t, 1),
+                               "gcell_updates_per_s": round(i.n_ext * s.nt / t / 1e9, 2)}
+    nt3 = 40
+    s = synth.cfg3(nt=nt3)
+    with jv.Context.from_survey(s, device=device, precision=jv.JV_FP16) as ctx:
+        i = ctx.info()
+        tr = torch.empty((3, i.n_recv, i.nt), dtype=torch.float32, device=f"cuda:{device}")
+        ptrs = [tr[q].data_ptr() for q in range(3)]
+        ctx.forward_device(0, ptrs)
+        ctx.rtm_shot_device(0, ptrs)  # warm-up
+        ctx.rtm_shot_device(0, ptrs)
+        t = ctx.last_ms() / 1000.0
+        cells = nt3 * (2 * i.n_ext + i.n_phy)
+        out["cfg3_rtm_fp16_store"] = {
+            "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt_run": nt3, "nt_config": 3000, "n_recv": i.n_recv,
+            "ms_per_step": round(1000 * t / nt3, 3), "gcell_updates_per_s": round(cells / t / 1e9, 2),
+            "shot_s_at_3000_steps": round(t / nt3 * 3000, 1),
+            "store_bytes_per_step": int(i.store_bytes_per_step), "device_bytes": int(i.device_bytes),
+            "note": "the configured 3000 steps cut to 40 to keep the bench short; per-step cost is constant"}
+        del tr
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -331,6 +371,7 @@ def main():
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server leg")
     ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--no-extra", action="store_true", help="skip the cfg1 / cfg3 side measurements")
     ap.add_argument("--ref-sample-steps", type=int, default=40)
     ap.add_argument("--variant", type=int, default=None, help="interior kernel variant (default: library default)")
     ap.add_argument("--store", default="fp32", choices=["fp32", "bf16", "fp16"],
@@ -486,6 +527,9 @@ def main():
     serving = None
     if world == 1 and not args.no_serve:
         serving = serve_leg(jv, jv.synth, args.serve_requests)
+    extra = None
+    if world == 1 and not args.no_extra:
+        extra = extra_configs(jv, jv.synth, torch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -524,7 +568,8 @@ def main():
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
                    "boundary_store": args.store,
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "serving": serving, "clocks": clk,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "serving": serving,
+        "other_configs": extra, "clocks": clk,
         "gpu_launches": launches * args.steps if launches else None,
         "gpu_launches_note": "kernels of the timed shots, counted from one instrumented shot (graph path)",
         "wall_s": round(wall, 3),

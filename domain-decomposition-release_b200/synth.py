@@ -142,6 +142,22 @@ def cfg2(rec_width: int = 1, seed: int = 2, nt: int = 2000) -> Survey:
                   _pos(rec, d), rec_width=rec_width, name=f"cfg2_rtm_200_w{rec_width}", seed=seed)
 
 
+def cfg3(nt: int = 3000, seed: int = 3, rec_step: int = 4) -> Survey:
+    """Precision form, large model: 676 x 676 x 210 + 20 CPML, d = 10 m,
+    dt = 0.8 ms, vp in [1800, 4500] m/s in 4 layers with 3 dipping
+    interfaces.  Choices where the configuration is silent: the source at
+    the surface centre, depth 5 cells; receivers every rec_step cells on the
+    surface grid at z = 5."""
+    nx, ny, nz = 676, 676, 210
+    vp = layered_vp(nx, ny, nz, seed, n_layers=4, vmin=1800, vmax=4500, dip=True)
+    vp, vs, rho = gardner(vp)
+    d = (10.0, 10.0, 10.0)
+    jj, ii = np.meshgrid(np.arange(0, ny, rec_step), np.arange(0, nx, rec_step), indexing="ij")
+    rec = np.stack([ii.ravel(), jj.ravel(), np.full(ii.size, 5)], axis=1)
+    return Survey(nx, ny, nz, 20, 10.0, 10.0, 10.0, 8e-4, 20.0, nt, vp, vs, rho, _pos([(nx // 2, ny // 2, 5)], d),
+                  _pos(rec, d), name="cfg3_large_676x676x210", seed=seed)
+
+
 def scaled_cfg2(n: int, nt: int, rec_width: int = 1, seed: int = 2, pml: int = 20) -> Survey:
     """cfg2's construction at another size (same spacing, source at the
     centre of the surface at depth 5 cells, full receiver plane at z=5)."""
