@@ -291,11 +291,19 @@ class Context:
         return {k: self.image(v) for k, v in (("ip", IMG_IP), ("pp", IMG_PP), ("ps", IMG_PS), ("sp", IMG_SP),
                                               ("ss", IMG_SS))}
 
-    def finalize(self):
-        """(compensated {pp,ps,sp,ss}, laplacian {pp,ps,sp,ss}) float32."""
+    def finalize(self, out=None):
+        """(compensated {pp,ps,sp,ss}, laplacian {pp,ps,sp,ss}) float32.  out:
+        eight C-contiguous float32 arrays of gridphy to fill (e.g. views of
+        pinned memory, reused across shots); None allocates them."""
         i = self.info()
         shp = (i.grid.nz, i.grid.ny, i.grid.nx)
-        arr = [np.zeros(shp, np.float32) for _ in range(8)]
+        if out is None:
+            arr = [np.zeros(shp, np.float32) for _ in range(8)]
+        else:
+            arr = list(out)
+            if len(arr) != 8 or any(a.dtype != np.float32 or not a.flags.c_contiguous or a.size != i.n_phy
+                                    for a in arr):
+                raise JvError(JV_EINVAL, "finalize(out=...) takes eight C-contiguous float32 arrays of gridphy")
         _check(lib().jv_image_finalize(self._h, *[_fptr(a) for a in arr]))
         keys = ("pp", "ps", "sp", "ss")
         return dict(zip(keys, arr[:4])), dict(zip(keys, arr[4:]))
