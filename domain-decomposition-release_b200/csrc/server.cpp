@@ -65,6 +65,11 @@ struct jv_server {
     std::vector<std::thread> workers;
     std::vector<double> latencies_ms;
     long long n_completed = 0, n_failed = 0, n_cancelled = 0;
+    // the device's stream-ordered pool keeps up to the budget cached while
+    // the server is open (contexts of later requests reuse it instead of
+    // mapping fresh memory); the previous threshold is put back at close
+    cudaMemPool_t pool = nullptr;
+    uint64_t pool_threshold_before = 0;
 };
 
 namespace {
@@ -196,6 +201,15 @@ jv_status jv_server_create(int device, int slots, size_t hbm_budget, jv_server *
     jv_server *s = new jv_server();
     s->device = device;
     s->budget = budget;
+    cudaSetDevice(device);
+    if (cudaDeviceGetDefaultMemPool(&s->pool, device) == cudaSuccess &&
+        cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &s->pool_threshold_before) == cudaSuccess) {
+        uint64_t keep = budget;
+        if (cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) s->pool = nullptr;
+    } else {
+        s->pool = nullptr;
+        cudaGetLastError();
+    }
     for (int k = 0; k < slots; k++) s->workers.emplace_back(worker_main, s);
     *out = s;
     jv::set_last_error("");
@@ -310,6 +324,11 @@ jv_status jv_server_close(jv_server *s) {
     s->done_cv.notify_all();
     for (std::thread &t : s->workers)
         if (t.joinable()) t.join();
+    if (s->pool) {
+        cudaSetDevice(s->device);
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &s->pool_threshold_before);
+        cudaMemPoolTrimTo(s->pool, 0);  // hand the cached memory back
+    }
     delete s;
     return JV_OK;
 }
