@@ -122,6 +122,7 @@ Engine::~Engine() {
     for (void *p : allocs_)
         if (p) cudaFreeAsync(p, stream_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (host_store_) cudaFreeHost(host_store_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -841,23 +842,41 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         size_t freeb = 0, totalb = 0;
         JV_CU(cudaMemGetInfo(&freeb, &totalb));
         size_t budget = opt_.store_budget ? opt_.store_budget : (freeb > (2ULL << 30) ? freeb - (2ULL << 30) : 0);
-        if (opt_.store_mode == JV_STORE_HOST || bytes > budget)
-            return bad(JV_ENOTSUP, "boundary store of " + std::to_string(bytes) +
-                                       " bytes does not fit the device budget; host streaming is not built");
-        void *p;
+        const size_t nrec = (size_t)per_step_ * nslot_;
+        const size_t rec_bytes = nrec * (s16 ? sizeof(uint16_t) : sizeof(float));
+        // placement: the device when the store fits its budget, else (or
+        // when asked) pinned host memory mapped into the device's address
+        // space -- the pack and unpack kernels then write and read it across
+        // the host link, each step's record in one contiguous range
+        const bool on_host = opt_.store_mode == JV_STORE_HOST || (opt_.store_mode != JV_STORE_DEVICE && bytes > budget);
+        if (!on_host && bytes > budget)
+            return bad(JV_ENOMEM, "boundary store of " + std::to_string(bytes) + " bytes does not fit the device budget of " +
+                                      std::to_string(budget) + " bytes (store_mode JV_STORE_HOST keeps it in host memory)");
+        void *rec = nullptr, *p;
+        if (on_host) {
+            void *h = nullptr;
+            cudaError_t e = cudaHostAlloc(&h, rec_bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return bad(JV_ENOMEM, "pinned host allocation of " + std::to_string(rec_bytes) +
+                                          " bytes for the boundary store failed: " + cudaGetErrorString(e));
+            }
+            host_store_ = h;
+            JV_CU(cudaHostGetDevicePointer(&rec, h, 0));
+        } else {
+            JV_TRY(alloc(&rec, rec_bytes));
+        }
+        store_on_host_ = on_host;
         if (s16) {
-            // 16-bit records, then one FP32 scale per box and step, then the
-            // two rows of largest magnitudes
-            const size_t nrec = (size_t)per_step_ * nslot_;
-            JV_TRY(alloc(&p, round_up((long long)(nrec * sizeof(uint16_t)), 256) +
-                                 (size_t)vowr_.nseg * (nslot_ + 2) * sizeof(float)));
-            vowr_.store16 = (uint16_t *)p;
-            vowr_.scales = (float *)((char *)p + round_up((long long)(nrec * sizeof(uint16_t)), 256));
+            // 16-bit records; on the device one FP32 scale per box and step,
+            // then the two rows of largest magnitudes
+            JV_TRY(alloc(&p, (size_t)vowr_.nseg * (nslot_ + 2) * sizeof(float)));
+            vowr_.store16 = (uint16_t *)rec;
+            vowr_.scales = (float *)p;
             vowr_.amax = (unsigned *)(vowr_.scales + (size_t)vowr_.nseg * nslot_);
             JV_CU(cudaMemsetAsync(vowr_.amax, 0, 2 * (size_t)vowr_.nseg * sizeof(unsigned), stream_));
         } else {
-            JV_TRY(alloc(&p, bytes));
-            store_ = (float *)p;
+            store_ = (float *)rec;
             vowr_.store = store_;
         }
     }
@@ -974,7 +993,7 @@ void Engine::info(jv_info *i) const {
     i->n_phy = (long long)g_.px * g_.py * g_.pz;
     i->store_bytes_per_step = (size_t)per_step_ * (opt_.precision == JV_FP32 ? sizeof(float) : sizeof(uint16_t));
     i->device_bytes = dev_bytes_;
-    i->store_on_device = 1;
+    i->store_on_device = store_on_host_ ? 0 : 1;
 }
 
 }  // namespace jv

@@ -149,6 +149,8 @@ class Engine {
     VowrDev vowr_{};
     long long per_step_ = 0;
     float *store_ = nullptr;
+    void *host_store_ = nullptr;   // pinned, mapped host memory of a host-resident store
+    bool store_on_host_ = false;
     int nslot_ = 0;
 
     StackDev img_{};             // FP64 stacks over shots

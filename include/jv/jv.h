@@ -67,7 +67,10 @@ typedef struct jv_grid {
  * arithmetic is FP32. */
 typedef enum jv_precision { JV_FP32 = 0, JV_BF16 = 1, JV_FP16 = 2 } jv_precision;
 
-/* Boundary-store placement for VOWR. */
+/* Boundary-store placement for VOWR: DEVICE = HBM (JV_ENOMEM beyond
+ * store_budget), HOST = pinned host memory mapped into the device (the pack
+ * and unpack kernels cross the host link), AUTO = the device when the store
+ * fits, else the host. */
 typedef enum jv_store_mode { JV_STORE_AUTO = 0, JV_STORE_DEVICE = 1, JV_STORE_HOST = 2 } jv_store_mode;
 
 typedef struct jv_options {

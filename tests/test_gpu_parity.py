@@ -336,3 +336,22 @@ def test_full_kernels_x_tiles_rtm_vs_oracle(oracle, synth):
     assert {"stress_fz_rtmfwd", "stress_fz_rev"} <= names and "stress_pml_sau" not in names, names
     for k in ("ip", "pp", "ps", "sp", "ss"):
         assert rel_l2(raw[k], ref[k]) <= 5e-5, (k, rel_l2(raw[k], ref[k]))
+
+
+@pytest.mark.parametrize("prec", [jv.JV_FP32, jv.JV_FP16])
+def test_host_resident_boundary_store(synth, prec):
+    """The boundary store in pinned host memory mapped into the device
+    (store_mode JV_STORE_HOST, or a device budget too small under AUTO): the
+    same images, bit for bit, as the store in HBM."""
+    s = synth.small_case(n=(22, 18, 21), pml=6, nt=120, seed=21, rec_width=2, shot_idx=[(11, 9, 3)])
+    out = {}
+    for name, opts in (("device", dict(store_mode=jv.JV_STORE_DEVICE)), ("host", dict(store_mode=jv.JV_STORE_HOST)),
+                       ("auto_small_budget", dict(store_mode=jv.JV_STORE_AUTO, store_budget=1))):
+        with jv.Context.from_survey(s, precision=prec, **opts) as ctx:
+            obs = ctx.forward(0)
+            ctx.rtm_shot(0, obs)
+            out[name] = (ctx.images(), ctx.info().store_on_device)
+    assert out["device"][1] == 1 and out["host"][1] == 0 and out["auto_small_budget"][1] == 0
+    for name in ("host", "auto_small_budget"):
+        for k in out["device"][0]:
+            assert np.array_equal(out[name][0][k], out["device"][0][k]), (name, k)
