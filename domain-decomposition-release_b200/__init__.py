@@ -37,7 +37,8 @@ IMG_IP, IMG_PP, IMG_PS, IMG_SP, IMG_SS = range(5)
 
 # every symbol include/jv/jv.h declares
 EXPORTS = (
-    "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_get_info", "jv_forward",
+    "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_get_info", "jv_get_kernel_config",
+    "jv_forward",
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
     "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
     "jv_last_timing", "jv_sync", "jv_close", "jv_last_error", "jv_build_info", "jv_forward_noalloc",
@@ -144,6 +145,7 @@ def lib() -> C.CDLL:
     L.jv_open.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(ctxp)]
     L.jv_set_geometry.argtypes = [ctxp, C.c_int, fp, C.c_int, fp]
     L.jv_get_info.argtypes = [ctxp, C.POINTER(Info)]
+    L.jv_get_kernel_config.argtypes = [ctxp, C.POINTER(Options)]
     L.jv_forward.argtypes = [ctxp, C.c_int, fp, fp, fp]
     L.jv_forward_device.argtypes = [ctxp, C.c_int, vp, vp, vp]
     L.jv_rtm_shot.argtypes = [ctxp, C.c_int, fp, fp, fp]
@@ -249,6 +251,12 @@ class Context:
         _check(lib().jv_set_geometry(self._h, sh.shape[0], _fptr(sh), rc.shape[0], _fptr(rc)))
 
     # -- queries ------------------------------------------------------------
+    def kernel_config(self) -> dict:
+        """The options this context runs with, the kernel choice as made."""
+        o = Options()
+        _check(lib().jv_get_kernel_config(self._h, C.byref(o)))
+        return {k: getattr(o, k) for k, _ in Options._fields_}
+
     def info(self) -> Info:
         i = Info()
         _check(lib().jv_get_info(self._h, C.byref(i)))

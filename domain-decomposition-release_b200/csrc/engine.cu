@@ -9,10 +9,13 @@
 #include "engine.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace jv {
 
@@ -317,7 +320,8 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread < 0 || opt.planes_per_thread > 2 || opt.pml_planes_per_thread < 0 ||
         opt.pml_planes_per_thread > 2)
         return bad(JV_EINVAL, "planes_per_thread and pml_planes_per_thread must be 0, 1 or 2");
-    if (opt.kernel_variant < 0 || opt.kernel_variant > 4) return bad(JV_EINVAL, "kernel_variant must be 0..4");
+    if (opt.kernel_variant < -1 || opt.kernel_variant > 4)
+        return bad(JV_EINVAL, "kernel_variant must be 0..4, or -1 (measured choice)");
     if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
         return bad(JV_EINVAL, "tile_gx * tile_gy must be <= 256");
     long long next = (long long)(grid.nx + 2 * grid.pml) * (grid.ny + 2 * grid.pml) * (grid.nz + 2 * grid.pml);
@@ -332,7 +336,10 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     E->fm_ = fm;
     E->nt_ = nt;
     E->dev_ = opt.device;
-    E->kc_.variant = opt.kernel_variant;
+    // -1: the resources of variant 4 (a superset of 3's and 2's), then the
+    // measured choice after allocation
+    const bool tune = opt.kernel_variant < 0;
+    E->kc_.variant = tune ? 4 : opt.kernel_variant;
     E->kc_.zchunk = opt.zchunk;
     E->kc_.gx = opt.tile_gx;
     E->kc_.gy = opt.tile_gy;
@@ -343,11 +350,84 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
+    if (s && tune) s = E->autotune();
     if (!s) {
         delete E;
         return s;
     }
     *out = E;
+    return Status{};
+}
+
+// The measured kernel choice (kernel_variant -1): a few forward-modelling
+// steps of each candidate on this grid -- variant 4 where its kernels
+// apply, variant 3 where its stress kernel applies, variant 2 -- and, for
+// the variants with separate absorbing-layer kernels, their register
+// budget (3 or 4 blocks per SM).  The fastest wins; the choice is kept per
+// grid shape and device for the contexts that follow.
+Status Engine::autotune() {
+    struct Cand {
+        int variant, pml_minb;
+    };
+    static std::mutex mu;
+    static std::map<std::array<long long, 6>, Cand> cache;
+    int dev = 0;
+    JV_CU(cudaGetDevice(&dev));
+    cudaDeviceProp prop{};
+    JV_CU(cudaGetDeviceProperties(&prop, dev));
+    const std::array<long long, 6> key = {grid_.nx, grid_.ny, grid_.nz, grid_.pml, prop.multiProcessorCount,
+                                          (long long)prop.totalGlobalMem};
+    auto apply = [&](const Cand &c) {
+        kc_.variant = c.variant;
+        kc_.pml_minb = c.pml_minb;
+        use_full_ = c.variant == 4 && fullF_.ok;
+        vel_full_ = use_full_ && fullF_.geo.NTX == 1;
+    };
+    {
+        std::lock_guard<std::mutex> l(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            apply(it->second);
+            return Status{};
+        }
+    }
+    std::vector<Cand> cands;
+    if (fullF_.ok) cands.push_back({4, 4});
+    if (mapsF_.ok) {
+        cands.push_back({3, 4});
+        cands.push_back({3, 3});
+    }
+    cands.push_back({2, 4});
+    cands.push_back({2, 3});
+    const long long src = (long long)g_.xoff + (g_.m + g_.px / 2) + g_.sy * (g_.m + g_.py / 2) +
+                          g_.sz * (g_.m + g_.pz / 2);
+    float best = -1.f;
+    Cand pick = cands[0];
+    const int warm = 2, steps = 6;
+    for (const Cand &c : cands) {
+        apply(c);
+        JV_TRY(zero_wave(F_, 9));
+        JV_TRY(zero_psi(cpF_));
+        JV_TRY(set_state(0, src, nullptr, nullptr));
+        for (int i = 0; i < warm; i++) JV_TRY(launch_step(kStepModel, 0, true));
+        JV_CU(cudaEventRecord(ev0_, stream_));
+        for (int i = 0; i < steps; i++) JV_TRY(launch_step(kStepModel, 0, true));
+        JV_CU(cudaEventRecord(ev1_, stream_));
+        JV_CU(cudaEventSynchronize(ev1_));
+        JV_TRY(check_zm_err());
+        float ms = 0.f;
+        JV_CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+        if (best < 0.f || ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    apply(pick);
+    JV_TRY(zero_wave(F_, 9));
+    JV_TRY(zero_psi(cpF_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    std::lock_guard<std::mutex> l(mu);
+    cache[key] = pick;
     return Status{};
 }
 
@@ -414,6 +494,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, &fullF_));
         // the fused velocity update runs on one-tile grids, where it measured
         // faster than the split kernels; x-tiled grids keep the split ones
+        use_full_ = fullF_.ok;
         vel_full_ = fullF_.ok && fullF_.geo.NTX == 1;
     }
 
@@ -669,7 +750,7 @@ Status Engine::launch_step(int kind, int off, bool advance) {
             JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
             JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         }
-        if (fullF_.ok) {
+        if (use_full_) {
             JV_L("stress_fz_fwd", k_stress_full(kFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
         } else {
             JV_L("stress_pml", k_stress_pml(g_, cpF_, F_, lam_, mu_, vp_, 0, kc_, s));
@@ -686,7 +767,7 @@ Status Engine::launch_step(int kind, int off, bool advance) {
             JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
             JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
         }
-        if (fullF_.ok) {
+        if (use_full_) {
             // the boundary boxes lie in the absorbing layers: pack them after their update
             JV_L("stress_fz_rtmfwd", k_stress_full(kRtmFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
             JV_L("vowr_pack", k_vowr(g_, F_, vowr_, st_, off, 1, 0, s));

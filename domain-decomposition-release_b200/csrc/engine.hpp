@@ -100,6 +100,20 @@ class Engine {
     Status check_shot(int shot, long long *src) const;
     Status run_loop(int kind, int nsteps);
     Status launch_step(int kind, int off, bool advance);
+    Status autotune();
+
+  public:
+    // the options this context runs with, the kernel choice as made
+    void kernel_config(jv_options *o) const {
+        *o = opt_;
+        o->kernel_variant = kc_.variant;
+        o->min_blocks = kc_.minb;
+        o->pml_min_blocks = kc_.pml_minb;
+        o->planes_per_thread = kc_.zp;
+        o->pml_planes_per_thread = kc_.pml_zp;
+    }
+
+  private:
     Status cu(cudaError_t e, const char *what) const;
     Status zero_wave(const WaveDev &w, int nfld);
     Status zero_psi(const CpmlDev &c);
@@ -120,6 +134,7 @@ class Engine {
     FullMaps fullF_{}, fullR_{};  // TMA descriptors of the full-gridext stress kernel (variant 4)
     float *fzpsiF_ = nullptr, *fzpsiR_ = nullptr;  // its axis-major stress memory variables
     long long fz_psi_total_ = 0;                   // floats of one of them
+    bool use_full_ = false;                        // the stress update of absorbing steps runs in stress_fz
     bool vel_full_ = false;                        // the forward passes' velocity update runs in vel_fz
     int *zm_err_ = nullptr;       // device flag of variant 3's bounded waits
     Status check_zm_err();

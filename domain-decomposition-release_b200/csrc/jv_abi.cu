@@ -272,6 +272,12 @@ jv_status jv_get_info(const jv_ctx *c, jv_info *info) {
     return JV_OK;
 }
 
+jv_status jv_get_kernel_config(const jv_ctx *c, jv_options *out) {
+    if (!c || !out) return fail(JV_EINVAL, "NULL argument");
+    c->eng->kernel_config(out);
+    return JV_OK;
+}
+
 jv_status jv_forward_device(jv_ctx *c, int shot, float *d_vx, float *d_vy, float *d_vz) {
     JV_IDLE(c);
     return ret(c->eng->forward(shot, d_vx, d_vy, d_vz));

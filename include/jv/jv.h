@@ -84,7 +84,10 @@ typedef struct jv_options {
     int kernel_variant; /* stencil kernels: 0 one plane per block, 1 z-marching, 2 x-vectorised,
                            3 as 2 with a TMA-fed z-marching stress update, 4 (default) as 3
                            with the absorbing layers' stress update in the same TMA kernel
-                           (even pml_num and nx; other grids run variant 3's kernels) */
+                           (even pml_num and nx; other grids run variant 3's kernels);
+                           -1: measured choice among 4, 3, 2 (and the absorbing-layer
+                           register budget) on this grid at creation, kept per grid shape;
+                           jv_get_kernel_config reports it */
     int zchunk;         /* z planes per block for variant 1 (0 -> auto)          */
     int tile_gx;        /* variant 2: 4-cell x groups per block (0 -> auto)      */
     int tile_gy;        /* variant 2: rows per block (0 -> auto)                 */
@@ -97,6 +100,7 @@ typedef struct jv_options {
 /* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,
  * graphs on). */
 void jv_options_default(jv_options *o);
+
 
 /* Creates a context from host model arrays on gridphy (vp, vs, rho).
  * Replaces elasticGeoModel<global/local>::initialize
@@ -152,6 +156,11 @@ typedef struct jv_info {
     int store_on_device; /* 1: boundary store in HBM, 0: pinned host  */
 } jv_info;
 jv_status jv_get_info(const jv_ctx *c, jv_info *info);
+
+/* The options a context runs with: those it was created with, with the
+ * kernel choice (kernel_variant, register budgets, planes per thread) as
+ * made -- after kernel_variant -1, the measured one. */
+jv_status jv_get_kernel_config(const jv_ctx *c, jv_options *out);
 
 /* Forward modelling of one shot: replaces
  * fdtd3d_blend_elastic_model_mpi_module<pure_forward>::reset_for_next_shot

@@ -355,3 +355,24 @@ def test_host_resident_boundary_store(synth, prec):
     for name in ("host", "auto_small_budget"):
         for k in out["device"][0]:
             assert np.array_equal(out[name][0][k], out["device"][0][k]), (name, k)
+
+
+def test_measured_kernel_choice(oracle, synth):
+    """kernel_variant -1: the context times the candidate variants on its
+    grid at creation and keeps the fastest; the choice is reported, reused
+    for the next context of the same shape, and its results match the
+    oracle."""
+    s = synth.small_case(n=(40, 24, 20), pml=8, nt=100, seed=61)
+    ref = oracle.forward(_problem(oracle, s))
+    picks = []
+    for _ in range(2):
+        with jv.Context.from_survey(s, kernel_variant=-1) as ctx:
+            cfg = ctx.kernel_config()
+            tr = ctx.forward(0)
+        picks.append((cfg["kernel_variant"], cfg["pml_min_blocks"]))
+        assert cfg["kernel_variant"] in (2, 3, 4) and cfg["pml_min_blocks"] in (3, 4)
+        for a, b in zip(tr, ref):
+            assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
+    assert picks[0] == picks[1], picks  # the second context reuses the first one's choice
+    with jv.Context.from_survey(s) as ctx:
+        assert ctx.kernel_config()["kernel_variant"] == 4
