@@ -47,6 +47,9 @@ sys.path.insert(0, ROOT)
 METRIC = "RTM shots/h & Gcell-updates/s, batched+served vs plain, 1 B200, rel-L2≤1e-3"
 
 
+NOMINAL_HBM_GBS = 7700.0  # B200 HBM3e, NVIDIA's HGX figure; reported beside the measured peak
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -468,6 +471,7 @@ def main():
             tr = traffic_from_profiles(name)
             roof = {"bound": "hbm", "kernel": name, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(ach / peak, 4), "peak_source": peak_kind,
+                    "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": round(ach / NOMINAL_HBM_GBS, 4),
                     "traffic": tr, "algorithmic_bytes_per_launch": b, "avg_launch_us": round(avg_s * 1e6, 2),
                     "share": round(ms / tot, 4) if tot > 0 else None}
 

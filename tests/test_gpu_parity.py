@@ -3,10 +3,11 @@ against the reference's own outputs.
 
 Tolerances (relative L2), FP32 GPU arithmetic:
   traces vs FP64 oracle ............................. 2e-5
-  traces vs reference (7-digit text, FP32) .......... 1e-5
+  traces vs reference (7-digit text, FP32) .......... 5e-6
   raw stacked images / Ip vs FP64 oracle ............ 5e-5
-  uncompensated images vs reference ................. 3e-5
-  Laplacian of uncompensated pp ..................... 5e-5
+  uncompensated images vs reference ................. 1e-5
+  Ip vs reference ................................... 2e-5
+  Laplacian of uncompensated pp vs reference ........ 1e-5
   compensated images (division by small Ip) ......... 2e-3
 """
 import numpy as np
@@ -55,7 +56,11 @@ def test_forward_vs_oracle(oracle, synth, kw, graphs, variant):
 @pytest.mark.parametrize("name", list(mg.CASES))
 def test_pins_vs_reference(synth, name):
     """Traces and images of the full reference job against the reference's
-    own outputs (tests/golden/ref_*.npz)."""
+    own outputs (tests/golden/ref_*.npz).  Measured on the three cases:
+    traces <= 1.2e-6, uncompensated images 2.1-7.5e-6, Laplacian of pp
+    <= 6.5e-6, Ip <= 1.3e-5 relative L2.  The compensated images divide by
+    a small illumination and amplify the reference's own FP32 noise (up to
+    7.6e-4)."""
     s = mg.case_survey(name)
     f = np.load(f"{mg.os.path.dirname(mg.__file__)}/ref_{name}.npz")
     with jv.Context.from_survey(s) as ctx:
@@ -63,16 +68,16 @@ def test_pins_vs_reference(synth, name):
         for sh in range(s.shots.shape[0]):
             tr = ctx.forward(sh)
             for c, t in zip(("vx", "vy", "vz"), tr):
-                assert rel_l2(t, f[f"tr_{c}_{sh}"]) <= 1e-5, (sh, c, rel_l2(t, f[f"tr_{c}_{sh}"]))
+                assert rel_l2(t, f[f"tr_{c}_{sh}"]) <= 5e-6, (sh, c, rel_l2(t, f[f"tr_{c}_{sh}"]))
             ctx.rtm_shot(sh, tr)
         raw = ctx.images()
         comp, lap = ctx.finalize()
     ip = f["img_ip"].astype(np.float64)
-    assert rel_l2(raw["ip"], ip) <= 5e-5
-    assert rel_l2(lap["pp"], f["lap_pp"]) <= 5e-5
+    assert rel_l2(raw["ip"], ip) <= 2e-5
+    assert rel_l2(lap["pp"], f["lap_pp"]) <= 1e-5
     for k in ("pp", "ps", "sp", "ss"):
         unc = f["img_" + k].astype(np.float64) * np.where(ip > 3.4e-38, ip, 1.0)
-        assert rel_l2(raw[k], unc) <= 3e-5, (k, rel_l2(raw[k], unc))
+        assert rel_l2(raw[k], unc) <= 1e-5, (k, rel_l2(raw[k], unc))
         assert rel_l2(comp[k], f["img_" + k]) <= 2e-3, (k, rel_l2(comp[k], f["img_" + k]))
 
 
