@@ -38,6 +38,7 @@ IMG_IP, IMG_PP, IMG_PS, IMG_SP, IMG_SS = range(5)
 # every symbol include/jv/jv.h declares
 EXPORTS = (
     "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_get_info", "jv_get_kernel_config",
+    "jv_reconstruction_energy",
     "jv_forward",
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
     "jv_image_finalize", "jv_image_get_device", "jv_run_project", "jv_set_profiling", "jv_profile_entry",
@@ -146,6 +147,7 @@ def lib() -> C.CDLL:
     L.jv_set_geometry.argtypes = [ctxp, C.c_int, fp, C.c_int, fp]
     L.jv_get_info.argtypes = [ctxp, C.POINTER(Info)]
     L.jv_get_kernel_config.argtypes = [ctxp, C.POINTER(Options)]
+    L.jv_reconstruction_energy.argtypes = [ctxp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.jv_forward.argtypes = [ctxp, C.c_int, fp, fp, fp]
     L.jv_forward_device.argtypes = [ctxp, C.c_int, vp, vp, vp]
     L.jv_rtm_shot.argtypes = [ctxp, C.c_int, fp, fp, fp]
@@ -251,6 +253,13 @@ class Context:
         _check(lib().jv_set_geometry(self._h, sh.shape[0], _fptr(sh), rc.shape[0], _fptr(rc)))
 
     # -- queries ------------------------------------------------------------
+    def reconstruction_energy(self):
+        """(energy at the end of the last RTM shot's forward pass, energy left
+        after its reconstruction back to t = 0), FP64."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().jv_reconstruction_energy(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def kernel_config(self) -> dict:
         """The options this context runs with, the kernel choice as made."""
         o = Options()

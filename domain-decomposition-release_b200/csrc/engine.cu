@@ -968,13 +968,25 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
     JV_TRY(zero_psi(cpF_));
     JV_TRY(set_state(0, src, nullptr, obs));
     JV_TRY(run_loop(kStepRtmFwd, nt_));
+    // reconstruction check: the source wavefield's FP64 energy over gridphy
+    // where the reconstruction starts, and what is left of it when the
+    // reverse loop has carried it back to its zero initial state
+    if (!energy_d_) {
+        void *p;
+        JV_TRY(alloc(&p, 2 * sizeof(double)));
+        energy_d_ = (double *)p;
+    }
+    JV_CU(cudaMemsetAsync(energy_d_, 0, 2 * sizeof(double), stream_));
+    JV_K(k_wave_energy(g_, F_, energy_d_, stream_));
     // time reverse: backward (reconstruction) + reverse (receivers) + image
     JV_TRY(zero_wave(R_, kNumFld));
     JV_TRY(zero_psi(cpR_));
     JV_TRY(set_state(nt_ - 1, src, nullptr, obs));
     JV_CU(cudaMemsetAsync(shot_img_.ip, 0, 5 * shot_img_pitch_ * sizeof(float), stream_));
     JV_TRY(run_loop(kStepRtmRev, nt_));
+    JV_K(k_wave_energy(g_, F_, energy_d_ + 1, stream_));
     JV_K(k_image_stack(g_, shot_img_, img_, stream_));
+    JV_CU(cudaMemcpyAsync(recon_energy_, energy_d_, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     JV_CU(cudaEventRecord(ev1_, stream_));
     JV_CU(cudaEventSynchronize(ev1_));
     JV_CU(cudaGetLastError());

@@ -134,6 +134,18 @@ class Engine {
     FullMaps fullF_{}, fullR_{};  // TMA descriptors of the full-gridext stress kernel (variant 4)
     float *fzpsiF_ = nullptr, *fzpsiR_ = nullptr;  // its axis-major stress memory variables
     long long fz_psi_total_ = 0;                   // floats of one of them
+    double *energy_d_ = nullptr;          // device: the two energies of the reconstruction check
+    double recon_energy_[2] = {0.0, 0.0};  // host copy after each RTM shot
+
+  public:
+    // FP64 energy of the source wavefield over gridphy at the end of the last
+    // RTM shot's forward pass, and after its reconstruction back to t = 0
+    void reconstruction_energy(double *fwd, double *res) const {
+        *fwd = recon_energy_[0];
+        *res = recon_energy_[1];
+    }
+
+  private:
     bool use_full_ = false;                        // the stress update of absorbing steps runs in stress_fz
     bool vel_full_ = false;                        // the forward passes' velocity update runs in vel_fz
     int *zm_err_ = nullptr;       // device flag of variant 3's bounded waits

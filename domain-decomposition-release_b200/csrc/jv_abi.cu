@@ -272,6 +272,12 @@ jv_status jv_get_info(const jv_ctx *c, jv_info *info) {
     return JV_OK;
 }
 
+jv_status jv_reconstruction_energy(const jv_ctx *c, double *e_forward_end, double *e_residual) {
+    if (!c || !e_forward_end || !e_residual) return fail(JV_EINVAL, "NULL argument");
+    c->eng->reconstruction_energy(e_forward_end, e_residual);
+    return JV_OK;
+}
+
 jv_status jv_get_kernel_config(const jv_ctx *c, jv_options *out) {
     if (!c || !out) return fail(JV_EINVAL, "NULL argument");
     c->eng->kernel_config(out);

@@ -253,6 +253,8 @@ int k_step_advance(StepState *st, int delta, void *stream);
 int k_image_finalize(const GridDev &g, const StackDev &img, float *out /* 8 arrays */, void *stream);
 // stack += shot image (FP64 sums of the FP32 shot accumulators)
 int k_image_stack(const GridDev &g, const ImageDev &shot, const StackDev &stack, void *stream);
+// FP64 energy of the velocity and stress fields of w over gridphy, added into *out
+int k_wave_energy(const GridDev &g, const WaveDev &w, double *out, void *stream);
 int upload_coefficients(const float list[5][4], const float dc2[2]);
 int k_count_nonfinite(const void *p, size_t n, int is_double, unsigned long long *out, void *stream);
 

@@ -2445,6 +2445,26 @@ __global__ void count_nonfinite_f(const float *p, size_t n, unsigned long long *
         c += !isfinite(p[i]);
     if (c) atomicAdd(out, c);
 }
+// FP64 energy (sum of squares) of the nine velocity and stress fields over
+// gridphy, added into *out
+__global__ void wave_energy(GridDev g, WaveDev w, double *out) {
+    const long long n = (long long)g.px * g.py * g.pz;
+    double e = 0.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long t = c / g.px;
+        const int x = (int)(c - t * g.px), y = (int)(t % g.py), z = (int)(t / g.py);
+        const long long i = g.xoff + (x + g.m) + g.sy * (y + g.m) + g.sz * (z + g.m);
+#pragma unroll
+        for (int f = VX; f <= SYZ; f++) {
+            const double v = w.f[f][i];
+            e += v * v;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(out, e);
+}
+
 __global__ void count_nonfinite_d(const double *p, size_t n, unsigned long long *out) {
     unsigned long long c = 0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -3034,6 +3054,11 @@ int k_vowr(const GridDev &g, const WaveDev &w, const VowrDev &v, const StepState
 
 int k_step_advance(StepState *st, int delta, void *stream) {
     step_advance<<<1, 1, 0, (cudaStream_t)stream>>>(st, delta);
+    return cerr();
+}
+
+int k_wave_energy(const GridDev &g, const WaveDev &w, double *out, void *stream) {
+    wave_energy<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(g, w, out);
     return cerr();
 }
 

@@ -162,6 +162,14 @@ jv_status jv_get_info(const jv_ctx *c, jv_info *info);
  * made -- after kernel_variant -1, the measured one. */
 jv_status jv_get_kernel_config(const jv_ctx *c, jv_options *out);
 
+/* Reconstruction check of the last jv_rtm_shot (FP64, on the GPU): the energy
+ * (sum of squares of the velocity and stress fields over gridphy) of the
+ * source wavefield at the end of the forward pass, and of what is left of it
+ * after the reverse loop has reconstructed it back to its zero initial
+ * state.  Their ratio measures the VOWR reconstruction error (exact time
+ * reversal at rec_width 4 up to FP32 rounding; an approximation below). */
+jv_status jv_reconstruction_energy(const jv_ctx *c, double *e_forward_end, double *e_residual);
+
 /* Forward modelling of one shot: replaces
  * fdtd3d_blend_elastic_model_mpi_module<pure_forward>::reset_for_next_shot
  * + mpi_sub_forward + SeisRecord::copy_seis_into_host
