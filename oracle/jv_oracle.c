@@ -674,6 +674,50 @@ static void ctx_free(ctx_t *c)
     free(c->rec_idx);
 }
 
+/* ------------------------------------------------------------------ */
+/* storage-precision study (jvo_set_store16; off by default)          */
+/* ------------------------------------------------------------------ */
+
+static int g_store16 = 0;
+
+void jvo_set_store16(int mode) { g_store16 = (mode == 1 || mode == 2) ? mode : 0; }
+
+/* x rounded to 16 bits: FP16 by the compiler's round-to-nearest-even
+ * conversion, BF16 by round-to-nearest-even on the upper half of the
+ * FP32 bit pattern */
+static inline float round16(float x)
+{
+    if (g_store16 == 1) return (float)(_Float16)x;
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+/* fields f0..f1 of w as 16-bit storage would hold them: per z plane of
+ * gridext a power-of-two scale s (FP16: largest magnitude / s in
+ * (2^11, 2^12]; BF16: in (1/2, 1]), values v -> s * round16(v / s) */
+static void store16(const grid_t *g, wave_t *w, int f0, int f1)
+{
+    if (!g_store16) return;
+    for (int f = f0; f <= f1; f++) {
+        real *a = w->f[f];
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < g->nz; k++) {
+            real *p = a + g->sz * (size_t)k;
+            double amax = 0;
+            for (size_t i = 0; i < g->sz; i++) amax = fmax(amax, fabs((double)p[i]));
+            if (amax == 0) continue;
+            int e;
+            frexp(amax, &e);
+            if (e < -100) e = -100;  /* keep 1/s finite for subnormal planes */
+            const float s = ldexpf(1.0f, g_store16 == 1 ? e - 12 : e), inv = 1.0f / s;
+            for (size_t i = 0; i < g->sz; i++) p[i] = (real)(s * round16((float)p[i] * inv));
+        }
+    }
+}
+
 static void add_source(wave_t *w, size_t s, real a)
 {
     /* sub_add_stress_source / sub_subtract_stress_source
@@ -691,10 +735,12 @@ static void step_forward(ctx_t *c, wave_t *w, int it, int mode, const box_t *bx,
 {
     vel_pml(&c->g, &c->cf, &c->md, w);
     vel_interior(&c->g, &c->cf, &c->md, w, mode, PHY_HALF, c->g.dt);
+    store16(&c->g, w, VX, VZ);
     add_source(w, c->src_idx, (real)c->wl[it]);
     stress_pml(&c->g, &c->cf, &c->md, w);
     if (store) box_copy(&c->g, w, bx, nb, store, 1, 0, 0);
     stress_interior(&c->g, &c->cf, &c->md, w, mode, PHY_HALF, c->g.dt);
+    store16(&c->g, w, SXX, SAU);
 }
 
 int jvo_forward(const jvo_problem *p, const float *vp, const float *vs, const float *rho, int shot,
@@ -828,19 +874,27 @@ static int rtm_core(const jvo_problem *p, const float *vp, const float *vs, cons
             R.f[VY][s] += (real)obs_vy[o];
             R.f[VZ][s] += (real)obs_vz[o];
         }
+        store16(&c.g, &R, VX, VZ);
         stress_interior(&c.g, &c.cf, &c.md, &F, M_BWD, w, -c.g.dt);
+        store16(&c.g, &F, SXX, SAU);
         vel_pml(&c.g, &c.cf, &c.md, &R);
         vel_interior(&c.g, &c.cf, &c.md, &R, M_REV, PHY_HALF, c.g.dt);
+        store16(&c.g, &R, VX, VZ);
+        store16(&c.g, &R, VXP, VZP);
         int sl = it - 1;
         int have = (sl >= 0 && sl <= nt - 2);
         /* a bounded sample keeps only nslice slots and cycles through them */
         real *slot = have ? store + per * (size_t)(nrun < nt ? sl % nslice : sl) : NULL;
         if (have) box_copy(&c.g, &F, bx, nb, slot, 0, 0, 1);
+        store16(&c.g, &F, SXX, SAU);
         /* UPDATE 2 */
         vel_interior(&c.g, &c.cf, &c.md, &F, M_BWD, w, -c.g.dt);
+        store16(&c.g, &F, VX, VZ);
         stress_pml(&c.g, &c.cf, &c.md, &R);
         stress_interior(&c.g, &c.cf, &c.md, &R, M_REV, PHY_HALF, c.g.dt);
+        store16(&c.g, &R, SXX, SAU);
         if (have) box_copy(&c.g, &F, bx, nb, slot, 0, 1, 0);
+        store16(&c.g, &F, VX, VZ);
         image_accumulate(&c.g, &F, &R, tip, tpp, tps, tsp, tss);
         if (snap && it == it_chk) *recon_err = rel_l2_vel(&c.g, &F, snap);
     }

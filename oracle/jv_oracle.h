@@ -107,6 +107,15 @@ void jvo_finalize_image(int nx, int ny, int nz, const double *ip,
 double jvo_rtm_sample(const jvo_problem *p, const float *vp, const float *vs,
                       const float *rho, int shot, int steps);
 
+/* Storage-precision study (not part of the reference's algorithm; default
+ * off): with mode 1 (FP16) or 2 (BF16) every later call rounds each stored
+ * wavefield component to 16 bits after every update that writes it, with
+ * one power-of-two FP32 scale per z plane of gridext (FP16: the plane's
+ * largest magnitude maps into (2^11, 2^12]); mode 0 restores plain
+ * storage.  Arithmetic stays JVO_REAL.  Used to measure what 16-bit
+ * wavefield storage would cost in trace and image error. */
+void jvo_set_store16(int mode);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,8 @@ def lib(precision: str = "f64") -> C.CDLL:
     L.jvo_finalize_image.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp]
     L.jvo_rtm_sample.argtypes = [P, fp, fp, fp, C.c_int, C.c_int]
     L.jvo_rtm_sample.restype = C.c_double
+    L.jvo_set_store16.argtypes = [C.c_int]
+    L.jvo_set_store16.restype = None
     _LIBS[precision] = L
     return L
 
@@ -198,6 +200,26 @@ def finalize_image(images: dict, nx: int, ny: int, nz: int):
     lib().jvo_finalize_image(nx, ny, nz, _d(comp["ip"]), _d(comp["pp"]), _d(comp["ps"]), _d(comp["sp"]),
                              _d(comp["ss"]), _d(lap["pp"]), _d(lap["ps"]), _d(lap["sp"]), _d(lap["ss"]))
     return comp, lap
+
+
+class store16:
+    """Context manager of the storage-precision study (jvo_set_store16):
+    inside it, the `precision` library rounds every stored wavefield
+    component to FP16 ("fp16") or BF16 ("bf16") after each update, with a
+    power-of-two scale per z plane; on exit storage is plain again.  The
+    setting is process-wide state of that library."""
+
+    def __init__(self, kind: str, precision: str = "f32"):
+        self.mode = {"f32": 0, "fp16": 1, "bf16": 2}[kind]
+        self.precision = precision
+
+    def __enter__(self):
+        lib(self.precision).jvo_set_store16(self.mode)
+        return self
+
+    def __exit__(self, *exc):
+        lib(self.precision).jvo_set_store16(0)
+        return False
 
 
 def rtm_sample(p: Problem, steps: int, shot: int = 0) -> float:

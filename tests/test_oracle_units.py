@@ -83,3 +83,28 @@ def test_rtm_reconstruction_w4_exact_order(oracle, synth):
         _, errs[w] = oracle.rtm_shot(p, tr, want_recon=True)
     assert errs[4] < 1e-9, errs
     assert errs[1] < 0.2 and errs[1] > errs[4]
+
+
+def test_store16_study_error(oracle, synth):
+    """16-bit wavefield storage, emulated on the oracle (FP32 arithmetic,
+    per-plane power-of-two scales), against plain FP32 storage: on a small
+    RTM shot FP32 storage stays within 1e-4 of the FP64 oracle, while FP16
+    and BF16 storage already exceed the 1e-3 image bound."""
+    s = synth.small_case(n=(20, 18, 16), pml=6, nt=120, seed=3)
+    p = oracle.Problem(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.dt, s.fm, s.T, 1, s.shots, s.recvs, s.vp,
+                       s.vs, s.rho)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+
+    def err(kind):
+        with oracle.store16(kind):
+            img = oracle.rtm_shot(p, obs, precision="f32")
+        return max(float(np.linalg.norm(img[k] - ref[k]) / np.linalg.norm(ref[k])) for k in ref)
+
+    e32, e16, eb16 = err("f32"), err("fp16"), err("bf16")
+    assert e32 <= 1e-4, e32
+    assert e16 > 1e-3, e16
+    assert eb16 > e16, (eb16, e16)
+    # the setting does not outlive the context
+    img = oracle.rtm_shot(p, obs, precision="f32")
+    assert max(float(np.linalg.norm(img[k] - ref[k]) / np.linalg.norm(ref[k])) for k in ref) <= 1e-4
