@@ -283,6 +283,80 @@ def serve_leg(jv, synth, n_req):
                     "warm-up requests on a server of their own are not counted"}
 
 
+def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
+    """The batched configuration, bounded in shots and steps.
+
+    (a) n_shots shots at seeded surface positions (depth 5 cells) on one
+    160^3 + 16 CPML model, nt steps: one jv_rtm_batch of all shots and one
+    finalize, against one jv_rtm_shot + finalize per shot.  Traces are
+    modelled first (not timed); host traces in, host images out.
+    (b) n_models independent seeded models with interior sizes drawn
+    uniformly from {80, 96, 120, 160, 200}^3 (+16 CPML), nt_mixed steps, one
+    RTM request each (modelling its own traces) through jv_server with 4
+    slots, against the same requests one at a time (1 slot)."""
+    import dataclasses
+    rng = np.random.default_rng(64)
+    base = synth.scaled_cfg2(160, nt, pml=16, seed=64)
+    pos = np.stack([rng.integers(8, 152, n_shots), rng.integers(8, 152, n_shots), np.full(n_shots, 5)], axis=1)
+    s = dataclasses.replace(base, shots=(pos * 5.0).astype(np.float32), name="shots_160")
+    out = {}
+    with jv.Context.from_survey(s, device=device) as ctx:
+        i = ctx.info()
+        obs = [ctx.forward(k) for k in range(n_shots)]
+        himg = torch.empty((8, s.nz, s.ny, s.nx), dtype=torch.float32, pin_memory=True)
+        hout = [himg[q].numpy() for q in range(8)]
+        ctx.rtm_shot(0, obs[0])  # warm-up: graph capture
+        ctx.finalize(out=hout)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(n_shots):
+            ctx.rtm_shot(k, obs[k])
+            ctx.finalize(out=hout)
+        torch.cuda.synchronize()
+        tp = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        ctx.rtm_batch(list(range(n_shots)), obs)
+        ctx.finalize(out=hout)
+        torch.cuda.synchronize()
+        tb = time.perf_counter() - t0
+        cells = nt * (2 * i.n_ext + i.n_phy)
+        out["shots_one_model"] = {
+            "grid_phy": [160, 160, 160], "pml": 16, "nt": nt, "shots": n_shots, "n_recv": i.n_recv,
+            "unit": "shots/h", "plain": round(n_shots / tp * 3600.0, 1), "batched": round(n_shots / tb * 3600.0, 1),
+            "gcell_updates_per_s": {"plain": round(n_shots * cells / tp / 1e9, 2),
+                                    "batched": round(n_shots * cells / tb / 1e9, 2)}}
+        del obs
+
+    sizes = [int(n) for n in rng.choice([80, 96, 120, 160, 200], n_models)]
+    models = [synth.scaled_cfg2(n, nt_mixed, pml=16, seed=200 + k) for k, n in enumerate(sizes)]
+    cells = sum(nt_mixed * (3 * m.n_ext) for m in models)  # own modelling + source and receiver propagations
+
+    def run(slots):
+        with jv.Server(slots=slots) as srv:
+            t0 = time.perf_counter()
+            subs = [srv.submit_survey(jv.JOB_RTM, m) for m in models]
+            for rid, _ in subs:
+                if srv.wait(rid, timeout=900.0) != 0:
+                    raise RuntimeError("mixed-batch request failed")
+            dt = time.perf_counter() - t0
+            st = srv.stats()
+        return dt, st
+
+    t1, st1 = run(1)
+    t4, st4 = run(4)
+    out["mixed_models"] = {
+        "models": n_models, "sizes": {str(n): sizes.count(n) for n in sorted(set(sizes))}, "pml": 16,
+        "nt": nt_mixed, "unit": "RTM shots/h", "slots1": round(n_models / t1 * 3600.0, 1),
+        "slots4": round(n_models / t4 * 3600.0, 1), "speedup": round(t1 / t4, 3),
+        "gcell_updates_per_s": {"slots1": round(cells / t1 / 1e9, 2), "slots4": round(cells / t4 / 1e9, 2)},
+        "p50_ms": {"slots1": round(st1["p50_ms"], 1), "slots4": round(st4["p50_ms"], 1)},
+        "p99_ms": {"slots1": round(st1["p99_ms"], 1), "slots4": round(st4["p99_ms"], 1)},
+        "note": "each request models its own traces, then migrates; all submitted at once; latency from "
+                "submission; the configured 64 shots / 48 models are cut in steps (and shots) to keep the bench "
+                "short"}
+    return out
+
+
 def extra_configs(jv, synth, torch, device):
     """The other configurations, one short measurement each (not the
     headline): cfg1 plain forward modelling in full, and the large cfg3
@@ -376,6 +450,11 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the request-server leg")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-extra", action="store_true", help="skip the cfg1 / cfg3 side measurements")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-configuration leg")
+    ap.add_argument("--batch-shots", type=int, default=8, help="shots of the one-model batch (160^3)")
+    ap.add_argument("--batch-nt", type=int, default=600, help="time steps of the one-model batch")
+    ap.add_argument("--mixed-models", type=int, default=48, help="models of the mixed batch")
+    ap.add_argument("--mixed-nt", type=int, default=200, help="time steps of each mixed-batch request")
     ap.add_argument("--ref-sample-steps", type=int, default=40)
     ap.add_argument("--variant", type=int, default=None, help="interior kernel variant (default: library default)")
     ap.add_argument("--store", default="fp32", choices=["fp32", "bf16", "fp16"],
@@ -538,6 +617,10 @@ def main():
     extra = None
     if world == 1 and not args.no_extra:
         extra = extra_configs(jv, jv.synth, torch, local)
+    batched_cfg = None
+    if world == 1 and not args.no_batched:
+        batched_cfg = batched_leg(jv, jv.synth, torch, local, args.batch_shots, args.batch_nt, args.mixed_models,
+                                  args.mixed_nt)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -577,6 +660,7 @@ def main():
                    "boundary_store": args.store,
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "serving": serving,
+        "batched_config": batched_cfg,
         "other_configs": extra, "clocks": clk,
         "gpu_launches": launches * args.steps if launches else None,
         "gpu_launches_note": "kernels of the timed shots, counted from one instrumented shot (graph path)",

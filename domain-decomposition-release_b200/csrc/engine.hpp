@@ -31,6 +31,11 @@ void ricker(int nt, float fm, float dt, float *w);
 // message returned by jv_last_error() on the calling thread
 void set_last_error(const std::string &m);
 
+// RTM of `shot` on traces the context models first (forward modelling of
+// the same shot); the traces stay in the context's device buffer (the
+// request server's RTM requests without observed traces)
+jv_status rtm_self_modelled(jv_ctx *c, int shot);
+
 // Pitched gridext layout of a gridphy + pml problem (elem = base + xoff +
 // i + sy*j + sz*k, first gridphy column 128-byte aligned); *field_elems =
 // floats of one field array (gridext plus tail slack for the aligned

@@ -157,6 +157,19 @@ static jv_status rtm_host(jv_ctx *c, int shot, const float *ox, const float *oy,
     return ret(c->eng->rtm_shot(shot, c->d_tr[0], c->d_tr[0] + per, c->d_tr[0] + 2 * per));
 }
 
+namespace jv {
+jv_status rtm_self_modelled(jv_ctx *c, int shot) {
+    JV_IDLE(c);
+    const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
+    jv_status st = ensure_traces(c, 3 * per);
+    if (st != JV_OK) return st;
+    float *d = c->d_tr[0];
+    st = ret(c->eng->forward(shot, d, d + per, d + 2 * per));
+    if (st != JV_OK) return st;
+    return ret(c->eng->rtm_shot(shot, d, d + per, d + 2 * per));
+}
+}  // namespace jv
+
 extern "C" {
 
 void jv_options_default(jv_options *o) {

@@ -88,17 +88,12 @@ jv_status run_request(int device, const jv_request &q) {
         if (q.kind == JV_JOB_FORWARD) {
             st = jv_forward(c, 0, q.out[0], q.out[1], q.out[2]);
         } else {
-            std::vector<float> tr;
-            const float *obs[3] = {q.obs[0], q.obs[1], q.obs[2]};
-            if (!obs[0] && !obs[1] && !obs[2]) {
-                jv_info inf;
-                jv_get_info(c, &inf);
-                const size_t per = (size_t)inf.n_recv * inf.nt;
-                tr.resize(3 * per);
-                st = jv_forward(c, 0, tr.data(), tr.data() + per, tr.data() + 2 * per);
-                for (int k = 0; k < 3; k++) obs[k] = tr.data() + k * per;
-            }
-            if (st == JV_OK) st = jv_rtm_shot(c, 0, obs[0], obs[1], obs[2]);
+            // without observed traces the request models its own, which
+            // stay on the device
+            if (!q.obs[0] && !q.obs[1] && !q.obs[2])
+                st = jv::rtm_self_modelled(c, 0);
+            else
+                st = jv_rtm_shot(c, 0, q.obs[0], q.obs[1], q.obs[2]);
             for (int k = 0; k < 5 && st == JV_OK; k++)
                 if (q.image[k]) st = jv_image_get(c, k, q.image[k]);
         }
