@@ -235,8 +235,8 @@ int upload_all_coefficients() {
 // VOWR face boxes (FD/fdtd3d_0_base_module/fdtd3d_base_5_wave_recon_meat.hpp:19-30;
 // face frames .jarvis_0_meta/.jarvis_3_operator/jarvis_1_mpicu_halo_store_operator_meat.hpp:129-134),
 // velocity fields first, with their offsets in the per-step record and their
-// first 256-cell block
-std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, long long *blocks) {
+// first 256-thread block
+std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, long long *blocks, bool vec) {
     const int W[10][6] = {
         {r - 1, r, r - 1, r, r, r - 1}, {r - 1, r, r, r - 1, r - 1, r}, {r, r - 1, r - 1, r, r - 1, r},
         {0, 0, 0, 0, r - 1, r},         {0, 0, r - 1, r, 0, 0},         {r - 1, r, 0, 0, 0, 0},
@@ -263,13 +263,17 @@ std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, 
             SegDev sg{};
             sg.fld = flds[f];
             sg.x0 = x0; sg.nxb = x1 - x0; sg.y0 = y0; sg.nyb = y1 - y0; sg.z0 = z0; sg.nzb = z1 - z0;
+            if (vec) off = (off + 3) / 4 * 4;  // 16-byte aligned box records
             sg.off = off;
             sg.nblk_first = blk;
+            // rows of whole 16-byte x groups: 4 values a thread
+            sg.vw = vec && sg.nxb % 4 == 0 && (g.xoff + x0) % 4 == 0 ? 4 : 1;
             long long cnt = (long long)sg.nxb * sg.nyb * sg.nzb;
             off += cnt;
-            blk += (cnt + 255) / 256;
+            blk += (cnt + 256LL * sg.vw - 1) / (256LL * sg.vw);
             segs.push_back(sg);
         }
+    if (vec) off = (off + 3) / 4 * 4;  // every step's record starts 16-byte aligned
     *per_step = off;
     *blocks = blk;
     return segs;
@@ -289,7 +293,7 @@ size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm) {
     b += 16 * ((size_t)grid.nx + grid.ny + grid.nz + 2 * grid.pml * 3) + (1 << 20);  // tables, state, slack
     if (rtm) {
         long long per = 0, blk = 0;
-        vowr_segments(g, rec_width, &per, &blk);
+        vowr_segments(g, rec_width, &per, &blk, true);  // the FP32 layout: the larger record
         b += (kNumFld * fe + 32) * sizeof(float) + (size_t)(psi + 2 * fz_psi_floats(g)) * sizeof(float);  // receiver wavefield
         b += (size_t)per * (size_t)(nt > 1 ? nt - 1 : 0) * sizeof(float);          // boundary store
         b += 5 * ((nphy + 63) / 64 * 64) * sizeof(float);                           // shot image
@@ -516,7 +520,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     // VOWR face boxes
     {
         long long off = 0, blk = 0;
-        segs_h_ = vowr_segments(g_, opt_.rec_width, &off, &blk);
+        segs_h_ = vowr_segments(g_, opt_.rec_width, &off, &blk, opt_.precision == JV_FP32);
         per_step_ = off;
         if (blk >= (1LL << 31) || per_step_ >= (1LL << 31)) return bad(JV_EINVAL, "boundary store too large");
         nslot_ = nt_ > 1 ? nt_ - 1 : 0;
@@ -529,7 +533,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         std::vector<int> blk_seg((size_t)blk);
         for (size_t q = 0; q < segs_h_.size(); q++) {
             const SegDev &S = segs_h_[q];
-            const long long nb = ((long long)S.nxb * S.nyb * S.nzb + 255) / 256;
+            const long long nb = ((long long)S.nxb * S.nyb * S.nzb + 256LL * S.vw - 1) / (256LL * S.vw);
             for (long long b = 0; b < nb; b++) blk_seg[(size_t)(S.nblk_first + b)] = (int)q;
             if (S.fld <= VZ) vowr_.vel_blocks = (int)(S.nblk_first + nb);
         }

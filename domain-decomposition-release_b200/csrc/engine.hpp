@@ -51,8 +51,10 @@ CpmlDev make_pml_slabs(const GridDev &g, int zp, long long *psi_total);
 // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_1_host_meat.hpp:147-620).
 void pml_axis_tables(const GridDev &g, float fm, std::vector<float4> t[3]);
 // VOWR face boxes of rec_width r for a layout, velocity fields first;
-// *per_step = floats of one step's record, *blocks = 256-cell blocks.
-std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, long long *blocks);
+// *per_step = values of one step's record, *blocks = 256-thread blocks.
+// With vec (the FP32 store) box offsets are rounded up to 4 values and a
+// box whose rows are 4-aligned whole x groups moves 4 values a thread.
+std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, long long *blocks, bool vec);
 // Device bytes a context of this problem holds after one forward (rtm false)
 // or RTM shot (rtm true), traces excluded.
 size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm);

@@ -83,11 +83,12 @@ struct SegDev {          // one VOWR face box
     int x0, nxb, y0, nyb, z0, nzb;
     long long off;       // offset in the packed per-step record
     long long nblk_first;
+    int vw;              // values a thread moves: 4 (16-byte accesses along x rows) or 1
 };
 
 // The VOWR boundary store and its face boxes.  Boxes of the velocity
-// fields come first; each box is cut into blocks of 256 cells and
-// blk_seg maps a block to its box.
+// fields come first; each box is cut into blocks of 256 threads of vw
+// cells each and blk_seg maps a block to its box.
 // boundary-store precision (the values of jv_precision)
 constexpr int kStoreF32 = 0, kStoreBF16 = 1, kStoreFP16 = 2;
 

@@ -2365,7 +2365,7 @@ __global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, VowrDev v, con
     if (slot < 0 || slot >= v.nslot) return;
     const int b = b0 + (int)blockIdx.x;
     const SegDev &S = v.segs[v.blk_seg[b]];
-    const int e = (b - (int)S.nblk_first) * 256 + (int)threadIdx.x;
+    const int e = ((b - (int)S.nblk_first) * 256 + (int)threadIdx.x) * S.vw;
     const int cnt = S.nxb * S.nyb * S.nzb;
     if (e >= cnt) return;
     const int t = e / S.nxb;
@@ -2374,8 +2374,15 @@ __global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, VowrDev v, con
     const int y = S.y0 + (t - z * S.nyb);
     const int i = (int)g.xoff + x + (int)g.sy * y + (int)g.sz * (S.z0 + z);
     float *rec = v.store + (long long)slot * v.per_step + S.off + e;
-    if (pack) *rec = w.f[S.fld][i];
-    else w.f[S.fld][i] = *rec;
+    if (S.vw == 4) {  // 4 values of one row; record and field both 16-byte aligned (vowr_segments)
+        float4 *f4 = reinterpret_cast<float4 *>(w.f[S.fld] + i), *r4 = reinterpret_cast<float4 *>(rec);
+        if (pack) *r4 = *f4;
+        else *f4 = *r4;
+    } else if (pack) {
+        *rec = w.f[S.fld][i];
+    } else {
+        w.f[S.fld][i] = *rec;
+    }
 }
 
 // 16-bit boundary store.  Pass 1: each box's largest magnitude in this
