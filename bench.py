@@ -288,8 +288,10 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
 
     (a) n_shots shots at seeded surface positions (depth 5 cells) on one
     160^3 + 16 CPML model, nt steps: one jv_rtm_batch of all shots and one
-    finalize, against one jv_rtm_shot + finalize per shot.  Traces are
-    modelled first (not timed); host traces in, host images out.
+    finalize, against one jv_rtm_shot + finalize per shot.  The context
+    makes the measured kernel choice (kernel_variant -1: variant and run
+    chunking) when it is created.  Traces are modelled first (not timed);
+    host traces in, host images out.
     (b) n_models independent seeded models with interior sizes drawn
     uniformly from {80, 96, 120, 160, 200}^3 (+16 CPML), nt_mixed steps, one
     RTM request each (modelling its own traces) through jv_server with 4
@@ -300,8 +302,9 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
     pos = np.stack([rng.integers(8, 152, n_shots), rng.integers(8, 152, n_shots), np.full(n_shots, 5)], axis=1)
     s = dataclasses.replace(base, shots=(pos * 5.0).astype(np.float32), name="shots_160")
     out = {}
-    with jv.Context.from_survey(s, device=device) as ctx:
+    with jv.Context.from_survey(s, device=device, kernel_variant=-1) as ctx:
         i = ctx.info()
+        kcfg = ctx.kernel_config()
         obs = [ctx.forward(k) for k in range(n_shots)]
         himg = torch.empty((8, s.nz, s.ny, s.nx), dtype=torch.float32, pin_memory=True)
         hout = [himg[q].numpy() for q in range(8)]
@@ -322,6 +325,7 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
         cells = nt * (2 * i.n_ext + i.n_phy)
         out["shots_one_model"] = {
             "grid_phy": [160, 160, 160], "pml": 16, "nt": nt, "shots": n_shots, "n_recv": i.n_recv,
+            "kernel_choice": {"kernel_variant": kcfg["kernel_variant"], "run_chunks": kcfg["run_chunks"]},
             "unit": "shots/h", "plain": round(n_shots / tp * 3600.0, 1), "batched": round(n_shots / tb * 3600.0, 1),
             "gcell_updates_per_s": {"plain": round(n_shots * cells / tp / 1e9, 2),
                                     "batched": round(n_shots * cells / tb / 1e9, 2)}}

@@ -351,6 +351,7 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.pml_min_blocks) E->kc_.pml_minb = opt.pml_min_blocks;
     if (opt.planes_per_thread) E->kc_.zp = opt.planes_per_thread;
     if (opt.pml_planes_per_thread) E->kc_.pml_zp = opt.pml_planes_per_thread;
+    if (opt.run_chunks > 0) E->kc_.fzq = opt.run_chunks;
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
@@ -365,13 +366,14 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
 
 // The measured kernel choice (kernel_variant -1): a few forward-modelling
 // steps of each candidate on this grid -- variant 4 where its kernels
-// apply, variant 3 where its stress kernel applies, variant 2 -- and, for
-// the variants with separate absorbing-layer kernels, their register
+// apply, with the cost model's three best run chunkings (unless run_chunks
+// fixes one), variant 3 where its stress kernel applies, variant 2 -- and,
+// for the variants with separate absorbing-layer kernels, their register
 // budget (3 or 4 blocks per SM).  The fastest wins; the choice is kept per
 // grid shape and device for the contexts that follow.
 Status Engine::autotune() {
     struct Cand {
-        int variant, pml_minb;
+        int variant, pml_minb, q;  // q: variant 4's run chunks
     };
     static std::mutex mu;
     static std::map<std::array<long long, 6>, Cand> cache;
@@ -381,9 +383,15 @@ Status Engine::autotune() {
     JV_CU(cudaGetDeviceProperties(&prop, dev));
     const std::array<long long, 6> key = {grid_.nx, grid_.ny, grid_.nz, grid_.pml, prop.multiProcessorCount,
                                           (long long)prop.totalGlobalMem};
+    Status st{};
     auto apply = [&](const Cand &c) {
         kc_.variant = c.variant;
         kc_.pml_minb = c.pml_minb;
+        if (c.variant == 4 && fullF_.ok && c.q > 0 && c.q != fullF_.geo.Q) {
+            kc_.fzq = c.q;
+            const int e = k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_);
+            if (e != 0 || !fullF_.ok) st = bad(JV_ECUDA, "variant-4 descriptors for the measured choice");
+        }
         use_full_ = c.variant == 4 && fullF_.ok;
         vel_full_ = use_full_ && fullF_.geo.NTX == 1;
     };
@@ -392,17 +400,24 @@ Status Engine::autotune() {
         auto it = cache.find(key);
         if (it != cache.end()) {
             apply(it->second);
-            return Status{};
+            return st;
         }
     }
     std::vector<Cand> cands;
-    if (fullF_.ok) cands.push_back({4, 4});
-    if (mapsF_.ok) {
-        cands.push_back({3, 4});
-        cands.push_back({3, 3});
+    if (fullF_.ok) {
+        if (kc_.fzq > 0) {
+            cands.push_back({4, 4, fullF_.geo.Q});
+        } else {
+            for (int k = 0; k < 3; k++)
+                if (fullF_.qcand[k] > 0) cands.push_back({4, 4, fullF_.qcand[k]});
+        }
     }
-    cands.push_back({2, 4});
-    cands.push_back({2, 3});
+    if (mapsF_.ok) {
+        cands.push_back({3, 4, 0});
+        cands.push_back({3, 3, 0});
+    }
+    cands.push_back({2, 4, 0});
+    cands.push_back({2, 3, 0});
     const long long src = (long long)g_.xoff + (g_.m + g_.px / 2) + g_.sy * (g_.m + g_.py / 2) +
                           g_.sz * (g_.m + g_.pz / 2);
     float best = -1.f;
@@ -410,6 +425,7 @@ Status Engine::autotune() {
     const int warm = 2, steps = 6;
     for (const Cand &c : cands) {
         apply(c);
+        JV_TRY(st);
         JV_TRY(zero_wave(F_, 9));
         JV_TRY(zero_psi(cpF_));
         JV_TRY(set_state(0, src, nullptr, nullptr));
@@ -427,6 +443,7 @@ Status Engine::autotune() {
         }
     }
     apply(pick);
+    JV_TRY(st);
     JV_TRY(zero_wave(F_, 9));
     JV_TRY(zero_psi(cpF_));
     JV_CU(cudaStreamSynchronize(stream_));
@@ -495,7 +512,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         fz_psi_total_ = 2 * fz_psi_floats(g_);  // velocity and stress sets
         JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
         fzpsiF_ = (float *)p;
-        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, &fullF_));
+        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_));
         // the fused velocity update runs on one-tile grids, where it measured
         // faster than the split kernels; x-tiled grids keep the split ones
         use_full_ = fullF_.ok;
@@ -906,7 +923,7 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
         if (kc_.variant == 4) {
             JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
             fzpsiR_ = (float *)p;
-            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, rho_, axis_d_, fzpsiR_, zm_err_, &fullR_));
+            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, rho_, axis_d_, fzpsiR_, zm_err_, kc_.fzq, &fullR_));
         }
     }
     if (!shot_img_.ip) {

@@ -118,6 +118,7 @@ class Engine {
         o->pml_min_blocks = kc_.pml_minb;
         o->planes_per_thread = kc_.zp;
         o->pml_planes_per_thread = kc_.pml_zp;
+        o->run_chunks = use_full_ ? fullF_.geo.Q : 0;
     }
 
   private:

@@ -190,6 +190,7 @@ struct FullMaps {
     int grid = 0;
     size_t smem = 0, vsmem = 0;
     int *err = nullptr;
+    int qcand[3] = {0, 0, 0};     // the cost model's three best run-chunk counts, best first
 };
 
 // interior-kernel choice: variant 0 = one z plane per block, 1 = z-marching
@@ -202,6 +203,7 @@ struct KCfg {
     int pml_minb = 4;    // CPML kernels: the same
     int zp = 1;          // variant 2: z planes per thread (1 or 2)
     int pml_zp = 1;      // CPML kernels: the same
+    int fzq = 0;         // variant 4: run chunks per tile (0: the cost model's choice)
 };
 
 // kernels.cu ------------------------------------------------------------
@@ -221,12 +223,15 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
 // or the driver entry point missing).  Returns a cudaError_t.
 int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
                      WaveMaps *maps);
-// The descriptors of the full-gridext stress kernel (variant 4); maps->ok
+// The descriptors of the full-gridext stress kernel (variant 4), with the
+// run schedule cut into `chunks` chunks per tile (0: the cost model's
+// choice; maps->qcand lists its three best); maps->ok
 // stays false when the grid does not suit it (odd pml_num or nx, a tile
 // row of more than 512 threads or a halo row wider than 256 floats, the
 // driver entry point missing).  Returns a cudaError_t.
 int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
-                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps);
+                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, int chunks,
+                     FullMaps *maps);
 // Stress update of every updated cell of gridext, interior and absorbing
 // layers in one launch (modes kFwd, kRtmFwd, kRev).
 int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const float *wavelet, const StepState *st,

@@ -2734,7 +2734,8 @@ long long fz_psi_floats(const GridDev &g) {
 }
 
 int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
-                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, FullMaps *maps) {
+                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, int chunks,
+                     FullMaps *maps) {
     maps->ok = false;
     const int m = g.m, xoff = (int)g.xoff;
     if ((m & 1) || (g.px & 1) || !psi) return 0;
@@ -2778,19 +2779,30 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     const size_t vsmem = (size_t)2 * fv_stage(geo) * sizeof(float);
     if (vsmem + 1024 > (size_t)smem_max) return 0;
     // runs: the chunking with the shortest longest-CTA time (a run's first
-    // plane costs about a window refill more)
-    long long best = -1;
+    // plane costs about a window refill more); the three cheapest are kept
+    // as the candidates of the measured choice
+    long long qc[3] = {-1, -1, -1};
+    int qn[3] = {0, 0, 0};
     for (int Q = 1; Q <= 64 && Q <= geo.nzi; Q++) {
         const int L = (geo.nzi + Q - 1) / Q, R = geo.NTX * geo.ytiles * Q;
         const int G = std::min(nsm, R);
         const long long cost = (long long)((R + G - 1) / G) * (L + 6);
-        if (best < 0 || cost < best) {
-            best = cost;
-            geo.Q = Q;
-            geo.L = L;
-            geo.R = R;
+        for (int k = 0; k < 3; k++) {
+            if (qc[k] < 0 || cost < qc[k]) {
+                for (int j = 2; j > k; j--) {
+                    qc[j] = qc[j - 1];
+                    qn[j] = qn[j - 1];
+                }
+                qc[k] = cost;
+                qn[k] = Q;
+                break;
+            }
         }
     }
+    const int Q = chunks >= 1 && chunks <= geo.nzi ? chunks : qn[0];
+    geo.Q = Q;
+    geo.L = (geo.nzi + Q - 1) / Q;
+    geo.R = geo.NTX * geo.ytiles * Q;
     for (int a = 0; a < 3; a++) geo.ax[a] = ax[a];
     FzGeo vgeo = geo;
     // memory variables: the velocity set, then the stress set
@@ -2880,6 +2892,7 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     maps->smem = smem;
     maps->vsmem = vsmem;
     maps->err = err_flag;
+    for (int k = 0; k < 3; k++) maps->qcand[k] = qn[k];
     maps->ok = true;
     return 0;
 }

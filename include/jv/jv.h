@@ -95,6 +95,10 @@ typedef struct jv_options {
     int pml_min_blocks; /* absorbing-layer kernels: the same (0 -> 4)            */
     int planes_per_thread;     /* variant 2: z planes a thread updates, 1 or 2 (0 -> 1) */
     int pml_planes_per_thread; /* absorbing-layer kernels: the same (0 -> 1)      */
+    int run_chunks;     /* variant 4: chunks each tile's planes are cut into for the
+                           persistent kernels' run schedule (0 -> the cost model's
+                           choice; with kernel_variant -1 the measured choice among the
+                           cost model's three best); jv_get_kernel_config reports it */
 } jv_options;
 
 /* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,

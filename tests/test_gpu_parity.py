@@ -374,13 +374,37 @@ def test_measured_kernel_choice(oracle, synth):
         with jv.Context.from_survey(s, kernel_variant=-1) as ctx:
             cfg = ctx.kernel_config()
             tr = ctx.forward(0)
-        picks.append((cfg["kernel_variant"], cfg["pml_min_blocks"]))
+        picks.append((cfg["kernel_variant"], cfg["pml_min_blocks"], cfg["run_chunks"]))
         assert cfg["kernel_variant"] in (2, 3, 4) and cfg["pml_min_blocks"] in (3, 4)
+        assert (cfg["run_chunks"] > 0) == (cfg["kernel_variant"] == 4)
         for a, b in zip(tr, ref):
             assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
     assert picks[0] == picks[1], picks  # the second context reuses the first one's choice
     with jv.Context.from_survey(s) as ctx:
         assert ctx.kernel_config()["kernel_variant"] == 4
+
+
+@pytest.mark.parametrize("chunks", [1, 3, 7, 40])
+def test_run_chunks_change_no_result(synth, chunks):
+    """The run schedule of the persistent TMA kernels (run_chunks: chunks
+    of each tile's planes) only decides which CTA updates which cells, so
+    traces and images are bit-identical to the cost model's schedule; the
+    chunking in use is reported (a count past the planes falls back to the
+    cost model's)."""
+    s = synth.small_case(n=(24, 20, 18), pml=6, nt=60, seed=3)
+    out = {}
+    for q in (0, chunks):
+        with jv.Context.from_survey(s, run_chunks=q) as ctx:
+            cfg = ctx.kernel_config()
+            tr = ctx.forward(0)
+            ctx.rtm_shot(0, tr)
+            out[q] = (tr, ctx.images(), cfg["run_chunks"])
+    nzi = s.nz + 2 * s.pml - 4
+    assert out[chunks][2] == (chunks if chunks <= nzi else out[0][2]), (out[chunks][2], out[0][2])
+    for a, b in zip(out[0][0], out[chunks][0]):
+        assert np.array_equal(a, b)
+    for k in out[0][1]:
+        assert np.array_equal(out[0][1][k], out[chunks][1][k]), k
 
 
 @pytest.mark.parametrize("variant", [4, 2])
