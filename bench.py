@@ -364,7 +364,9 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
 def extra_configs(jv, synth, torch, device):
     """The other configurations, one short measurement each (not the
     headline): cfg1 plain forward modelling in full, and the large cfg3
-    grid's RTM shot with the FP16 boundary store, cut to a few time steps."""
+    grid's RTM shot with the FP16 boundary store, cut to a few time steps,
+    with the measured kernel choice (kernel_variant -1, made when the
+    context is created)."""
     out = {}
     s = synth.cfg1()
     with jv.Context.from_survey(s, device=device) as ctx:
@@ -382,8 +384,9 @@ def extra_configs(jv, synth, torch, device):
                                "gcell_updates_per_s": round(i.n_ext * s.nt / t / 1e9, 2)}
     nt3 = 40
     s = synth.cfg3(nt=nt3)
-    with jv.Context.from_survey(s, device=device, precision=jv.JV_FP16) as ctx:
+    with jv.Context.from_survey(s, device=device, precision=jv.JV_FP16, kernel_variant=-1) as ctx:
         i = ctx.info()
+        kcfg = ctx.kernel_config()
         tr = torch.empty((3, i.n_recv, i.nt), dtype=torch.float32, device=f"cuda:{device}")
         ptrs = [tr[q].data_ptr() for q in range(3)]
         ctx.forward_device(0, ptrs)
@@ -396,6 +399,7 @@ def extra_configs(jv, synth, torch, device):
             "ms_per_step": round(1000 * t / nt3, 3), "gcell_updates_per_s": round(cells / t / 1e9, 2),
             "shot_s_at_3000_steps": round(t / nt3 * 3000, 1),
             "store_bytes_per_step": int(i.store_bytes_per_step), "device_bytes": int(i.device_bytes),
+            "kernel_choice": {k: kcfg[k] for k in ("kernel_variant", "run_chunks", "tile_gx", "pml_min_blocks")},
             "note": "the configured 3000 steps cut to 40 to keep the bench short; per-step cost is constant"}
         del tr
     return out

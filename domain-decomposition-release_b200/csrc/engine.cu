@@ -369,12 +369,18 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
 // apply, with the cost model's three best run chunkings (unless run_chunks
 // fixes one), variant 3 where its stress kernel applies, variant 2 -- and,
 // for the variants with separate absorbing-layer kernels, their register
-// budget (3 or 4 blocks per SM).  The fastest wins; the choice is kept per
-// grid shape and device for the contexts that follow.
+// budget (3 or 4 blocks per SM).  Then, unless tile_gx / tile_gy were
+// given, the float4 kernels' block shape: the default number of blocks per
+// gridphy row and one fewer or one more, timed on the reverse loop's
+// float4 velocity update and the backward stress update (the forward step
+// of a one-tile grid does not run them).  The fastest wins; the choice is
+// kept per grid shape and device for the contexts that follow.
 Status Engine::autotune() {
     struct Cand {
         int variant, pml_minb, q;  // q: variant 4's run chunks
+        int gx = 0;                // float4 kernels' x groups per block (0: the default shape)
     };
+    const bool shape_free = opt_.tile_gx <= 0 && opt_.tile_gy <= 0;
     static std::mutex mu;
     static std::map<std::array<long long, 6>, Cand> cache;
     int dev = 0;
@@ -387,6 +393,10 @@ Status Engine::autotune() {
     auto apply = [&](const Cand &c) {
         kc_.variant = c.variant;
         kc_.pml_minb = c.pml_minb;
+        if (shape_free) {
+            kc_.gx = c.gx;
+            kc_.gy = 0;
+        }
         if (c.variant == 4 && fullF_.ok && c.q > 0 && c.q != fullF_.geo.Q) {
             kc_.fzq = c.q;
             const int e = k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_);
@@ -444,7 +454,35 @@ Status Engine::autotune() {
     }
     apply(pick);
     JV_TRY(st);
-    JV_TRY(zero_wave(F_, 9));
+    if (shape_free) {
+        const int ngx = (g_.px + 3) / 4, nb0 = (ngx + 63) / 64;
+        float sbest = -1.f;
+        for (int nb = std::max(1, nb0 - 1); nb <= nb0 + 1; nb++) {
+            const int gx = (ngx + nb - 1) / nb;
+            if (gx > 256) continue;
+            kc_.gx = nb == nb0 ? 0 : gx;
+            kc_.gy = 0;
+            JV_TRY(zero_wave(F_, kNumFld));
+            JV_TRY(set_state(0, src, nullptr, nullptr));
+            for (int i = 0; i < warm + steps; i++) {
+                if (i == warm) JV_CU(cudaEventRecord(ev0_, stream_));
+                JV_K(k_vel_phy(kRev, g_, F_, rho_, dt_, opt_.rec_width, nullptr, nullptr, kc_, stream_));
+                JV_K(k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt_, opt_.rec_width, wavelet_, st_, 0, kc_, stream_,
+                                  &mapsF_));
+            }
+            JV_CU(cudaEventRecord(ev1_, stream_));
+            JV_CU(cudaEventSynchronize(ev1_));
+            JV_TRY(check_zm_err());
+            float ms = 0.f;
+            JV_CU(cudaEventElapsedTime(&ms, ev0_, ev1_));
+            if (sbest < 0.f || ms < sbest) {
+                sbest = ms;
+                pick.gx = kc_.gx;
+            }
+        }
+        apply(pick);
+    }
+    JV_TRY(zero_wave(F_, kNumFld));
     JV_TRY(zero_psi(cpF_));
     JV_CU(cudaStreamSynchronize(stream_));
     std::lock_guard<std::mutex> l(mu);

@@ -119,6 +119,8 @@ class Engine {
         o->planes_per_thread = kc_.zp;
         o->pml_planes_per_thread = kc_.pml_zp;
         o->run_chunks = use_full_ ? fullF_.geo.Q : 0;
+        o->tile_gx = kc_.gx;
+        o->tile_gy = kc_.gy;
     }
 
   private:

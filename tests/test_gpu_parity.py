@@ -377,6 +377,8 @@ def test_measured_kernel_choice(oracle, synth):
         picks.append((cfg["kernel_variant"], cfg["pml_min_blocks"], cfg["run_chunks"]))
         assert cfg["kernel_variant"] in (2, 3, 4) and cfg["pml_min_blocks"] in (3, 4)
         assert (cfg["run_chunks"] > 0) == (cfg["kernel_variant"] == 4)
+        # the float4 kernels' block shape: the default (0) or one more or one fewer block per row
+        assert cfg["tile_gx"] in (0, 5, 10) and cfg["tile_gy"] == 0, (cfg["tile_gx"], cfg["tile_gy"])
         for a, b in zip(tr, ref):
             assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
     assert picks[0] == picks[1], picks  # the second context reuses the first one's choice
