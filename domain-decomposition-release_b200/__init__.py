@@ -83,7 +83,8 @@ class Request(C.Structure):
                 ("rho", C.POINTER(C.c_float)), ("dt", C.c_float), ("fm", C.c_float), ("nt", C.c_int),
                 ("rec_width", C.c_int), ("shot_xyz", C.c_float * 3), ("n_recv", C.c_int),
                 ("recv_xyz", C.POINTER(C.c_float)), ("obs", C.POINTER(C.c_float) * 3),
-                ("out", C.POINTER(C.c_float) * 3), ("image", C.POINTER(C.c_double) * 5)]
+                ("out", C.POINTER(C.c_float) * 3), ("image", C.POINTER(C.c_double) * 5),
+                ("precision", C.c_int)]
 
 
 class ServerStats(C.Structure):
@@ -463,13 +464,15 @@ class Server:
         self._refs = {}
 
     def submit(self, kind, nx, ny, nz, pml, dx, dy, dz, vp, vs, rho, dt, fm, nt, shot_xyz, recv_xyz,
-               rec_width=1, obs=None, out=None, image=None) -> int:
+               rec_width=1, obs=None, out=None, image=None, precision=JV_FP32) -> int:
         """Queues one request.  out (FORWARD) / obs (RTM) are 3 float32
         arrays [n_kept][nt]; image (RTM) up to 5 float64 arrays of gridphy
-        (ip, pp, ps, sp, ss; None skips one).  The arrays are kept alive here
+        (ip, pp, ps, sp, ss; None skips one); precision: the RTM boundary
+        store's (JV_FP32, JV_BF16, JV_FP16).  The arrays are kept alive here
         until the request has been waited for."""
         r = Request()
         r.kind = kind
+        r.precision = precision
         r.grid = Grid(nx, ny, nz, pml, dx, dy, dz)
         refs = []
 
@@ -506,7 +509,7 @@ class Server:
         self._refs[rid.value] = refs
         return rid.value
 
-    def submit_survey(self, kind, s, shot: int = 0, obs=None):
+    def submit_survey(self, kind, s, shot: int = 0, obs=None, precision=JV_FP32):
         """Queues shot `shot` of a synth.Survey-like object; returns (id,
         outputs): the three trace arrays [n_recv][nt] of a FORWARD request,
         or the five image arrays (ip, pp, ps, sp, ss; gridphy, float64) of an
@@ -519,7 +522,7 @@ class Server:
         else:
             outs = tuple(np.zeros((s.nz, s.ny, s.nx), np.float64) for _ in range(5))
             rid = self.submit(kind, s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt,
-                              s.shots[shot], rv, rec_width=s.rec_width, obs=obs, image=outs)
+                              s.shots[shot], rv, rec_width=s.rec_width, obs=obs, image=outs, precision=precision)
         return rid, outs
 
     def poll(self, rid: int):

@@ -279,7 +279,7 @@ std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, 
     return segs;
 }
 
-size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm) {
+size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm, int precision) {
     size_t fe = 0;
     const GridDev g = make_layout(grid, &fe);
     long long psi = 0;
@@ -293,9 +293,12 @@ size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm) {
     b += 16 * ((size_t)grid.nx + grid.ny + grid.nz + 2 * grid.pml * 3) + (1 << 20);  // tables, state, slack
     if (rtm) {
         long long per = 0, blk = 0;
-        vowr_segments(g, rec_width, &per, &blk, true);  // the FP32 layout: the larger record
+        const bool s16 = precision == JV_BF16 || precision == JV_FP16;
+        const std::vector<SegDev> segs = vowr_segments(g, rec_width, &per, &blk, !s16);
+        const size_t nslot = nt > 1 ? nt - 1 : 0;
         b += (kNumFld * fe + 32) * sizeof(float) + (size_t)(psi + 2 * fz_psi_floats(g)) * sizeof(float);  // receiver wavefield
-        b += (size_t)per * (size_t)(nt > 1 ? nt - 1 : 0) * sizeof(float);          // boundary store
+        b += (size_t)per * nslot * (s16 ? sizeof(uint16_t) : sizeof(float));      // boundary store
+        if (s16) b += (nslot + 2) * segs.size() * sizeof(float);                    // its per-box scales
         b += 5 * ((nphy + 63) / 64 * 64) * sizeof(float);                           // shot image
         b += (size_t)blk * sizeof(int) + 64 * sizeof(SegDev);
     }

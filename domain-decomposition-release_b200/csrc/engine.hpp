@@ -56,8 +56,9 @@ void pml_axis_tables(const GridDev &g, float fm, std::vector<float4> t[3]);
 // box whose rows are 4-aligned whole x groups moves 4 values a thread.
 std::vector<SegDev> vowr_segments(const GridDev &g, int r, long long *per_step, long long *blocks, bool vec);
 // Device bytes a context of this problem holds after one forward (rtm false)
-// or RTM shot (rtm true), traces excluded.
-size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm);
+// or RTM shot (rtm true) with a boundary store of `precision`
+// (jv_precision), traces excluded.
+size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm, int precision);
 // Uploads the staggered coefficient rows of every order and the 4th-order
 // CPML pair to constant memory of the current device.
 int upload_all_coefficients();

@@ -80,6 +80,7 @@ jv_status run_request(int device, const jv_request &q) {
     jv_options_default(&o);
     o.device = device;
     o.rec_width = q.rec_width > 0 ? q.rec_width : 1;
+    o.precision = q.precision;
     jv_ctx *c = nullptr;
     jv_status st = jv_create(&q.grid, q.vp, q.vs, q.rho, q.dt, q.fm, q.nt, &o, &c);
     if (st != JV_OK) return st;
@@ -175,7 +176,7 @@ jv_status jv_footprint(const jv_grid *grid, int nt, int rec_width, int kind, int
     if (grid->nx < 8 || grid->ny < 8 || grid->nz < 8 || grid->pml < 4 || nt < 1 || n_recv < 0)
         return fail(JV_EINVAL, "jv_footprint: bad problem");
     // the context's trace buffer: three components of every receiver
-    *bytes = jv::footprint_bytes(*grid, nt, rec_width > 0 ? rec_width : 1, kind == JV_JOB_RTM) +
+    *bytes = jv::footprint_bytes(*grid, nt, rec_width > 0 ? rec_width : 1, kind == JV_JOB_RTM, JV_FP32) +
              3 * (size_t)n_recv * (size_t)nt * sizeof(float);
     jv::set_last_error("");
     return JV_OK;
@@ -216,9 +217,16 @@ jv_status jv_server_submit(jv_server *s, const jv_request *r, long long *id) {
     if (r->kind != JV_JOB_FORWARD && r->kind != JV_JOB_RTM) return fail(JV_EINVAL, "unknown request kind");
     if (!r->vp || !r->vs || !r->rho || (r->n_recv > 0 && !r->recv_xyz) || r->n_recv < 0)
         return fail(JV_EINVAL, "request model or receivers missing");
+    if (r->precision != JV_FP32 && r->precision != JV_BF16 && r->precision != JV_FP16)
+        return fail(JV_EINVAL, "request precision must be JV_FP32, JV_BF16 or JV_FP16");
     size_t bytes = 0;
     jv_status st = jv_footprint(&r->grid, r->nt, r->rec_width, r->kind, r->n_recv, &bytes);
     if (st != JV_OK) return st;
+    if (r->precision != JV_FP32)  // a 16-bit store: the footprint with 2-byte records
+        bytes = bytes - jv::footprint_bytes(r->grid, r->nt, r->rec_width > 0 ? r->rec_width : 1,
+                                            r->kind == JV_JOB_RTM, JV_FP32) +
+                jv::footprint_bytes(r->grid, r->nt, r->rec_width > 0 ? r->rec_width : 1, r->kind == JV_JOB_RTM,
+                                    r->precision);
     std::lock_guard<std::mutex> l(s->mu);
     if (bytes > s->budget)
         return fail(JV_ENOMEM, "request needs about " + std::to_string(bytes >> 20) + " MiB, the server's budget is " +

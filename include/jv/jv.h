@@ -85,8 +85,9 @@ typedef struct jv_options {
                            3 as 2 with a TMA-fed z-marching stress update, 4 (default) as 3
                            with the absorbing layers' stress update in the same TMA kernel
                            (even pml_num and nx; other grids run variant 3's kernels);
-                           -1: measured choice among 4, 3, 2 (and the absorbing-layer
-                           register budget) on this grid at creation, kept per grid shape;
+                           -1: measured choice among 4, 3, 2, variant 4's run chunking,
+                           the absorbing-layer register budget and the float4 kernels'
+                           block shape on this grid at creation, kept per grid shape;
                            jv_get_kernel_config reports it */
     int zchunk;         /* z planes per block for variant 1 (0 -> auto)          */
     int tile_gx;        /* variant 2: 4-cell x groups per block (0 -> auto)      */
@@ -314,6 +315,9 @@ typedef struct jv_request {
     float *out[3];              /* FORWARD: traces [n_kept][nt] (NULL skips one)     */
     double *image[5];           /* RTM: this shot's FP64 stacks ip, pp, ps, sp, ss
                                    (gridphy, NULL skips one)                         */
+    int precision;              /* RTM boundary store: JV_FP32 (0), JV_BF16, JV_FP16; a
+                                   16-bit store halves the store's share of the
+                                   footprint the server admits the request by         */
 } jv_request;
 typedef struct jv_server jv_server;
 typedef struct jv_server_stats {
@@ -322,7 +326,9 @@ typedef struct jv_server_stats {
     size_t bytes_in_use, budget;
 } jv_server_stats;
 /* Device bytes a context holds for one request of this size with n_recv
- * receivers (an estimate from the layout; the server's admission unit). */
+ * receivers and an FP32 boundary store (an estimate from the layout; the
+ * server's admission unit, which counts 2-byte records for a request with a
+ * 16-bit store). */
 jv_status jv_footprint(const jv_grid *grid, int nt, int rec_width, int kind, int n_recv, size_t *bytes);
 /* hbm_budget 0: 90 % of the device's free memory now. */
 jv_status jv_server_create(int device, int slots, size_t hbm_budget, jv_server **out);

@@ -23,8 +23,8 @@ def _cases():
             synth.small_case(n=(20, 18, 24), pml=5, nt=90, seed=13, shot_idx=[(9, 9, 4)], nrec=25)]
 
 
-def _alone(s, kind, obs=None):
-    with jv.Context.from_survey(s) as ctx:
+def _alone(s, kind, obs=None, precision=jv.JV_FP32):
+    with jv.Context.from_survey(s, precision=precision) as ctx:
         if kind == jv.JOB_FORWARD:
             return ctx.forward(0)
         if obs is None:
@@ -61,6 +61,26 @@ def test_mixed_requests_match_each_run_alone():
     assert st["submitted"] == 6 and st["completed"] == 6 and st["failed"] == 0
     assert st["running"] == 0 and st["queued"] == 0 and st["bytes_in_use"] == 0
     assert 0 < st["p50_ms"] <= st["p99_ms"] and st["mean_ms"] > 0
+
+
+@pytest.mark.parametrize("precision", [jv.JV_FP16, jv.JV_BF16])
+def test_request_boundary_store_precision(precision):
+    """A request's own boundary-store precision reaches its context: a
+    16-bit-store request next to an FP32 one gives the images of a context
+    with that store, and they differ from the FP32 store's (the replayed rim
+    is rounded), within the 16-bit store's image error."""
+    cases = _cases()
+    w16 = _alone(cases[0], jv.JOB_RTM, precision=precision)
+    w32 = _alone(cases[0], jv.JOB_RTM)
+    with jv.Server(slots=2, budget=1 << 30) as srv:
+        a = srv.submit_survey(jv.JOB_RTM, cases[0], precision=precision)
+        b = srv.submit_survey(jv.JOB_RTM, cases[0])
+        for rid, _ in (a, b):
+            assert srv.wait(rid, timeout=180.0) == jv.JV_OK
+    _check_same(jv.JOB_RTM, a[1], w16)
+    _check_same(jv.JOB_RTM, b[1], w32)
+    assert any(not np.array_equal(a[1][q], b[1][q]) for q in range(5))
+    assert max(rel_l2(a[1][q], b[1][q]) for q in range(5)) <= 1e-3
 
 
 def test_concurrent_grids_of_different_stage_sizes():

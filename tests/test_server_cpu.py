@@ -47,3 +47,22 @@ def test_server_argument_checks():
                        np.zeros((1, 3), np.float32))
         with pytest.raises(jv.JvError):
             srv.poll(12345)
+
+
+def test_sixteen_bit_store_admitted_where_fp32_is_not(synth):
+    """The server admits a request by its footprint with the boundary store
+    it asks for: a budget one byte short of the FP32 request's footprint
+    refuses it, and admits the same request with a 16-bit store."""
+    s = synth.small_case(n=(24, 20, 18), pml=6, nt=2000, seed=3)
+    args = (jv.JOB_RTM, s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt, s.shots[0],
+            s.recvs)
+    need = jv.footprint(s.nx, s.ny, s.nz, s.pml, s.nt, kind=jv.JOB_RTM, n_recv=s.recvs.shape[0])
+    with jv.Server(slots=1, budget=need - 1) as srv:
+        with pytest.raises(jv.JvError) as e:
+            srv.submit(*args)
+        assert e.value.code == jv.JV_ENOMEM
+        with pytest.raises(jv.JvError):  # not a jv_precision
+            srv.submit(*args, precision=7)
+        rid = srv.submit(*args, precision=jv.JV_FP16)
+        assert rid > 0 and srv.stats()["submitted"] == 1
+        srv.cancel(rid)
