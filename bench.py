@@ -283,6 +283,41 @@ def serve_leg(jv, synth, n_req):
                     "warm-up requests on a server of their own are not counted"}
 
 
+def serve_config_leg(jv, synth, n_req, nt, rate):
+    """Serving at the configured grid sizes, bounded: n_req RTM requests
+    (each modelling its own traces first) on grids drawn (seeded) from
+    {120^3, 200^3, 320^3, 480 x 480 x 200} + 20 CPML, nt steps, seeded
+    layered models and source positions, arriving as a Poisson stream at
+    `rate` requests/s (the low end of the configured 1-50/s; it already
+    exceeds what these grids allow, so latency is mostly queueing), served
+    with 4 slots under the default HBM budget."""
+    grids = [(120, 120, 120), (200, 200, 200), (320, 320, 320), (480, 480, 200)]
+    rng = np.random.default_rng(5)
+    picks = [grids[int(k)] for k in rng.permutation(np.arange(n_req) % len(grids))]
+    reqs = [synth.serving_grid(*g, nt, seed=300 + k) for k, g in enumerate(picks)]
+    cells = sum(nt * (2 * r.n_ext + r.n_phy + r.n_ext) for r in reqs)  # own modelling + migration
+    with jv.Server(slots=4) as srv:
+        t0 = time.perf_counter()
+        due, subs = 0.0, []
+        for r in reqs:
+            due += rng.exponential(1.0 / rate)
+            pause = t0 + due - time.perf_counter()
+            if pause > 0:
+                time.sleep(pause)
+            subs.append(srv.submit_survey(jv.JOB_RTM, r))
+        for rid, _ in subs:
+            if srv.wait(rid, timeout=1200.0) != 0:
+                raise RuntimeError("served request failed")
+        dt = time.perf_counter() - t0
+        st = srv.stats()
+    return {"requests": n_req, "grids": ["x".join(map(str, g)) for g in picks], "pml": 20, "nt": nt,
+            "offered_per_s": rate, "unit": "RTM requests/h", "value": round(n_req / dt * 3600.0, 1),
+            "gcell_updates_per_s": round(cells / dt / 1e9, 2), "p50_ms": round(st["p50_ms"], 1),
+            "p99_ms": round(st["p99_ms"], 1), "seconds": round(dt, 2),
+            "note": "4 slots; each request models its own traces, then migrates; the configured 1500-3000 "
+                    "steps and 1-50 requests/s cut to one step count and the lowest rate"}
+
+
 def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
     """The batched configuration, bounded in shots and steps.
 
@@ -459,6 +494,9 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-extra", action="store_true", help="skip the cfg1 / cfg3 side measurements")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-configuration leg")
+    ap.add_argument("--serve-config-requests", type=int, default=6,
+                    help="requests of the configured-grid serving sample (0 skips it)")
+    ap.add_argument("--serve-config-nt", type=int, default=1500)
     ap.add_argument("--batch-shots", type=int, default=8, help="shots of the one-model batch (160^3)")
     ap.add_argument("--batch-nt", type=int, default=600, help="time steps of the one-model batch")
     ap.add_argument("--mixed-models", type=int, default=48, help="models of the mixed batch")
@@ -622,6 +660,9 @@ def main():
     serving = None
     if world == 1 and not args.no_serve:
         serving = serve_leg(jv, jv.synth, args.serve_requests)
+        if args.serve_config_requests > 0:
+            serving["configured_grids"] = serve_config_leg(jv, jv.synth, args.serve_config_requests,
+                                                           args.serve_config_nt, 1.0)
     extra = None
     if world == 1 and not args.no_extra:
         extra = extra_configs(jv, jv.synth, torch, local)

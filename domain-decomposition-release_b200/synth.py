@@ -169,3 +169,19 @@ def scaled_cfg2(n: int, nt: int, rec_width: int = 1, seed: int = 2, pml: int = 2
     return Survey(n, n, n, pml, 5.0, 5.0, 5.0, 4e-4, 20.0, nt, vp, vs, rho,
                   _pos([(n // 2, n // 2, min(5, n - 1))], d), _pos(rec, d), rec_width=rec_width,
                   name=f"rtm_{n}_w{rec_width}", seed=seed)
+
+
+def serving_grid(nx: int, ny: int, nz: int, nt: int, seed: int, rec_step: int = 4, pml: int = 20) -> Survey:
+    """One request of the serving mix: a seeded 4-layer model with dipping
+    interfaces (vp in [2000, 4000] m/s) on nx x ny x nz cells of 5 m, dt =
+    0.4 ms, 20 Hz; the source at a seeded surface position at depth 5
+    cells; receivers every rec_step cells on the surface grid at z = 5."""
+    vp = layered_vp(nx, ny, nz, seed, n_layers=4, vmin=2000, vmax=4000, dip=True)
+    vp, vs, rho = gardner(vp)
+    d = (5.0, 5.0, 5.0)
+    rng = np.random.default_rng(seed + 7)
+    src = [(int(rng.integers(nx // 4, 3 * nx // 4)), int(rng.integers(ny // 4, 3 * ny // 4)), min(5, nz - 1))]
+    jj, ii = np.meshgrid(np.arange(0, ny, rec_step), np.arange(0, nx, rec_step), indexing="ij")
+    rec = np.stack([ii.ravel(), jj.ravel(), np.full(ii.size, min(5, nz - 1))], axis=1)
+    return Survey(nx, ny, nz, pml, 5.0, 5.0, 5.0, 4e-4, 20.0, nt, vp, vs, rho, _pos(src, d), _pos(rec, d),
+                  name=f"serve_{nx}x{ny}x{nz}", seed=seed)
