@@ -146,7 +146,8 @@ struct WaveMaps {
 //    hxi = px/2, the first also the low absorbing strip [2, m), the last the
 //    high one [m+px, nx-2) (one tile: both); hxe: absorbing pairs a tile
 //    row carries (m-2 with one tile, else (m-2)/2); tpad: 4 TPP rounded up
-//    to whole warps, the first thread of the absorbing pairs; corew: the
+//    to whole warps (4 TPP where the rounding alone would take the tile
+//    past one CTA), the first thread of the absorbing pairs; corew: the
 //    core box width (the widest tile's).  ytiles, nzi: 4-row tiles over y in
 //    [2, ny-2), planes z in [2, nz-2).
 //  - The stress memory variables of this kernel are axis-major: per axis

@@ -1488,8 +1488,8 @@ __host__ __device__ inline int fz_xhi(const GridDev &g, const FzGeo &q, int xt) 
 // (computed once per thread); fz_lane gives, for tile xt, the row r, the
 // first cell x, whether it absorbs in x, and live = false when the thread
 // has no pair there.  Threads [0, 4 TPP): physical pairs; up to tpad (a
-// warp multiple): none; from tpad: absorbing pairs -- no warp mixes the
-// two updates.
+// warp multiple where that still fits one CTA): none; from tpad:
+// absorbing pairs -- then no warp mixes the two updates.
 struct FzLane {
     int r, k;   // row; pair within the tile's physical pairs, or absorbing pair index
     bool phys;
@@ -2754,6 +2754,10 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
         geo.TPP = (geo.hxi + geo.NTX - 1) / geo.NTX;
         geo.hxe = geo.NTX == 1 ? m - 2 : (m - 2) / 2;
         geo.tpad = (kZmRows * geo.TPP + 31) / 32 * 32;
+        // the physical pairs end on a warp boundary unless that alone takes
+        // the tile past one CTA; then one warp carries both updates (the
+        // kernels have no warp-level collectives) rather than a tile more
+        if (geo.tpad + kZmRows * geo.hxe > kZmMaxThreads) geo.tpad = kZmRows * geo.TPP;
         threads = geo.tpad + kZmRows * geo.hxe;
         bool fits = threads <= kZmMaxThreads && (geo.NTX - 1) * geo.TPP < geo.hxi;
         geo.corew = 0;

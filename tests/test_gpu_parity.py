@@ -386,6 +386,26 @@ def test_measured_kernel_choice(oracle, synth):
         assert ctx.kernel_config()["kernel_variant"] == 4
 
 
+def test_tile_with_a_mixed_warp(oracle, synth):
+    """A grid whose x tiles fit one CTA only without rounding the physical
+    pairs up to whole warps (484 cells, pml 6: two tiles of 121 pairs, 484 +
+    8 threads): one warp then carries both the physical and the absorbing
+    update.  Traces and images against the oracle."""
+    s = synth.small_case(n=(484, 10, 9), pml=6, nt=50, seed=17, shot_idx=[(240, 5, 3)])
+    p = _problem(oracle, s)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    with jv.Context.from_survey(s) as ctx:
+        assert ctx.kernel_config()["run_chunks"] > 0  # variant 4's kernels run
+        tr = ctx.forward(0)
+        ctx.rtm_shot(0, [o.astype(np.float32) for o in obs])
+        raw = ctx.images()
+    for a, b in zip(tr, obs):
+        assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
+    for k in ("ip", "pp", "ps", "sp", "ss"):
+        assert rel_l2(raw[k], ref[k]) <= 5e-5, (k, rel_l2(raw[k], ref[k]))
+
+
 @pytest.mark.parametrize("chunks", [1, 3, 7, 40])
 def test_run_chunks_change_no_result(synth, chunks):
     """The run schedule of the persistent TMA kernels (run_chunks: chunks
