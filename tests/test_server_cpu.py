@@ -65,4 +65,5 @@ def test_sixteen_bit_store_admitted_where_fp32_is_not(synth):
             srv.submit(*args, precision=7)
         rid = srv.submit(*args, precision=jv.JV_FP16)
         assert rid > 0 and srv.stats()["submitted"] == 1
-        srv.cancel(rid)
+        # admitted: a worker takes it at once (without a GPU it fails there)
+        srv.wait(rid, timeout=120.0)
