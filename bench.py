@@ -128,6 +128,8 @@ class ClockSampler:
 
 
 def survey(args, synth):
+    if args.grid:
+        return synth.serving_grid(*args.grid, args.nt, seed=3)
     if args.n == 200 and args.nt == 2000:
         return synth.cfg2(rec_width=args.rec_width)
     return synth.scaled_cfg2(args.n, args.nt, rec_width=args.rec_width)
@@ -491,6 +493,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="jv", choices=["jv", "reference"])
     ap.add_argument("--n", type=int, default=200, help="interior cells per axis")
+    ap.add_argument("--grid", type=int, nargs=3, metavar=("NX", "NY", "NZ"), default=None,
+                    help="a non-cubic interior instead of --n (seeded dipping layers, 5 m cells, 20 CPML)")
     ap.add_argument("--nt", type=int, default=2000)
     ap.add_argument("--rec-width", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=None)
