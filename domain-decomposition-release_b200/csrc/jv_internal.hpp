@@ -137,6 +137,7 @@ struct WaveMaps {
     int rows = 0;    // rows of a tile
     int boxw = 0, boxh = 0;  // halo box
     int corew = 0;           // core box width (rows = `rows`)
+    int ntx = 1, tpp = 0;    // x tiles and the x pairs of each (even when ntx > 1)
     int nsm = 0;     // CTAs of the persistent grid
     int *err = nullptr;  // device flag: a bounded wait in the kernel ran out
 };
@@ -219,9 +220,11 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,
                  int rec_w, const float *wavelet, const StepState *st, int it_off, const KCfg &kc, void *stream,
                  const WaveMaps *maps = nullptr);
-// Builds the TMA descriptors of w's velocity fields for variant 3 (leaves
-// maps->ok false when the grid does not suit it: more than 248 cells in x
-// or the driver entry point missing).  Returns a cudaError_t.
+// Builds the TMA descriptors of w's velocity fields for variant 3's
+// z-marching stress kernel (also variant 4's source reconstruction).  Rows
+// of more than 248 cells are cut into x tiles of an even number of pairs.
+// maps->ok stays false when those tiles would have fewer than 384 threads,
+// or the driver entry point is missing.  Returns a cudaError_t.
 int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
                      WaveMaps *maps);
 // The descriptors of the full-gridext stress kernel (variant 4), with the

@@ -849,28 +849,35 @@ template <int MODE>
 __global__ void __launch_bounds__(kZmMaxThreads, 1)
     stress_zm3(GridDev g, const __grid_constant__ ZmMaps maps, WaveDev w, float dt, int rec_w,
                const float *__restrict__ wavelet, const StepState *__restrict__ st, int it_off, int corew,
-               int ytiles, int *err) {
+               int ytiles, int ntx, int tpp, int *err) {
     constexpr int NC = (MODE == kFwd) ? kZmCore - 1 : kZmCore;  // sau is not read in forward modelling
     extern __shared__ __align__(128) float sm[];
     constexpr int hb = kZmHB, cb = kZmCB, stage = kZmStage, boxw = kZmPitch;
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int s_abort;
-    const int total = ytiles * g.pz;
+    const int total = ytiles * ntx * g.pz;  // items (y tile, x tile, plane), plane fastest
     const int w0 = (int)((long long)total * blockIdx.x / gridDim.x);
     const int w1 = (int)((long long)total * (blockIdx.x + 1) / gridDim.x);
     if (w0 >= w1) return;
     const int tid = threadIdx.x;
-    const int hx = (g.px + 1) / 2;               // x pairs of a row
-    const int r = tid / hx, x = 2 * (tid - r * hx);
-    const int nval = min(kZmCPT, g.px - x);      // 1 for the last pair of an odd row
+    const int r = tid / tpp, xl = 2 * (tid - r * tpp);  // row; the pair's first cell within an x tile
     const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
     const uint32_t bytes_all = (uint32_t)(3 * kZmHB + NC * corew * kZmRows) * 4u;
     const uint32_t bytes_feed = (uint32_t)(3 * corew * kZmRows) * 4u;  // the window feed's share
     const int m = g.m;
-    const int XH = (int)g.xoff + m - kZmHalo;  // TMA x of the halo box (a multiple of 4)
-    const int XC = (int)g.xoff + m;            // TMA x of the core box (a multiple of 32)
+    // x tile xt covers the gridphy pairs [xt tpp, (xt+1) tpp); its core box
+    // starts at gridphy column 2 xt tpp (tpp even with several tiles, so
+    // every box origin is a multiple of 4 floats) and its halo box 4 before
+    auto tile_of = [&](int item, int &xt, int &yt, int &z) {
+        const int t = item / g.pz;
+        z = item - t * g.pz;
+        yt = t / ntx;
+        xt = t - yt * ntx;
+    };
     auto issue = [&](int item, int b) {
-        const int yt = item / g.pz, z = item - yt * g.pz;
+        int xt, yt, z;
+        tile_of(item, xt, yt, z);
+        const int XC = (int)g.xoff + m + 2 * xt * tpp, XH = XC - kZmHalo;
         const uint32_t bar = b ? bar1 : bar0;
         const int Y = m + yt * kZmRows, Z = m + z;
         float *base = sm + b * stage;
@@ -898,21 +905,25 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
     }
     const int sy = (int)g.sy, sz = (int)g.sz;
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
-    const float *cx[2] = {c_list[(MODE == kBwd) ? rim_order(x, g.px, rec_w) : kPhyHalf],
-                          c_list[(MODE == kBwd) ? rim_order(min(x + 1, g.px - 1), g.px, rec_w) : kPhyHalf]};
     float2 rv[3][9];  // z windows of the pair: planes z-4 .. z+4 of vx, vy, vz
     const float *fv[3] = {w.f[VX], w.f[VY], w.f[VZ]};
-    int cur_yt = -1, cur_z = -2;
+    int cur_t = -1, cur_z = -2;
     for (int k = w0; k < w1; k++) {
-        const int yt = k / g.pz, z = k - yt * g.pz;
+        int xt, yt, z;
+        tile_of(k, xt, yt, z);
+        const int tile = k / g.pz;
+        const int x = 2 * xt * tpp + xl;              // the pair's first gridphy column
+        const int nval = min(kZmCPT, g.px - x);      // 1 for the last pair of an odd row
+        const float *cx[2] = {c_list[(MODE == kBwd) ? rim_order(x, g.px, rec_w) : kPhyHalf],
+                              c_list[(MODE == kBwd) ? rim_order(min(x + 1, g.px - 1), g.px, rec_w) : kPhyHalf]};
         const int y = yt * kZmRows + r;
-        const bool live = y < g.py;
+        const bool live = y < g.py && x < g.px;
         const int i0 = (int)g.xoff + (x + m) + sy * (y + m) + sz * (z + m);  // even: float2-aligned
         const int b = (k - w0) & 1;
         const uint32_t parity = (uint32_t)(((k - w0) >> 1) & 1);
         const float *base = sm + b * stage;
-        const int cc = r * corew + x;  // the pair in a core tile
-        if (yt != cur_yt || z != cur_z + 1) {
+        const int cc = r * corew + xl;  // the pair in a core tile
+        if (tile != cur_t || z != cur_z + 1) {
             // a new run of planes: fill the z windows from global memory
 #pragma unroll
             for (int f = 0; f < 3; f++) {
@@ -922,7 +933,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                                     : make_float2(0.f, 0.f);
             }
         }
-        cur_yt = yt;
+        cur_t = tile;
         cur_z = z;
         if (!mbar_wait_bounded(b ? bar1 : bar0, parity)) {
             s_abort = 1;
@@ -930,7 +941,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
         }
         if (live) {
             const float *P = base + 3 * hb;  // core tiles
-            const int c0 = (r + kZmHalo) * boxw + (x + kZmHalo);
+            const int c0 = (r + kZmHalo) * boxw + (xl + kZmHalo);
             const float *cy = c_list[(MODE == kBwd) ? rim_order(y, g.py, rec_w) : kPhyHalf];
             const float *cz = c_list[(MODE == kBwd) ? rim_order(z, g.pz, rec_w) : kPhyHalf];
             // x window of a field around the pair: e[j] = f[x - 4 + j], j = 0..9
@@ -2670,10 +2681,25 @@ static size_t zm3_smem() { return (size_t)2 * kZmStage * sizeof(float); }
 int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, int *err_flag,
                      WaveMaps *maps) {
     maps->ok = false;
-    const int pxr = (g.px + 3) / 4 * 4;
     const int boxw = kZmPitch, boxh = kZmBoxH;
-    // the tile must fit one CTA, and a row with its halo one box
-    if ((g.px + 1) / 2 * kZmRows > kZmMaxThreads || pxr + 2 * kZmHalo > kZmPitch) return 0;
+    // x tiles: the whole row when its pairs fit one CTA and the row with its
+    // halo one box; else the fewest tiles of an even number of pairs (so
+    // that every tile's box origin stays 16-byte aligned) that fit both.
+    // Tiles of fewer than 12 warps measured slower than the float4 kernel
+    // (320 cells: two tiles of 320 threads, 665 against 633 us), so such
+    // grids leave this kernel unused.
+    const int hx = (g.px + 1) / 2;
+    int ntx = 1, tpp = hx;
+    auto fits = [&](int n) { return n * kZmRows <= kZmMaxThreads && (2 * n + 3) / 4 * 4 + 2 * kZmHalo <= kZmPitch; };
+    if (!fits(tpp)) {
+        for (ntx = 2; ntx <= 16; ntx++) {
+            tpp = (hx + ntx - 1) / ntx;
+            tpp += tpp & 1;
+            if (fits(tpp)) break;
+        }
+        if (ntx > 16 || tpp * kZmRows < 384) return 0;
+    }
+    const int pxr = (2 * tpp + 3) / 4 * 4;  // the core box width
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void *fn = nullptr;
@@ -2721,6 +2747,8 @@ int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     maps->boxw = boxw;
     maps->boxh = boxh;
     maps->corew = pxr;
+    maps->ntx = ntx;
+    maps->tpp = tpp;
     maps->nsm = nsm;
     maps->err = err_flag;
     maps->ok = true;
@@ -2951,13 +2979,14 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
         std::memcpy(zm.halo, maps->halo, sizeof(maps->halo));
         std::memcpy(zm.core, maps->core, sizeof(maps->core));
         const int ytiles = (g.py + maps->rows - 1) / maps->rows;
-        const long long items = (long long)ytiles * g.pz;
+        const long long items = (long long)ytiles * maps->ntx * g.pz;
         const int grid = (int)std::min<long long>(maps->nsm, items);
-        const dim3 b((g.px + 1) / 2 * maps->rows);
+        const dim3 b(maps->tpp * maps->rows);
         const size_t smem = zm3_smem();
         switch (mode) {
 #define JV_ZM3(M)                                                                                              \
-    stress_zm3<M><<<grid, b, smem, s>>>(g, zm, w, dt, rec_w, wavelet, st, it_off, maps->corew, ytiles, maps->err)
+    stress_zm3<M><<<grid, b, smem, s>>>(g, zm, w, dt, rec_w, wavelet, st, it_off, maps->corew, ytiles, maps->ntx, \
+                                        maps->tpp, maps->err)
         case kFwd: JV_ZM3(kFwd); break;
         case kRtmFwd: JV_ZM3(kRtmFwd); break;
         case kBwd: JV_ZM3(kBwd); break;

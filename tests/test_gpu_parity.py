@@ -328,6 +328,35 @@ def test_full_kernels_x_tiles_forward_vs_oracle(oracle, synth, kw):
         assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
 
 
+ZM3_WIDE = [
+    dict(n=(400, 10, 9), pml=6, nt=60, seed=61),                                   # 2 tiles of 100 pairs
+    dict(n=(484, 9, 10), pml=8, nt=60, seed=62, shot_idx=[(470, 4, 5)]),           # 2 tiles of 122 pairs
+    dict(n=(676, 8, 8), pml=4, nt=50, seed=63, shot_idx=[(338, 4, 4)], nrec=20),   # 3 tiles of 114 pairs
+]
+
+
+@pytest.mark.parametrize("kw", ZM3_WIDE)
+def test_zm3_x_tiles_vs_oracle(oracle, synth, kw):
+    """Variant 3 on grids wider than one 248-cell row: its z-marching
+    stress kernel cuts the rows into x tiles of at least 12 warps for every
+    stress update, forward modelling, the RTM forward pass, the source
+    reconstruction and the receiver side.  Traces and images against the
+    oracle."""
+    s = synth.small_case(**kw)
+    p = _problem(oracle, s)
+    obs = oracle.forward(p)
+    ref = oracle.rtm_shot(p, obs)
+    with jv.Context.from_survey(s, kernel_variant=3) as ctx:
+        assert ctx.kernel_config()["kernel_variant"] == 3
+        tr = ctx.forward(0)
+        ctx.rtm_shot(0, [o.astype(np.float32) for o in obs])
+        raw = ctx.images()
+    for a, b in zip(tr, obs):
+        assert rel_l2(a, b) <= 2e-5, rel_l2(a, b)
+    for k in ("ip", "pp", "ps", "sp", "ss"):
+        assert rel_l2(raw[k], ref[k]) <= 5e-5, (k, rel_l2(raw[k], ref[k]))
+
+
 def test_full_kernels_x_tiles_rtm_vs_oracle(oracle, synth):
     s = synth.small_case(**dict(WIDE[0], rec_width=2, anomaly=(0.1, 3.0)))
     p = _problem(oracle, s, 2)
