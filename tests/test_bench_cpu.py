@@ -66,3 +66,11 @@ def test_traffic_read_from_the_committed_profile():
     t = bench.traffic_from_profiles("vel_phy_bwd_image")
     assert t is not None and 1.0e9 < t < 1.5e9
     assert bench.traffic_from_profiles("no_such_kernel") is None
+
+
+def test_reference_arm_on_a_non_cubic_grid():
+    r = _run("--impl", "reference", "--grid", "24", "16", "12", "--nt", "20", "--steps", "1", "--warmup", "3",
+             "--ref-sample-steps", "4")
+    assert r.returncode == 0, r.stderr
+    d = json.loads([ln for ln in r.stdout.splitlines() if ln.strip()][0])
+    assert d["config"]["grid_phy"] == [24, 16, 12] and d["config"]["pml"] == 20 and d["value"] > 0
