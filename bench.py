@@ -448,6 +448,46 @@ def extra_configs(jv, synth, torch, device):
     return out
 
 
+def spawn_ranks(args) -> int:
+    """`--gpus N` (N > 1) without a launcher: start N ranks of this same
+    command under torch.distributed.run (one process per GPU, rendezvous on
+    127.0.0.1), as the reference's run script starts its MPI ranks itself
+    (build/jarvis/jarvis_2_run:5-12).  Rank 0 prints the line; the exit
+    code is the launcher's."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
+
+
+def dry_run(args) -> int:
+    """The rank plumbing alone, on CPU (gloo): every rank takes its shard of
+    the job's steps * world shots (replicas.shard_shots) and rank 0 prints
+    one line with the world size and every rank's shard.  Nothing is timed."""
+    import datetime
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    rep = importlib.import_module("domain-decomposition-release_b200.replicas")
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    mine = rep.shard_shots(args.steps * world, rank, world)
+    shards = [None] * world
+    if world > 1:
+        dist.all_gather_object(shards, mine)
+        dist.barrier()
+        dist.destroy_process_group()
+    else:
+        shards = [mine]
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "impl": args.impl, "n_gpus": world, "steps": args.steps,
+                          "shots": args.steps * world, "shards": shards}), flush=True)
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -472,7 +512,8 @@ def run_reference(args):
     sample = (f"{sample_steps} of {s.nt} time steps of each propagation of one RTM shot "
               f"({s.nx}^3 + {s.pml} CPML, {s.recvs.shape[0]} receivers), scaled to a full shot")
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "shots/h", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "shots/h",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * sec_per_shot, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)", "gcell_updates_per_s": round(cells * args.steps / tot / 1e9, 4),
@@ -515,10 +556,23 @@ def main():
     ap.add_argument("--variant", type=int, default=None, help="interior kernel variant (default: library default)")
     ap.add_argument("--store", default="fp32", choices=["fp32", "bf16", "fp16"],
                     help="boundary-store precision (wavefields are FP32 in every case)")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="CPU only: start the ranks and print their shot shards, no GPU work")
     args = ap.parse_args()
     if args.warmup < 3:
         print("bench.py: --warmup must be >= 3", file=sys.stderr)
         return 2
+    if args.gpus < 1:
+        print("bench.py: --gpus must be >= 1", file=sys.stderr)
+        return 2
+    launched = os.environ.get("WORLD_SIZE")
+    if launched is None and args.gpus > 1:
+        return spawn_ranks(args)
+    if launched is not None and int(launched) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but the launcher started WORLD_SIZE={launched} ranks", file=sys.stderr)
+        return 2
+    if args.dry_run:
+        return dry_run(args)
     if args.impl == "reference":
         return run_reference(args)
 
@@ -539,6 +593,13 @@ def main():
     if args.store != "fp32":
         kopts["precision"] = {"bf16": jv.JV_BF16, "fp16": jv.JV_FP16}[args.store]
     ctx = jv.Context.from_survey(s, device=local, **kopts)
+    # the job: steps * world shots at the survey's source position, shot s
+    # on rank s % world (replicas.shard_shots); per-shot work does not
+    # depend on the position, so the per-rank work is fixed as N grows
+    rep = importlib.import_module("domain-decomposition-release_b200.replicas")
+    n_job = args.steps * world
+    ctx.set_geometry(np.repeat(s.shots[:1], n_job, axis=0), s.recvs)
+    mine = rep.shard_shots(n_job, rank, world)
     info = ctx.info()
     nrec, nt = info.n_recv, info.nt
     obs = torch.empty((3, nrec, nt), dtype=torch.float32, device=f"cuda:{local}")
@@ -560,8 +621,8 @@ def main():
     barrier()
     dev_ms = 0.0
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        ctx.rtm_shot_device(0, ptrs)
+    for shot in mine:
+        ctx.rtm_shot_device(shot, ptrs)
         dev_ms += ctx.last_ms()
     barrier()
     wall = time.perf_counter() - t0
@@ -694,7 +755,6 @@ def main():
     # the job's one exchange: sum the FP64 stacks of all replicas (after timing)
     reduce_ms = None
     if dist is not None:
-        rep = importlib.import_module("domain-decomposition-release_b200.replicas")
         barrier()
         t0 = time.perf_counter()
         rep.reduce_images(ctx, device=local)
@@ -715,6 +775,7 @@ def main():
         "gcell_updates_per_s": round(gcells, 3),
         "config": {"workload": s.name, "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt,
                    "rec_width": s.rec_width, "n_recv": nrec, "mode": "plain one-shot-per-call, graph time loop",
+                   "job": f"{n_job} shots at the survey's source position, shot s on rank s % {world}",
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
                    "boundary_store": args.store,
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},

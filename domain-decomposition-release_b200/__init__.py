@@ -37,7 +37,8 @@ IMG_IP, IMG_PP, IMG_PS, IMG_SP, IMG_SS = range(5)
 
 # every symbol include/jv/jv.h declares
 EXPORTS = (
-    "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_get_info", "jv_get_kernel_config",
+    "jv_options_default", "jv_create", "jv_open", "jv_set_geometry", "jv_set_model", "jv_get_info",
+    "jv_get_kernel_config",
     "jv_reconstruction_energy",
     "jv_forward",
     "jv_forward_device", "jv_rtm_shot", "jv_rtm_shot_device", "jv_image_reset", "jv_image_get",
@@ -91,7 +92,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
                 ("cancelled", C.c_longlong), ("running", C.c_longlong), ("queued", C.c_longlong),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
-                ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t)]
+                ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t), ("reused", C.c_longlong),
+                ("pooled", C.c_longlong)]
 
 
 class ArgFileC(C.Structure):
@@ -146,6 +148,7 @@ def lib() -> C.CDLL:
                             C.POINTER(ctxp)]
     L.jv_open.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(ctxp)]
     L.jv_set_geometry.argtypes = [ctxp, C.c_int, fp, C.c_int, fp]
+    L.jv_set_model.argtypes = [ctxp, fp, fp, fp]
     L.jv_get_info.argtypes = [ctxp, C.POINTER(Info)]
     L.jv_get_kernel_config.argtypes = [ctxp, C.POINTER(Options)]
     L.jv_reconstruction_energy.argtypes = [ctxp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -252,6 +255,16 @@ class Context:
         sh = np.ascontiguousarray(shots, dtype=np.float32).reshape(-1, 3)
         rc = np.ascontiguousarray(recvs, dtype=np.float32).reshape(-1, 3)
         _check(lib().jv_set_geometry(self._h, sh.shape[0], _fptr(sh), rc.shape[0], _fptr(rc)))
+
+    def set_model(self, vp, vs, rho) -> None:
+        """A new model of the same grid (jv_set_model): buffers and captured
+        graphs are kept."""
+        i = self.info()
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho)]
+        for a in arrs:
+            if a.size != i.grid.nx * i.grid.ny * i.grid.nz:
+                raise JvError(JV_EINVAL, "model array size does not match the grid")
+        _check(lib().jv_set_model(self._h, _fptr(arrs[0]), _fptr(arrs[1]), _fptr(arrs[2])))
 
     # -- queries ------------------------------------------------------------
     def reconstruction_energy(self):

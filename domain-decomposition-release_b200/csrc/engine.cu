@@ -513,15 +513,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     float *mb = (float *)p + kGuard;
     vp_ = mb; rho_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
     const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
-    float *tmp = nullptr;
-    JV_CU(cudaMallocAsync(&tmp, 3 * nphy * sizeof(float), stream_));
-    cudaError_t e1 = cudaMemcpyAsync(tmp, vp, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    cudaError_t e2 = cudaMemcpyAsync(tmp + nphy, vs, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    cudaError_t e3 = cudaMemcpyAsync(tmp + 2 * nphy, rho, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    int ek = k_model_prep(g_, tmp, tmp + nphy, tmp + 2 * nphy, vp_, rho_, lam_, mu_, stream_);
-    cudaFreeAsync(tmp, stream_);
-    cudaError_t e4 = cudaStreamSynchronize(stream_);
-    JV_CU(e1); JV_CU(e2); JV_CU(e3); JV_K(ek); JV_CU(e4);
+    JV_TRY(upload_model(vp, vs, rho));
 
     // forward/backward wavefield (13 components, one arena)
     JV_TRY(alloc(&p, (kNumFld * field_elems_ + kGuard) * sizeof(float)));
@@ -608,6 +600,29 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     return Status{};
 }
 
+// vp, vs, rho (host, gridphy) -> the extended model and lambda, mu on the
+// device, in the buffers every kernel and tensor map of the context uses
+Status Engine::upload_model(const float *vp, const float *vs, const float *rho) {
+    if (!vp || !vs || !rho) return bad(JV_EINVAL, "model arrays must not be NULL");
+    const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
+    float *tmp = nullptr;
+    JV_CU(cudaMallocAsync(&tmp, 3 * nphy * sizeof(float), stream_));
+    cudaError_t e1 = cudaMemcpyAsync(tmp, vp, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    cudaError_t e2 = cudaMemcpyAsync(tmp + nphy, vs, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    cudaError_t e3 = cudaMemcpyAsync(tmp + 2 * nphy, rho, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
+    int ek = k_model_prep(g_, tmp, tmp + nphy, tmp + 2 * nphy, vp_, rho_, lam_, mu_, stream_);
+    cudaFreeAsync(tmp, stream_);
+    cudaError_t e4 = cudaStreamSynchronize(stream_);
+    JV_CU(e1); JV_CU(e2); JV_CU(e3); JV_K(ek); JV_CU(e4);
+    return Status{};
+}
+
+Status Engine::set_model(const float *vp, const float *vs, const float *rho) {
+    JV_CU(cudaSetDevice(dev_));
+    JV_CU(cudaStreamSynchronize(stream_));
+    return upload_model(vp, vs, rho);
+}
+
 Status Engine::set_geometry(int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz) {
     if (n_shot < 0 || n_recv < 0 || (n_shot > 0 && !shot_xyz) || (n_recv > 0 && !recv_xyz))
         return bad(JV_EINVAL, "bad geometry arguments");
@@ -626,6 +641,13 @@ Status Engine::set_geometry(int n_shot, const float *shot_xyz, int n_recv, const
         int i = gap_num(lx, q[0], grid_.dx), j = gap_num(ly, q[1], grid_.dy), k = gap_num(lz, q[2], grid_.dz);
         rec_h_.push_back(g_.xoff + i + g_.sy * j + g_.sz * k);
     }
+    // the same receiver count: the indices go into the buffer the captured
+    // graphs already read, and the graphs stay valid
+    if (rec_d_ && (int)rec_h_.size() == nrec_) {
+        JV_CU(cudaMemcpy(rec_d_, rec_h_.data(), nrec_ * sizeof(long long), cudaMemcpyHostToDevice));
+        return Status{};
+    }
+    if (!rec_d_ && rec_h_.empty() && nrec_ == 0) return Status{};
     nrec_ = (int)rec_h_.size();
     if (rec_d_) {
         cudaFreeAsync(rec_d_, stream_);

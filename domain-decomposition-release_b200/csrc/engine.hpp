@@ -76,6 +76,9 @@ class Engine {
                          int nt, const jv_options &opt, Engine **out);
 
     Status set_geometry(int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz);
+    // a new model of the same grid (host arrays on gridphy); buffers, tensor
+    // maps and captured graphs stay as they are
+    Status set_model(const float *vp, const float *vs, const float *rho);
     Status forward(int shot, float *d_vx, float *d_vy, float *d_vz);
     Status rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz);
     Status image_reset();
@@ -105,6 +108,7 @@ class Engine {
    private:
     Engine() = default;
     Status alloc_all(const float *vp, const float *vs, const float *rho);
+    Status upload_model(const float *vp, const float *vs, const float *rho);
     Status check_shot(int shot, long long *src) const;
     Status run_loop(int kind, int nsteps);
     Status launch_step(int kind, int off, bool advance);

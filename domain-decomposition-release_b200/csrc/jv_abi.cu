@@ -279,6 +279,11 @@ jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_re
     return ret(s);
 }
 
+jv_status jv_set_model(jv_ctx *c, const float *vp, const float *vs, const float *rho) {
+    JV_IDLE(c);
+    return ret(c->eng->set_model(vp, vs, rho));
+}
+
 jv_status jv_get_info(const jv_ctx *c, jv_info *info) {
     if (!c || !info) return fail(JV_EINVAL, "NULL argument");
     c->eng->info(info);

@@ -19,8 +19,14 @@
 //
 // Host code cannot use the array's name as a device address (in host code
 // it is a host-side stand-in), so the first call on each device, with that
-// device current, looks the address up with cudaGetSymbolAddress and caches
-// it.
+// device current, looks the address up with cudaGetSymbolAddress, uploads
+// the finite-difference coefficients into constant memory (the same values
+// every context uses) and caches both facts with the device's current
+// context.  A later call that finds another context current on the device
+// (after cudaDeviceReset, or a primary context torn down and created anew)
+// repeats that set-up.  The set-up synchronises the device once, so make the
+// first call on a device before any stream capture; later calls only queue
+// copies, memsets and kernels on `stream` and wait for that stream.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,25 +47,52 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void *g_addr[kMaxDevices] = {};
+struct DeviceSetup {
+    void *ctx = nullptr;   // the context current when the set-up ran
+    void *addr = nullptr;  // device address of g_noalloc_scratch in it
+};
+DeviceSetup g_setup[kMaxDevices];
 
 jv_status fail(jv_status c, const std::string &m) {
     jv::set_last_error(m);
     return c;
 }
 
-// device address of the scratch array for `dev` (looked up once per device)
-jv_status scratch_address(int dev, unsigned char **out) {
+// the calling thread's current context (driver API, reached through the
+// runtime so that the library needs no -lcuda); nullptr if unavailable
+void *current_context() {
+    typedef int (*CtxGetCurrent)(void **);
+    static CtxGetCurrent fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (CtxGetCurrent) nullptr;
+        return (CtxGetCurrent)f;
+    }();
+    void *c = nullptr;
+    if (fn && fn(&c) != 0) c = nullptr;
+    return c;
+}
+
+// Per-device set-up, once per device and context, under g_mu: the device
+// address of the scratch array and the constant-memory coefficients.
+jv_status device_setup(int dev, unsigned char **out) {
     if (dev < 0 || dev >= kMaxDevices) return fail(JV_EINVAL, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
+    DeviceSetup &d = g_setup[dev];
+    void *ctx = current_context();
+    if (!d.addr || ctx != d.ctx) {
+        d.addr = nullptr;
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return fail(JV_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-        g_addr[dev] = p;
+        if (jv::upload_all_coefficients() != 0) return fail(JV_ECUDA, "coefficient upload failed");
+        d.ctx = ctx;
+        d.addr = p;
     }
-    *out = (unsigned char *)g_addr[dev];
+    *out = (unsigned char *)d.addr;
     return JV_OK;
 }
 
@@ -121,7 +154,7 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
 
     // carve the scratch array; refuse problems that do not fit
     unsigned char *base = nullptr;
-    jv_status st = scratch_address(dev, &base);
+    jv_status st = device_setup(dev, &base);
     if (st != JV_OK) return st;
     Carver cv{base, 0, kNoAllocScratchBytes};
     float *model = cv.take<float>(4 * fe + guard);
@@ -136,9 +169,6 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
         return fail(JV_EINVAL, "problem needs more than the " + std::to_string(kNoAllocScratchBytes >> 20) +
                                    " MiB no-allocation scratch; use jv_create/jv_forward");
     if (fe >= ((size_t)1 << 31)) return fail(JV_EINVAL, "grid too large");
-
-    // coefficient tables (constant memory, no allocation)
-    if (upload_all_coefficients() != 0) return fail(JV_ECUDA, "coefficient upload failed");
 
     // host-side tables, copied into the scratch array
     std::vector<float4> t[3];
@@ -156,10 +186,15 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
         if (ee != cudaSuccess) return fail(JV_ECUDA, std::string(what) + ": " + cudaGetErrorString(ee));
         return JV_OK;
     };
+    // on failure, wait for the work already queued on `s` (it still writes the
+    // scratch array and the caller's trace buffers) before returning
 #define NA_CK(expr)                                    \
     do {                                               \
         jv_status _s = ck((cudaError_t)(expr), #expr); \
-        if (_s != JV_OK) return _s;                    \
+        if (_s != JV_OK) {                             \
+            (void)cudaStreamSynchronize(s);            \
+            return _s;                                 \
+        }                                              \
     } while (0)
     for (int a = 0; a < 3; a++)
         NA_CK(cudaMemcpyAsync(tabs[a], t[a].data(), t[a].size() * sizeof(float4), cudaMemcpyHostToDevice, s));

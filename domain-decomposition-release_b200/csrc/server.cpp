@@ -2,14 +2,22 @@
 //
 // A request is one shot of forward modelling or RTM on its own model and
 // grid.  The server keeps a queue of requests and `slots` worker threads;
-// a worker takes the first queued request whose device footprint
-// (footprint_bytes) fits the memory still free under the server's budget,
-// runs it on a context of its own (own stream, own device memory from the
-// stream-ordered allocator), copies the results to the request's host
-// buffers and releases the context.  Requests admitted together run
-// concurrently on the GPU.  Each request's result does not depend on what
-// else runs: a context's kernels touch only its own memory.  Every wait here
-// is a host wait, bounded where the caller asks for a time limit.
+// a worker takes the first queued request that it can place: one for which
+// an idle context of the same problem shape is pooled, or whose device
+// footprint (footprint_bytes) fits the memory still free under the server's
+// budget once idle pooled contexts are released, least recently used first.
+// The request runs on that context (own stream, own device memory from the
+// stream-ordered allocator); the results go to the request's host buffers
+// and the context goes back to the pool.
+//
+// A pooled context keeps its buffers, tensor maps and captured time-loop
+// graphs; the next request of its shape only uploads its model
+// (jv_set_model), geometry and a cleared image stack.  Requests admitted
+// together run concurrently on the GPU.  Each request's result does not
+// depend on what else runs, nor on whether its context is new or pooled:
+// every shot starts from cleared wavefields, memory variables and shot
+// images, and a context's kernels touch only its own memory.  Every wait
+// here is a host wait, bounded where the caller asks for a time limit.
 //
 // The reference has no counterpart: its driver runs the shots of one job
 // in a loop (RTM/rtm3d_1_model_mpi_blend/rtm3d_blend_elastic_model_mpi_meat.hpp:18-135,
@@ -19,11 +27,14 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
+#include <list>
 #include <map>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "engine.hpp"
@@ -35,6 +46,25 @@ using clk = std::chrono::steady_clock;
 
 // how many of the latest latencies the p50/p99 statistics are taken over
 constexpr size_t kLatencyWindow = 1 << 16;
+// finished requests the server still answers jv_server_poll/wait for; the
+// oldest finished records beyond this are forgotten
+constexpr size_t kFinishedKept = 1 << 16;
+
+// what a context is created for: requests with equal keys share contexts
+struct PoolKey {
+    int nx, ny, nz, pml;
+    float dx, dy, dz, dt, fm;
+    int nt, rec_width, precision, kind, n_recv;
+    auto tie() const {
+        return std::tie(nx, ny, nz, pml, dx, dy, dz, dt, fm, nt, rec_width, precision, kind, n_recv);
+    }
+    bool operator==(const PoolKey &o) const { return tie() == o.tie(); }
+};
+
+PoolKey key_of(const jv_request &q) {
+    return PoolKey{q.grid.nx, q.grid.ny, q.grid.nz, q.grid.pml, q.grid.dx, q.grid.dy, q.grid.dz, q.dt, q.fm,
+                   q.nt, q.rec_width > 0 ? q.rec_width : 1, q.precision, q.kind, q.n_recv};
+}
 
 struct Req {
     jv_request r{};
@@ -45,63 +75,130 @@ struct Req {
     clk::time_point t_submit, t_done;
 };
 
+struct Idle {
+    PoolKey key;
+    jv_ctx *ctx;
+    size_t bytes;
+};
+
 jv_status fail(jv_status c, const std::string &m) {
     jv::set_last_error(m);
     return c;
+}
+
+// The device's stream-ordered pool keeps up to the largest open server's
+// budget cached while any server on that device is open (transient
+// allocations of requests reuse it instead of mapping fresh memory).  The
+// first server on a device records the threshold it found; the last one to
+// close puts it back and trims the pool down to it.
+struct PoolThreshold {
+    int servers = 0;
+    uint64_t before = 0, kept = 0;
+};
+std::mutex g_thr_mu;
+std::map<int, PoolThreshold> g_thr;
+
+void pool_threshold_open(int device, uint64_t budget) {
+    std::lock_guard<std::mutex> l(g_thr_mu);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    PoolThreshold &t = g_thr[device];
+    if (t.servers == 0) {
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &t.before) != cudaSuccess) {
+            cudaGetLastError();
+            g_thr.erase(device);
+            return;
+        }
+        t.kept = t.before;
+    }
+    t.servers++;
+    if (budget > t.kept) {
+        t.kept = budget;
+        if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &t.kept) != cudaSuccess)
+            cudaGetLastError();
+    }
+}
+
+void pool_threshold_close(int device) {
+    std::lock_guard<std::mutex> l(g_thr_mu);
+    auto it = g_thr.find(device);
+    if (it == g_thr.end()) return;
+    if (--it->second.servers > 0) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t before = it->second.before;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &before);
+        cudaMemPoolTrimTo(pool, (size_t)before);
+    }
+    cudaGetLastError();
+    g_thr.erase(it);
 }
 
 }  // namespace
 
 struct jv_server {
     int device = 0;
-    size_t budget = 0, in_use = 0;
+    size_t budget = 0;
+    size_t in_use = 0;  // footprints of running requests and of pooled idle contexts
     std::mutex mu;
     std::condition_variable cv, done_cv;
     std::deque<long long> queue;
     std::map<long long, Req> reqs;
+    std::deque<long long> finished;  // ids in the order they ended
     long long next_id = 1;
     int running = 0;
     bool stop = false;
     std::vector<std::thread> workers;
     std::vector<double> latencies_ms;
-    long long n_completed = 0, n_failed = 0, n_cancelled = 0;
-    // the device's stream-ordered pool keeps up to the budget cached while
-    // the server is open (contexts of later requests reuse it instead of
-    // mapping fresh memory); the previous threshold is put back at close
-    cudaMemPool_t pool = nullptr;
-    uint64_t pool_threshold_before = 0;
+    long long n_completed = 0, n_failed = 0, n_cancelled = 0, n_reused = 0;
+    std::list<Idle> idle;  // pooled contexts, most recently used first
+    bool threshold_set = false;
 };
 
 namespace {
 
-// one request on a context of its own
-jv_status run_request(int device, const jv_request &q) {
-    jv_options o;
-    jv_options_default(&o);
-    o.device = device;
-    o.rec_width = q.rec_width > 0 ? q.rec_width : 1;
-    o.precision = q.precision;
-    jv_ctx *c = nullptr;
-    jv_status st = jv_create(&q.grid, q.vp, q.vs, q.rho, q.dt, q.fm, q.nt, &o, &c);
+// marks a request ended (under s->mu) and forgets the oldest ended ones
+void record_end(jv_server *s, long long id) {
+    s->finished.push_back(id);
+    while (s->finished.size() > kFinishedKept) {
+        s->reqs.erase(s->finished.front());
+        s->finished.pop_front();
+    }
+}
+
+// one request on `c`: a pooled context of its shape, or (c == NULL) a new one
+jv_status run_request(int device, const jv_request &q, jv_ctx **c) {
+    jv_status st;
+    if (*c) {
+        st = jv_set_model(*c, q.vp, q.vs, q.rho);
+        if (st == JV_OK) st = jv_image_reset(*c);
+    } else {
+        jv_options o;
+        jv_options_default(&o);
+        o.device = device;
+        o.rec_width = q.rec_width > 0 ? q.rec_width : 1;
+        o.precision = q.precision;
+        st = jv_create(&q.grid, q.vp, q.vs, q.rho, q.dt, q.fm, q.nt, &o, c);
+    }
     if (st != JV_OK) return st;
-    st = jv_set_geometry(c, 1, q.shot_xyz, q.n_recv, q.recv_xyz);
+    st = jv_set_geometry(*c, 1, q.shot_xyz, q.n_recv, q.recv_xyz);
     if (st == JV_OK) {
         if (q.kind == JV_JOB_FORWARD) {
-            st = jv_forward(c, 0, q.out[0], q.out[1], q.out[2]);
+            st = jv_forward(*c, 0, q.out[0], q.out[1], q.out[2]);
         } else {
             // without observed traces the request models its own, which
             // stay on the device
             if (!q.obs[0] && !q.obs[1] && !q.obs[2])
-                st = jv::rtm_self_modelled(c, 0);
+                st = jv::rtm_self_modelled(*c, 0);
             else
-                st = jv_rtm_shot(c, 0, q.obs[0], q.obs[1], q.obs[2]);
+                st = jv_rtm_shot(*c, 0, q.obs[0], q.obs[1], q.obs[2]);
             for (int k = 0; k < 5 && st == JV_OK; k++)
-                if (q.image[k]) st = jv_image_get(c, k, q.image[k]);
+                if (q.image[k]) st = jv_image_get(*c, k, q.image[k]);
         }
     }
-    const std::string msg = st == JV_OK ? std::string() : jv_last_error();
-    jv_close(c);
-    if (st != JV_OK) jv::set_last_error(msg);
     return st;
 }
 
@@ -110,13 +207,39 @@ void worker_main(jv_server *s) {
     for (;;) {
         long long id = 0;
         jv_request q{};
+        jv_ctx *ctx = nullptr;
+        size_t bytes = 0;
+        std::vector<jv_ctx *> evict;
         {
             std::unique_lock<std::mutex> l(s->mu);
-            // the first queued request that fits the memory still free
+            // The first queued request that can be placed: on a pooled idle
+            // context of its shape, or on a new context whose footprint fits
+            // the budget once idle contexts (least recently used first) are
+            // released.
             auto pick = [&]() -> bool {
+                size_t idle_bytes = 0;
+                for (const Idle &d : s->idle) idle_bytes += d.bytes;
                 for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
                     const Req &r = s->reqs[*it];
-                    if (s->in_use + r.bytes <= s->budget) {
+                    const PoolKey k = key_of(r.r);
+                    for (auto d = s->idle.begin(); d != s->idle.end(); ++d)
+                        if (d->key == k) {
+                            ctx = d->ctx;
+                            bytes = d->bytes;
+                            s->idle.erase(d);
+                            id = *it;
+                            s->queue.erase(it);
+                            s->n_reused++;
+                            return true;
+                        }
+                    if (s->in_use - idle_bytes + r.bytes <= s->budget) {
+                        while (s->in_use + r.bytes > s->budget && !s->idle.empty()) {
+                            evict.push_back(s->idle.back().ctx);
+                            s->in_use -= s->idle.back().bytes;
+                            s->idle.pop_back();
+                        }
+                        bytes = r.bytes;
+                        s->in_use += bytes;
                         id = *it;
                         s->queue.erase(it);
                         return true;
@@ -128,12 +251,16 @@ void worker_main(jv_server *s) {
             if (id == 0) return;  // stop requested
             Req &r = s->reqs[id];
             r.state = JV_JOB_RUNNING;
-            s->in_use += r.bytes;
             s->running++;
             q = r.r;
         }
-        const jv_status st = run_request(s->device, q);
+        for (jv_ctx *c : evict) jv_close(c);  // their memory returns before the new context allocates
+        jv_status st = run_request(s->device, q, &ctx);
         const std::string msg = st == JV_OK ? std::string() : jv_last_error();
+        if (st != JV_OK && ctx) {
+            jv_close(ctx);  // a failed context is not pooled
+            ctx = nullptr;
+        }
         {
             std::lock_guard<std::mutex> l(s->mu);
             Req &r = s->reqs[id];
@@ -141,7 +268,12 @@ void worker_main(jv_server *s) {
             r.result = st;
             r.msg = msg;
             r.t_done = clk::now();
-            s->in_use -= r.bytes;
+            if (ctx && !s->stop) {
+                s->idle.push_front(Idle{key_of(q), ctx, bytes});
+                ctx = nullptr;
+            } else {
+                s->in_use -= bytes;
+            }
             s->running--;
             if (st == JV_OK) {
                 // the latency record keeps the most recent requests only
@@ -152,9 +284,11 @@ void worker_main(jv_server *s) {
             } else {
                 s->n_failed++;
             }
+            record_end(s, id);
         }
+        if (ctx) jv_close(ctx);  // the server is closing
         s->done_cv.notify_all();
-        s->cv.notify_all();  // memory came free: another request may fit now
+        s->cv.notify_all();  // a context or memory came free: another request may be placed now
     }
 }
 
@@ -198,14 +332,8 @@ jv_status jv_server_create(int device, int slots, size_t hbm_budget, jv_server *
     s->device = device;
     s->budget = budget;
     cudaSetDevice(device);
-    if (cudaDeviceGetDefaultMemPool(&s->pool, device) == cudaSuccess &&
-        cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &s->pool_threshold_before) == cudaSuccess) {
-        uint64_t keep = budget;
-        if (cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) s->pool = nullptr;
-    } else {
-        s->pool = nullptr;
-        cudaGetLastError();
-    }
+    pool_threshold_open(device, budget);
+    s->threshold_set = true;
     for (int k = 0; k < slots; k++) s->workers.emplace_back(worker_main, s);
     *out = s;
     jv::set_last_error("");
@@ -258,15 +386,21 @@ jv_status jv_server_poll(jv_server *s, long long id, int *state, jv_status *resu
 jv_status jv_server_wait(jv_server *s, long long id, double timeout_s, jv_status *result) {
     if (!s) return fail(JV_EINVAL, "jv_server_wait: NULL server");
     std::unique_lock<std::mutex> l(s->mu);
-    auto it = s->reqs.find(id);
-    if (it == s->reqs.end()) return fail(JV_EINVAL, "no such request");
-    auto ended = [&] { return it->second.state == JV_JOB_DONE || it->second.state == JV_JOB_CANCELLED; };
+    if (s->reqs.find(id) == s->reqs.end()) return fail(JV_EINVAL, "no such request");
+    // looked up again on every wake: records of ended requests may be dropped meanwhile
+    auto ended = [&] {
+        auto it = s->reqs.find(id);
+        return it == s->reqs.end() || it->second.state == JV_JOB_DONE || it->second.state == JV_JOB_CANCELLED;
+    };
     if (timeout_s < 0) {
         s->done_cv.wait(l, ended);
     } else if (!s->done_cv.wait_for(l, std::chrono::duration<double>(timeout_s), ended)) {
+        auto it = s->reqs.find(id);
         jv::set_last_error(it->second.state == JV_JOB_RUNNING ? "request still running" : "request still queued");
         return JV_ETIMEOUT;
     }
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return fail(JV_EINVAL, "request ended and its record was dropped");
     if (result) *result = it->second.result;
     jv::set_last_error(it->second.msg);
     return JV_OK;
@@ -284,6 +418,7 @@ jv_status jv_server_cancel(jv_server *s, long long id) {
         it->second.result = JV_ECANCELED;
         it->second.msg = "cancelled before it started";
         s->n_cancelled++;
+        record_end(s, id);
     }
     s->done_cv.notify_all();
     jv::set_last_error("");
@@ -305,6 +440,8 @@ jv_status jv_server_get_stats(jv_server *s, jv_server_stats *out) {
     for (double v : s->latencies_ms) sum += v;
     out->mean_ms = s->latencies_ms.empty() ? 0.0 : sum / (double)s->latencies_ms.size();
     out->bytes_in_use = s->in_use;
+    out->reused = s->n_reused;
+    out->pooled = (long long)s->idle.size();
     out->budget = s->budget;
     jv::set_last_error("");
     return JV_OK;
@@ -327,11 +464,9 @@ jv_status jv_server_close(jv_server *s) {
     s->done_cv.notify_all();
     for (std::thread &t : s->workers)
         if (t.joinable()) t.join();
-    if (s->pool) {
-        cudaSetDevice(s->device);
-        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &s->pool_threshold_before);
-        cudaMemPoolTrimTo(s->pool, 0);  // hand the cached memory back
-    }
+    for (Idle &d : s->idle) jv_close(d.ctx);
+    s->idle.clear();
+    if (s->threshold_set) pool_threshold_close(s->device);
     delete s;
     return JV_OK;
 }

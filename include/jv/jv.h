@@ -146,6 +146,15 @@ jv_status jv_read_argfile(const char *proj_path, jv_argfile *out);
  * jarvis_device_geometry_meat.hpp:65-128).  Shots keep their input index. */
 jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_recv, const float *recv_xyz);
 
+/* Replaces the context's model with vp, vs, rho (host, gridphy, x fastest)
+ * of the same grid: the extension into the absorbing layers and lambda, mu
+ * are recomputed as jv_create does (elasticGeoModel<global>::initialize,
+ * FD/fdtd3d_0_base_module/fdtd3d_base_3_geomodel_meat.hpp:405-489).  Device
+ * buffers, tensor maps and captured time-loop graphs are kept, so a context
+ * serves many models of one grid without being created again (the request
+ * server's context pool does this).  The image stacks are not touched. */
+jv_status jv_set_model(jv_ctx *c, const float *vp, const float *vs, const float *rho);
+
 /* Sizes of the context's problem. */
 typedef struct jv_info {
     jv_grid grid;
@@ -293,13 +302,19 @@ jv_status jv_cancel(jv_ctx *c, long long id);
 
 /* Requests and the server: a request is one shot of forward modelling or
  * RTM on a model and grid of its own.  jv_server keeps a queue and `slots`
- * worker threads; a worker takes the first queued request whose device
- * footprint (jv_footprint) fits the memory still free under the server's
- * budget, runs it on a context of its own and releases it, so requests of
- * different sizes run concurrently on the GPU as slots and memory come
- * free.  A request's result does not depend on what else runs.  The
- * reference has no counterpart.  Host buffers named in a request must stay
- * valid until it ends. */
+ * worker threads; a worker takes the first queued request it can place --
+ * on an idle pooled context of the same shape (grid, spacing, dt, fm, nt,
+ * rec_width, precision, kind, receiver count), or on a new context whose
+ * device footprint (jv_footprint) fits the memory still free under the
+ * server's budget once idle pooled contexts are released, least recently
+ * used first.  After the request the context stays pooled: the next request
+ * of its shape only uploads its model (jv_set_model) and geometry.  So
+ * requests of different sizes run concurrently on the GPU as slots and
+ * memory come free.  A request's result does not depend on what else runs,
+ * nor on whether its context was pooled.  The server answers poll/wait for
+ * the latest 65536 ended requests; older ids are forgotten (JV_EINVAL).
+ * The reference has no counterpart.  Host buffers named in a request must
+ * stay valid until it ends. */
 typedef struct jv_request {
     int kind;                   /* JV_JOB_FORWARD or JV_JOB_RTM                      */
     jv_grid grid;
@@ -323,7 +338,9 @@ typedef struct jv_server jv_server;
 typedef struct jv_server_stats {
     long long submitted, completed, failed, cancelled, running, queued;
     double p50_ms, p99_ms, mean_ms; /* submission to completion, over the latest 65536 completed */
-    size_t bytes_in_use, budget;
+    size_t bytes_in_use, budget;    /* running requests and pooled idle contexts */
+    long long reused;               /* requests that ran on a pooled context      */
+    long long pooled;               /* idle contexts pooled now                   */
 } jv_server_stats;
 /* Device bytes a context holds for one request of this size with n_recv
  * receivers and an FP32 boundary store (an estimate from the layout; the
@@ -365,11 +382,14 @@ jv_status jv_profile_entry(const jv_ctx *c, int idx, const char **name, double *
  * from one 64 MiB array compiled into the library, held on every device that
  * loads it; problems that need more are rejected with JV_EINVAL (the
  * limit is about 0.5 M cells of gridext, e.g. a 60^3 interior with a 10-cell
- * absorbing layer).  The first call on a device looks up that
- * array's address.  All calls share
- * the array: calls whose GPU work overlaps race; the call clears what must
- * start at zero and returns after its work on `stream` (cudaStream_t, NULL
- * for the legacy stream) has finished. */
+ * absorbing layer).  The first call on a device (and again after the
+ * device's context was replaced, e.g. by cudaDeviceReset) sets up: it looks
+ * up that array's address and uploads the constant finite-difference
+ * coefficients, which synchronises the device, so make that first call
+ * before any stream capture.  All calls share the array: calls whose GPU
+ * work overlaps race; the call clears what must start at zero and returns
+ * after its work on `stream` (cudaStream_t, NULL for the legacy stream) has
+ * finished, on failure as well. */
 jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, const float *d_vs, const float *d_rho, float dt,
                              float fm, int nt, const float *src_xyz, int n_recv, const float *recv_xyz, float *d_vx,
                              float *d_vy, float *d_vz, int *n_kept, void *stream);

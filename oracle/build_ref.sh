@@ -28,10 +28,11 @@
 #     -- also save Ip_fd and the ps/sp/ss images (the reference saves only
 #     image_pp and its Laplacian).
 #
-# Usage: oracle/build_ref.sh [rec_width ...]   (default: 1 4)
+# Usage: [JV_REFERENCE_ROOT=<reference checkout>] oracle/build_ref.sh [rec_width ...]   (default: 1 4)
 set -euo pipefail
-REF=${JV_REFERENCE_ROOT:-/root/reference}
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+# the reference checkout: JV_REFERENCE_ROOT, else a sibling of this repository
+REF=${JV_REFERENCE_ROOT:-$(cd "$HERE/../.." && pwd)/reference}
 OUT="$HERE/_ref"
 WIDTHS=("$@")
 if [ ${#WIDTHS[@]} -eq 0 ]; then WIDTHS=(1 4); fi

@@ -36,7 +36,8 @@ def test_reference_arm_line_on_a_small_problem():
 
 def test_reference_arm_is_rank_zero_only():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2")
-    r = _run("--impl", "reference", "--n", "16", "--nt", "20", "--steps", "1", "--warmup", "3", env=env)
+    r = _run("--impl", "reference", "--gpus", "2", "--n", "16", "--nt", "20", "--steps", "1", "--warmup", "3",
+             env=env)
     assert r.returncode == 0 and r.stdout.strip() == ""
 
 
@@ -74,3 +75,23 @@ def test_reference_arm_on_a_non_cubic_grid():
     assert r.returncode == 0, r.stderr
     d = json.loads([ln for ln in r.stdout.splitlines() if ln.strip()][0])
     assert d["config"]["grid_phy"] == [24, 16, 12] and d["config"]["pml"] == 20 and d["value"] > 0
+
+
+def test_gpus_n_starts_n_ranks_that_shard_the_shots():
+    """--gpus 2 without a launcher starts two ranks itself (gloo on CPU with
+    --dry-run); each takes its round-robin share of the job's shots and
+    rank 0 alone prints one line with the real world size."""
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    r = _run("--gpus", "2", "--dry-run", "--steps", "3", "--warmup", "3", env=env)
+    assert r.returncode == 0, r.stderr
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["shots"] == 6
+    assert d["shards"] == [[0, 2, 4], [1, 3, 5]]
+
+
+def test_gpus_and_launcher_world_size_must_agree():
+    env = dict(os.environ, WORLD_SIZE="2", RANK="0")
+    r = _run("--gpus", "1", "--dry-run", "--steps", "1", "--warmup", "3", env=env)
+    assert r.returncode == 2 and "WORLD_SIZE=2" in r.stderr

@@ -3,6 +3,7 @@ models and kinds admitted into concurrent slots give the same traces and
 images as each request run alone on a context of its own; the HBM budget
 holds while they run; queued requests can be cancelled; the statistics
 count what happened.  Every wait here is a host wait with a time limit."""
+import dataclasses
 import time
 
 import numpy as np
@@ -59,8 +60,58 @@ def test_mixed_requests_match_each_run_alone():
     for (s, kind, _), (_, got), w in zip(plan, subs, want):
         _check_same(kind, got, w)
     assert st["submitted"] == 6 and st["completed"] == 6 and st["failed"] == 0
-    assert st["running"] == 0 and st["queued"] == 0 and st["bytes_in_use"] == 0
+    assert st["running"] == 0 and st["queued"] == 0
+    assert 0 < st["bytes_in_use"] <= st["budget"] and st["pooled"] >= 1  # idle contexts stay pooled
     assert 0 < st["p50_ms"] <= st["p99_ms"] and st["mean_ms"] > 0
+
+
+def _same_grid_models(k):
+    """k problems of one grid and geometry with models of their own."""
+    base = synth.small_case(n=(22, 20, 16), pml=6, nt=70, seed=60, shot_idx=[(11, 10, 2)])
+    out = []
+    for q in range(k):
+        vp, vs, rho = synth.gardner(synth.layered_vp(base.nx, base.ny, base.nz, 61 + q, n_layers=3, vmin=2000,
+                                                     vmax=3000))
+        out.append(dataclasses.replace(base, vp=vp, vs=vs, rho=rho, seed=61 + q))
+    return out
+
+
+def test_pooled_contexts_give_the_results_of_new_ones():
+    """Requests of one shape with different models run on pooled contexts
+    (only the model and geometry are uploaded again): each result equals
+    that of a new context of its own, the 16-bit-store requests included,
+    and the server counts the reuse."""
+    models = _same_grid_models(4)
+    plan = [(m, k, p) for m in models for k, p in ((jv.JOB_RTM, jv.JV_FP32), (jv.JOB_FORWARD, jv.JV_FP32),
+                                                   (jv.JOB_RTM, jv.JV_FP16))]
+    want = [_alone(m, k, precision=p) for m, k, p in plan]
+    with jv.Server(slots=2, budget=1 << 30) as srv:
+        subs = [srv.submit_survey(k, m, precision=p) for m, k, p in plan]
+        for rid, _ in subs:
+            assert srv.wait(rid, timeout=180.0) == jv.JV_OK
+        st = srv.stats()
+    for (m, k, _), (_, got), w in zip(plan, subs, want):
+        _check_same(k, got, w)
+    # three shapes (RTM FP32, forward, RTM FP16), at most two contexts of each
+    assert st["reused"] >= len(plan) - 6 and st["pooled"] <= 6
+
+
+def test_idle_contexts_give_way_to_other_shapes():
+    """A budget that holds one context at a time: alternating shapes must
+    release the idle pooled context of the other shape before creating
+    their own, and every result is still that of a context of its own."""
+    a = _cases()[0]
+    b = _cases()[2]
+    fa = jv.footprint(a.nx, a.ny, a.nz, a.pml, a.nt, a.rec_width, jv.JOB_RTM, n_recv=len(a.recvs))
+    fb = jv.footprint(b.nx, b.ny, b.nz, b.pml, b.nt, b.rec_width, jv.JOB_RTM, n_recv=len(b.recvs))
+    want = {id(a): _alone(a, jv.JOB_RTM), id(b): _alone(b, jv.JOB_RTM)}
+    with jv.Server(slots=2, budget=max(fa, fb) + min(fa, fb) // 2) as srv:
+        for s in (a, b, a, b, a):
+            rid, got = srv.submit_survey(jv.JOB_RTM, s)
+            assert srv.wait(rid, timeout=180.0) == jv.JV_OK
+            _check_same(jv.JOB_RTM, got, want[id(s)])
+            st = srv.stats()
+            assert st["pooled"] == 1 and st["bytes_in_use"] <= st["budget"]
 
 
 @pytest.mark.parametrize("precision", [jv.JV_FP16, jv.JV_BF16])

@@ -10,7 +10,8 @@ failure has already run every other test.
 Checked here, through the C ABI: two calls in a row give the traces of the
 allocating context path (jv_create + jv_forward) within the trace tolerance
 of the parity tests (2e-5 relative L2), the second call leaves the device's
-free memory unchanged, and a problem too large for the array is refused.
+free memory unchanged, the same holds on a caller's non-blocking stream, and
+a problem too large for the array is refused.
 """
 import ctypes as C
 
@@ -61,6 +62,28 @@ def test_noalloc_matches_context_path_on_two_calls(synth):
         assert nkept.value == ref[0].shape[0]
         if call == 1:
             assert free1 == free0, (free0, free1)
+        got = out[:, :nkept.value].cpu().numpy()
+        for a, b in zip(got, ref):
+            assert np.all(np.isfinite(a))
+            assert rel_l2(a, b) <= 2e-5, (call, rel_l2(a, b))
+
+
+def test_noalloc_on_a_non_blocking_stream(synth):
+    """The copies, clears and kernels all go on the caller's stream: on a
+    non-blocking stream (no implicit ordering with the legacy stream) the
+    traces still match the context path, on two calls in a row."""
+    import torch
+
+    s = synth.small_case(n=(36, 32, 28), pml=8, nt=160, seed=33, nrec=40)
+    with jv.Context.from_survey(s) as ctx:
+        ref = ctx.forward(0)
+    out = torch.empty((3, s.recvs.shape[0], s.nt), dtype=torch.float32, device="cuda:0")
+    nkept = C.c_int(-1)
+    st = torch.cuda.Stream(device=0)
+    for call in range(2):
+        out.fill_(float("nan"))
+        rc = _run(s, out, nkept, stream=C.c_void_p(st.cuda_stream))
+        assert rc == jv.JV_OK, jv.lib().jv_last_error()
         got = out[:, :nkept.value].cpu().numpy()
         for a, b in zip(got, ref):
             assert np.all(np.isfinite(a))
