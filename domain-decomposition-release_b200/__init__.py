@@ -47,7 +47,7 @@ EXPORTS = (
     "jv_image_set", "jv_image_set_device", "jv_run_project_shard", "jv_read_argfile", "jv_rtm_batch",
     "jv_submit", "jv_poll", "jv_wait", "jv_cancel",
     "jv_footprint", "jv_server_create", "jv_server_submit", "jv_server_poll", "jv_server_wait", "jv_server_cancel",
-    "jv_server_get_stats", "jv_server_close",
+    "jv_server_get_stats", "jv_server_close", "jv_frame_make", "jv_fld_write", "jv_fld_read", "jv_raw_read",
 )
 JOB_FORWARD, JOB_RTM = 0, 1
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELLED = 0, 1, 2, 3
@@ -101,7 +101,42 @@ class ArgFileC(C.Structure):
                 ("output_path", C.c_char * 1024), ("is_output", C.c_int), ("t_snap", C.c_int), ("pml_num", C.c_int),
                 ("fm", C.c_float), ("dt", C.c_float), ("T", C.c_float), ("x_divide_num", C.c_int),
                 ("y_divide_num", C.c_int), ("z_divide_num", C.c_int), ("slots_per_node", C.c_int),
-                ("rec_width", C.c_int)]
+                ("rec_width", C.c_int), ("vp_path", C.c_char * 1024), ("vs_path", C.c_char * 1024),
+                ("rho_path", C.c_char * 1024), ("n_rows", C.c_int), ("n_cols", C.c_int), ("n_slices", C.c_int),
+                ("d_rows", C.c_float), ("d_cols", C.c_float), ("d_slices", C.c_float), ("save_fld", C.c_int)]
+
+
+class Frame(C.Structure):
+    """The reference's Frame as it lies in memory (jv_frame; a .fld header)."""
+    _fields_ = [("n_elem", C.c_uint64), ("n_rows", C.c_uint64), ("n_elem_slice", C.c_uint64),
+                ("n_cols", C.c_uint32), ("n_slices", C.c_uint32),
+                ("d_rows", C.c_float), ("d_cols", C.c_float), ("d_slices", C.c_float),
+                ("l_rows", C.c_float), ("l_cols", C.c_float), ("l_slices", C.c_float),
+                ("r_rows", C.c_float), ("r_cols", C.c_float), ("r_slices", C.c_float), ("type", C.c_int32)]
+
+
+def make_frame(n_rows, n_cols=1, n_slices=1, d=(0.0, 0.0, 0.0), l=(0.0, 0.0, 0.0)) -> Frame:
+    f = Frame()
+    lib().jv_frame_make(n_rows, n_cols, n_slices, d[0], d[1], d[2], l[0], l[1], l[2], C.byref(f))
+    return f
+
+
+def fld_write(path_noext: str, frame: Frame, data: np.ndarray) -> str:
+    """Field::save(.., binary_fld) through libjv: path_noext + '.fld'."""
+    a = np.ascontiguousarray(data, dtype=np.float32)
+    if a.size != frame.n_elem:
+        raise JvError(JV_EINVAL, "data size does not match the frame")
+    _check(lib().jv_fld_write(path_noext.encode(), C.byref(frame), _fptr(a)))
+    return path_noext + ".fld"
+
+
+def fld_read(path: str):
+    """(Frame, float32 array (n_slices, n_cols, n_rows)) of a .fld file."""
+    f = Frame()
+    _check(lib().jv_fld_read(path.encode(), C.byref(f), None, 0))
+    a = np.empty(int(f.n_elem), np.float32)
+    _check(lib().jv_fld_read(path.encode(), C.byref(f), _fptr(a), a.size))
+    return f, a.reshape(int(f.n_slices), int(f.n_cols), int(f.n_rows))
 
 
 def read_argfile(proj_path: str) -> dict:
@@ -182,6 +217,11 @@ def lib() -> C.CDLL:
     L.jv_read_argfile.argtypes = [C.c_char_p, C.POINTER(ArgFileC)]
     L.jv_forward_noalloc.argtypes = [C.POINTER(Grid), vp, vp, vp, C.c_float, C.c_float, C.c_int, fp, C.c_int, fp,
                                      vp, vp, vp, C.POINTER(C.c_int), vp]
+    L.jv_frame_make.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32] + [C.c_float] * 6 + [C.POINTER(Frame)]
+    L.jv_frame_make.restype = None
+    L.jv_fld_write.argtypes = [C.c_char_p, C.POINTER(Frame), fp]
+    L.jv_fld_read.argtypes = [C.c_char_p, C.POINTER(Frame), fp, C.c_size_t]
+    L.jv_raw_read.argtypes = [C.c_char_p, C.c_size_t, fp]
     L.jv_last_timing.argtypes = [ctxp, dp]
     L.jv_sync.argtypes = [ctxp]
     L.jv_close.argtypes = [ctxp]
@@ -190,7 +230,7 @@ def lib() -> C.CDLL:
     L.jv_build_info.argtypes = []
     L.jv_build_info.restype = C.c_char_p
     for n in EXPORTS:
-        if n not in ("jv_options_default", "jv_last_error", "jv_build_info"):
+        if n not in ("jv_options_default", "jv_last_error", "jv_build_info", "jv_frame_make"):
             getattr(L, n).restype = C.c_int
     _lib = L
     return L

@@ -19,6 +19,9 @@
 #include "jv/jv.h"
 #include "project_io.hpp"
 
+// the .fld header is the reference's Frame struct as x86-64 lays it out
+static_assert(sizeof(jv_frame) == 72, "jv_frame must match the reference Frame's 72 bytes");
+
 namespace {
 thread_local std::string g_err;
 
@@ -212,7 +215,7 @@ jv_status jv_open(const char *proj_path, const jv_options *opt, jv_ctx **out) {
     if (a.x_divide_num > 1 || a.y_divide_num > 1 || a.z_divide_num > 1)
         return fail(JV_EINVAL, "x/y/z_divide_num must be 1: the whole model is resident on one GPU");
     jv::GmsModel g;
-    m = jv::read_gms(a.model_path, &g);
+    m = a.vp_path.empty() ? jv::read_gms(a.model_path, &g) : jv::read_raw_model(a, &g);
     if (!m.empty()) return fail(JV_EIO, m);
     std::vector<float> shots, recvs;
     m = jv::read_points(a.shot_path, &shots);
@@ -265,6 +268,93 @@ jv_status jv_read_argfile(const char *proj_path, jv_argfile *out) {
     out->z_divide_num = a.z_divide_num;
     out->slots_per_node = a.slots_per_node;
     out->rec_width = a.rec_width;
+    const std::string *rsrc[3] = {&a.vp_path, &a.vs_path, &a.rho_path};
+    char *rdst[3] = {out->vp_path, out->vs_path, out->rho_path};
+    for (int q = 0; q < 3; q++) {
+        if (rsrc[q]->size() >= sizeof(out->vp_path)) return fail(JV_EINVAL, "path too long: " + *rsrc[q]);
+        std::memcpy(rdst[q], rsrc[q]->c_str(), rsrc[q]->size() + 1);
+    }
+    out->n_rows = a.n_rows;
+    out->n_cols = a.n_cols;
+    out->n_slices = a.n_slices;
+    out->d_rows = a.d_rows;
+    out->d_cols = a.d_cols;
+    out->d_slices = a.d_slices;
+    out->save_fld = a.save_fld ? 1 : 0;
+    g_err.clear();
+    return JV_OK;
+}
+
+void jv_frame_make(uint64_t n_rows, uint32_t n_cols, uint32_t n_slices, float d_rows, float d_cols, float d_slices,
+                   float l_rows, float l_cols, float l_slices, jv_frame *f) {
+    if (!f) return;
+    std::memset(f, 0, sizeof(*f));
+    f->n_rows = n_rows;
+    f->n_cols = n_cols;
+    f->n_slices = n_slices;
+    f->n_elem_slice = n_rows * n_cols;
+    f->n_elem = n_rows * n_cols * n_slices;
+    f->d_rows = d_rows; f->d_cols = d_cols; f->d_slices = d_slices;
+    f->l_rows = l_rows; f->l_cols = l_cols; f->l_slices = l_slices;
+    // an empty axis has l = r = 0
+    if (n_rows > 0) f->r_rows = l_rows + (float)(n_rows - 1) * d_rows; else f->l_rows = 0.f;
+    if (n_cols > 0) f->r_cols = l_cols + (float)(n_cols - 1) * d_cols; else f->l_cols = 0.f;
+    if (n_slices > 0) f->r_slices = l_slices + (float)(n_slices - 1) * d_slices; else f->l_slices = 0.f;
+    // Frame::Type: with a spacing the frame is a line/mesh/grid, else a vec/mat/cube
+    const bool spaced = d_rows > 0 || d_cols > 0 || d_slices > 0;
+    const bool one_axis = (n_rows == 1 && n_cols == 1) || (n_rows == 1 && n_slices == 1) || (n_cols == 1 && n_slices == 1);
+    const bool two_axes = (n_rows > 1 && n_cols > 1 && n_slices == 1) || (n_rows > 1 && n_slices > 1 && n_cols == 1) ||
+                          (n_cols > 1 && n_slices > 1 && n_rows == 1);
+    const bool three_axes = n_rows > 1 && n_cols > 1 && n_slices > 1;
+    if (one_axis) f->type = spaced ? 10 : 1;
+    else if (two_axes) f->type = spaced ? 20 : 2;
+    else if (three_axes) f->type = spaced ? 30 : 3;
+}
+
+jv_status jv_fld_write(const char *path_noext, const jv_frame *f, const float *data) {
+    if (!path_noext || !f || (f->n_elem && !data)) return fail(JV_EINVAL, "jv_fld_write: NULL argument");
+    const std::string path = std::string(path_noext) + ".fld";
+    FILE *fp = std::fopen(path.c_str(), "wb");
+    if (!fp) return fail(JV_EIO, "cannot create " + path);
+    bool ok = std::fwrite(f, sizeof(*f), 1, fp) == 1;
+    if (ok && f->n_elem) ok = std::fwrite(data, sizeof(float), (size_t)f->n_elem, fp) == (size_t)f->n_elem;
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(JV_EIO, "short write " + path);
+    g_err.clear();
+    return JV_OK;
+}
+
+jv_status jv_fld_read(const char *path, jv_frame *f, float *data, size_t capacity) {
+    if (!path || !f) return fail(JV_EINVAL, "jv_fld_read: NULL argument");
+    const std::string p(path);
+    if (p.size() < 4 || p.compare(p.size() - 4, 4, ".fld") != 0) return fail(JV_EINVAL, p + ": not a .fld file");
+    FILE *fp = std::fopen(path, "rb");
+    if (!fp) return fail(JV_EIO, "cannot open " + p);
+    jv_frame h;
+    if (std::fread(&h, sizeof(h), 1, fp) != 1 || h.n_elem != h.n_rows * h.n_cols * h.n_slices) {
+        std::fclose(fp);
+        return fail(JV_EIO, p + ": bad frame header");
+    }
+    *f = h;
+    if (data) {
+        if (capacity < h.n_elem) {
+            std::fclose(fp);
+            return fail(JV_EINVAL, p + ": " + std::to_string(h.n_elem) + " values do not fit the buffer");
+        }
+        if (std::fread(data, sizeof(float), (size_t)h.n_elem, fp) != (size_t)h.n_elem) {
+            std::fclose(fp);
+            return fail(JV_EIO, p + ": truncated data");
+        }
+    }
+    std::fclose(fp);
+    g_err.clear();
+    return JV_OK;
+}
+
+jv_status jv_raw_read(const char *path, size_t n, float *data) {
+    if (!path || (n && !data)) return fail(JV_EINVAL, "jv_raw_read: NULL argument");
+    std::string m = jv::read_raw(path, data, n);
+    if (!m.empty()) return fail(JV_EIO, m);
     g_err.clear();
     return JV_OK;
 }
@@ -587,9 +677,16 @@ jv_status jv_run_project_shard(jv_ctx *c, int rank, int world, jv_reduce_fn redu
     const std::string suf = jv::size_info(inf.grid.nx, inf.grid.ny, inf.grid.nz, 0.f, 0.f, 0.f) + ".raw";
     const char *names[6] = {"image_pp_0", "image_pp_laplace_0", "image_ps_0", "image_sp_0", "image_ss_0", nullptr};
     const float *srcs[5] = {o[0], o[4], o[1], o[2], o[3]};
+    jv_frame fr;
+    jv_frame_make((uint64_t)inf.grid.nx, (uint32_t)inf.grid.ny, (uint32_t)inf.grid.nz, inf.grid.dx, inf.grid.dy,
+                  inf.grid.dz, 0.f, 0.f, 0.f, &fr);
     for (int q = 0; q < 5; q++) {
         std::string m = jv::write_raw(c->arg.output_path + names[q] + suf, srcs[q], n);
         if (!m.empty()) return fail(JV_EIO, m);
+        if (c->arg.save_fld) {
+            st = jv_fld_write((c->arg.output_path + names[q]).c_str(), &fr, srcs[q]);
+            if (st != JV_OK) return st;
+        }
     }
     // source illumination, as a float raw image
     std::vector<double> ip(n);
@@ -598,6 +695,7 @@ jv_status jv_run_project_shard(jv_ctx *c, int rank, int world, jv_reduce_fn redu
     std::vector<float> ipf(ip.begin(), ip.end());
     std::string m = jv::write_raw(c->arg.output_path + "image_ipfd_0" + suf, ipf.data(), n);
     if (!m.empty()) return fail(JV_EIO, m);
+    if (c->arg.save_fld) return jv_fld_write((c->arg.output_path + "image_ipfd_0").c_str(), &fr, ipf.data());
     return JV_OK;
 }
 

@@ -194,6 +194,54 @@ std::string read_argfile(const std::string &proj_path_in, ArgFile *a) {
     a->is_output = io != m.end() && io->second.kind == JsonVal::kBool && io->second.b;
     a->rec_width = gi("rec_width", 0);
     a->precision = gs("precision");
+    if (!gs("vp_path").empty()) {
+        a->vp_path = proj + gs("vp_path");
+        a->vs_path = proj + gs("vs_path");
+        a->rho_path = proj + gs("rho_path");
+        a->n_rows = gi("n_rows", 0);
+        a->n_cols = gi("n_cols", 0);
+        a->n_slices = gi("n_slices", 0);
+        a->d_rows = gf("d_rows");
+        a->d_cols = gf("d_cols");
+        a->d_slices = gf("d_slices");
+        if (a->n_rows <= 0 || a->n_cols <= 0 || a->n_slices <= 0 || !(a->d_rows > 0) || !(a->d_cols > 0) ||
+            !(a->d_slices > 0))
+            return "argfile.json: a raw model (vp_path) needs n_rows, n_cols, n_slices > 0 and d_rows, d_cols, "
+                   "d_slices > 0";
+    }
+    auto sf = m.find("save_fld");
+    a->save_fld = sf != m.end() && sf->second.kind == JsonVal::kBool && sf->second.b;
+    return "";
+}
+
+std::string read_raw(const std::string &path, float *out, size_t n) {
+    FILE *fp = std::fopen(path.c_str(), "rb");
+    if (!fp) return "raw file open error: " + path;
+    std::fseek(fp, 0, SEEK_END);
+    const long long bytes = std::ftell(fp);
+    std::fseek(fp, 0, SEEK_SET);
+    if (bytes != (long long)(n * sizeof(float))) {
+        std::fclose(fp);
+        return path + ": " + std::to_string(bytes) + " bytes, the frame needs " + std::to_string(n * sizeof(float));
+    }
+    const size_t r = std::fread(out, sizeof(float), n, fp);
+    std::fclose(fp);
+    return r == n ? "" : path + ": short read";
+}
+
+std::string read_raw_model(const ArgFile &a, GmsModel *m) {
+    m->nx = a.n_rows;
+    m->ny = a.n_cols;
+    m->nz = a.n_slices;
+    m->dx = a.d_rows; m->dy = a.d_cols; m->dz = a.d_slices;
+    m->lx = m->ly = m->lz = 0.f;
+    const size_t n = (size_t)m->nx * m->ny * m->nz;
+    m->params.assign(3, std::vector<float>(n));
+    const std::string *paths[3] = {&a.vp_path, &a.vs_path, &a.rho_path};
+    for (int q = 0; q < 3; q++) {
+        std::string e = read_raw(*paths[q], m->params[q].data(), n);
+        if (!e.empty()) return e;
+    }
     return "";
 }
 

@@ -10,6 +10,11 @@
 //                (.jarvis_0_meta/.jarvis_2_field/jarvis_1_host_field_meat.hpp:159-197)
 //  images        raw float32 with Frame::size_info() in the name
 //                (.jarvis_0_meta/.jarvis_2_field/jarvis_0_frame_meat.hpp:347-351)
+//  raw models    one float32 file per parameter, x fastest, with its Frame given
+//                by the caller (host_single_field::read_raw,
+//                .jarvis_0_meta/.jarvis_2_field/jarvis_1_host_field_meat.hpp:65-79)
+//  .fld fields   the Frame struct's bytes, then the data
+//                (save_as_binary_fld / load, jarvis_1_host_field_meat.hpp:41-64,81-89)
 // (FD = src/jarvis_cpp/jarvis/.jarvis_2_app/.jarvis_3_seismology/elastic_1_fdtd3d_model_mpi)
 #pragma once
 
@@ -27,6 +32,13 @@ struct ArgFile {
     bool is_output = false;
     int rec_width = 0;       // optional key (0: not given)
     std::string precision;   // optional key
+    // optional raw model: vp/vs/rho files (prefixed with proj_path) on the
+    // Frame n_rows x n_cols x n_slices, d_rows/d_cols/d_slices; when vp_path
+    // is given, model_path is not read
+    std::string vp_path, vs_path, rho_path;
+    int n_rows = 0, n_cols = 0, n_slices = 0;
+    float d_rows = 0.f, d_cols = 0.f, d_slices = 0.f;
+    bool save_fld = false;   // optional key: also write the images as .fld
 };
 
 // Parses proj_path + "argfile.json".  Returns "" on success, else a message.
@@ -39,6 +51,11 @@ struct GmsModel {
     std::vector<std::vector<float>> params;  // each nx*ny*nz, x fastest
 };
 std::string read_gms(const std::string &path, GmsModel *m);
+
+// a raw model (vp, vs, rho files of nx*ny*nz floats, x fastest)
+std::string read_raw_model(const ArgFile &a, GmsModel *m);
+// exactly n floats from a raw file
+std::string read_raw(const std::string &path, float *out, size_t n);
 
 std::string size_info(int nx, int ny, int nz, float lx, float ly, float lz);
 std::string write_traces(const std::string &path_noext, const float *tr, int nrec, int nt);

@@ -14,6 +14,14 @@
   data with z fastest, then x, then y (src/jarvis_cpp/jarvis/.jarvis_1_util/
   .jarvis_0_gms/jarvis_device_gms_meat.hpp:11-79).  Parameters in order
   vp, vs, rho.
+* raw models -- one float32 file per parameter (vp, vs, rho), x fastest, on
+  a Frame the argfile gives (optional keys vp_path, vs_path, rho_path,
+  n_rows, n_cols, n_slices, d_rows, d_cols, d_slices), in place of the
+  reference's edit of its loader to call Field::read_raw
+  (src/jarvis_cpp/jarvis/.jarvis_0_meta/.jarvis_2_field/
+  jarvis_1_host_field_meat.hpp:65-79; README.md:131-144).
+* .fld -- the reference Frame struct's 72 bytes, then the float32 data
+  (save_as_binary_fld, jarvis_1_host_field_meat.hpp:81-89).
 * traces -- ``%10.6e\t`` per sample, one line per receiver
   (src/jarvis_cpp/jarvis/.jarvis_0_meta/.jarvis_2_field/
   jarvis_1_host_field_meat.hpp:159-197); images -- raw float32, x fastest,
@@ -178,16 +186,82 @@ def read_gms(path: str):
     return out, {"nx": nx, "ny": ny, "nz": nz, "dx": dx, "dy": dy, "dz": dz, "lx": lx, "ly": ly, "lz": lz}
 
 
-def write_project(proj_path: str, s, *, model_name: str = "model.gms", rec_width_key: bool = True) -> None:
-    """Writes argfile.json, shot.txt, rece.txt and the GMS model of a
-    synth.Survey into proj_path (creating proj_path/out/)."""
+def write_project(proj_path: str, s, *, model_name: str = "model.gms", rec_width_key: bool = True,
+                  raw_model: bool = False, save_fld: bool = False) -> None:
+    """Writes argfile.json, shot.txt, rece.txt and the model of a
+    synth.Survey into proj_path (creating proj_path/out/): a GMS file, or
+    with raw_model three raw float32 files (vp.raw, vs.raw, rho.raw, x
+    fastest) named by the raw-model keys.  save_fld asks jv_run_project to
+    write the images as .fld too."""
     os.makedirs(os.path.join(proj_path, "out"), exist_ok=True)
-    write_gms(os.path.join(proj_path, model_name), {"vp": s.vp, "vs": s.vs, "rho": s.rho},
-              d=(s.dx, s.dy, s.dz))
+    extra = {}
+    if raw_model:
+        for nm in ("vp", "vs", "rho"):
+            np.ascontiguousarray(getattr(s, nm), dtype=np.float32).tofile(os.path.join(proj_path, nm + ".raw"))
+            extra[nm + "_path"] = nm + ".raw"
+        extra.update({"n_rows": s.nx, "n_cols": s.ny, "n_slices": s.nz, "d_rows": float(s.dx),
+                      "d_cols": float(s.dy), "d_slices": float(s.dz)})
+        model_name = ""
+    else:
+        write_gms(os.path.join(proj_path, model_name), {"vp": s.vp, "vs": s.vs, "rho": s.rho},
+                  d=(s.dx, s.dy, s.dz))
+    if save_fld:
+        extra["save_fld"] = True
     write_points(os.path.join(proj_path, "shot.txt"), s.shots)
     write_points(os.path.join(proj_path, "rece.txt"), s.recvs)
     write_argfile(proj_path, model_path=model_name, pml_num=s.pml, fm=s.fm, dt=s.dt, T=s.T,
-                  rec_width=s.rec_width if rec_width_key else None)
+                  rec_width=s.rec_width if rec_width_key else None, extra=extra)
+
+
+# Frame (jarvis_0_frame_bones.hpp:9-51) on x86-64: n_elem, n_rows,
+# n_elem_slice (uint64), n_cols, n_slices (uint32), d/l/r of rows, cols,
+# slices (float), type (enum, int32)
+FRAME = struct.Struct("<QQQII9fi")
+assert FRAME.size == 72
+
+
+def frame(nx: int, ny: int = 1, nz: int = 1, d=(0.0, 0.0, 0.0), l=(0.0, 0.0, 0.0)) -> dict:
+    """Frame(nx, ny, nz, d, l) with its derived members and type
+    (jarvis_0_frame_meat.hpp:27-65, set_frame_type :219-241)."""
+    f32 = np.float32
+    d = [f32(v) for v in d]
+    l = [f32(v) for v in l]
+    n = (nx, ny, nz)
+    r = [f32(l[a] + f32(n[a] - 1) * d[a]) if n[a] > 0 else f32(0.0) for a in range(3)]
+    l = [l[a] if n[a] > 0 else f32(0.0) for a in range(3)]
+    spaced = any(v > 0 for v in d)
+    one = (nx == 1 and ny == 1) or (nx == 1 and nz == 1) or (ny == 1 and nz == 1)
+    two = (nx > 1 and ny > 1 and nz == 1) or (nx > 1 and nz > 1 and ny == 1) or (ny > 1 and nz > 1 and nx == 1)
+    three = nx > 1 and ny > 1 and nz > 1
+    t = (10 if spaced else 1) if one else (20 if spaced else 2) if two else (30 if spaced else 3) if three else 0
+    return {"n_elem": nx * ny * nz, "n_rows": nx, "n_elem_slice": nx * ny, "n_cols": ny, "n_slices": nz,
+            "d": d, "l": l, "r": r, "type": t}
+
+
+def write_fld(path_noext: str, a: np.ndarray, d=(0.0, 0.0, 0.0), l=(0.0, 0.0, 0.0)) -> str:
+    """A (nz, ny, nx) float32 field as path_noext + '.fld'."""
+    a = np.asarray(a, dtype=np.float32)
+    nz, ny, nx = a.shape if a.ndim == 3 else (1, 1, a.size)
+    f = frame(nx, ny, nz, d, l)
+    path = path_noext + ".fld"
+    with open(path, "wb") as fh:
+        fh.write(FRAME.pack(f["n_elem"], f["n_rows"], f["n_elem_slice"], f["n_cols"], f["n_slices"], *f["d"], *f["l"],
+                            *f["r"], f["type"]))
+        fh.write(np.ascontiguousarray(a).tobytes())
+    return path
+
+
+def read_fld(path: str):
+    """(frame dict, float32 array (n_slices, n_cols, n_rows)) of a .fld file."""
+    with open(path, "rb") as fh:
+        buf = fh.read()
+    v = FRAME.unpack_from(buf, 0)
+    f = {"n_elem": v[0], "n_rows": v[1], "n_elem_slice": v[2], "n_cols": v[3], "n_slices": v[4],
+         "d": list(v[5:8]), "l": list(v[8:11]), "r": list(v[11:14]), "type": v[14]}
+    if f["n_elem"] != f["n_rows"] * f["n_cols"] * f["n_slices"] or len(buf) != 72 + 4 * f["n_elem"]:
+        raise ValueError(f"{path}: bad .fld header or size")
+    a = np.frombuffer(buf, dtype=np.float32, count=f["n_elem"], offset=72)
+    return f, a.reshape(f["n_slices"], f["n_cols"], f["n_rows"]).copy()
 
 
 def size_info(nx: int, ny: int, nz: int, lx: float = 0.0, ly: float = 0.0, lz: float = 0.0) -> str:

@@ -138,8 +138,46 @@ typedef struct jv_argfile {
     float fm, dt, T;
     int x_divide_num, y_divide_num, z_divide_num, slots_per_node;
     int rec_width;
+    /* optional raw model (no reference key: the reference edits its model
+     * loader to call Field::read_raw with a Frame, README.md:131-144):
+     * vp/vs/rho files of n_rows*n_cols*n_slices float32, x fastest, prefixed
+     * with proj_path; when vp_path is set, jv_open reads them instead of
+     * model_path.  Empty / 0 when absent. */
+    char vp_path[1024];
+    char vs_path[1024];
+    char rho_path[1024];
+    int n_rows, n_cols, n_slices;
+    float d_rows, d_cols, d_slices;
+    int save_fld; /* optional key: jv_run_project also writes the images as .fld */
 } jv_argfile;
 jv_status jv_read_argfile(const char *proj_path, jv_argfile *out);
+
+/* The reference's Frame as it lies in memory (the header of a .fld file):
+ * .jarvis_0_meta/.jarvis_2_field/jarvis_0_frame_bones.hpp:9-51.  n_rows is
+ * the x count (fastest), n_cols y, n_slices z; r = l + (n - 1) d; type is
+ * Frame::Type (0 null, 1 vec, 2 mat, 3 cube, 10 line, 20 mesh, 30 grid). */
+typedef struct jv_frame {
+    uint64_t n_elem, n_rows, n_elem_slice;
+    uint32_t n_cols, n_slices;
+    float d_rows, d_cols, d_slices;
+    float l_rows, l_cols, l_slices;
+    float r_rows, r_cols, r_slices;
+    int32_t type;
+} jv_frame;
+/* Fills *f as Frame(n_rows, n_cols, n_slices, d.., l..) does
+ * (jarvis_0_frame_meat.hpp:27-65, set_frame_type :219-241). */
+void jv_frame_make(uint64_t n_rows, uint32_t n_cols, uint32_t n_slices, float d_rows, float d_cols, float d_slices,
+                   float l_rows, float l_cols, float l_slices, jv_frame *f);
+/* Field::save(.., SaveFormat::binary_fld): path_noext + ".fld", the frame's
+ * bytes then f->n_elem floats (jarvis_1_host_field_meat.hpp:81-89). */
+jv_status jv_fld_write(const char *path_noext, const jv_frame *f, const float *data);
+/* Field::load of a .fld file (jarvis_1_host_field_meat.hpp:41-64): the
+ * frame into *f and, when data is not NULL, its n_elem floats (JV_EINVAL
+ * if capacity, in floats, is smaller). */
+jv_status jv_fld_read(const char *path, jv_frame *f, float *data, size_t capacity);
+/* Field::read_raw (jarvis_1_host_field_meat.hpp:65-79): exactly n float32
+ * values from a raw file (JV_EIO if its size differs). */
+jv_status jv_raw_read(const char *path, size_t n, float *data);
 
 /* Sets the survey: shot and receiver positions (x,y,z metres).  Only the
  * points inside gridphy are kept (SubGeometry::get_sub_shot_and_recv,

@@ -181,9 +181,9 @@ def compare(s, g: dict, o: dict, r: dict) -> dict:
     return res
 
 
-def fixture(s, o: dict, r: dict) -> dict:
-    fx = {"case": np.array(s.name)}
-    if s.name == "cfg1":
+def fixture(name: str, s, o: dict, r: dict) -> dict:
+    fx = {"case": np.array(name)}
+    if name == "cfg1":
         for c, t in zip(("vx", "vy", "vz"), o["traces"]):
             fx[f"oracle_tr_{c}"] = t.astype(np.float32)
         for c, t in zip(("vx", "vy", "vz"), r["traces"]):
@@ -225,7 +225,7 @@ def run_case(name: str, out: str) -> None:
                 "reference_log_tail": r["log_tail"][-600:]})
     with open(os.path.join(out, name + ".json"), "w") as f:
         json.dump(res, f, indent=1)
-    np.savez_compressed(os.path.join(out, f"size_{name}.npz"), **fixture(s, o, r))
+    np.savez_compressed(os.path.join(out, f"size_{name}.npz"), **fixture(name, s, o, r))
     shutil.rmtree(d, ignore_errors=True)
     print(json.dumps({k: res[k] for k in ("case", "traces", "raw_images", "laplacian_pp")}), flush=True)
 

@@ -117,3 +117,25 @@ def test_shard_arguments_checked(tmp_path, project, synth):
             ctx.run_project_shard(2, 2)
         with pytest.raises(jv.JvError):
             ctx.run_project_shard(0, 2)  # several ranks need a reduce function
+
+
+def test_raw_model_project_matches_gms_project(tmp_path, project, synth):
+    """model_path (GMS) and the raw-model keys (vp/vs/rho float32 files, x
+    fastest, with their Frame) give the same job, bit for bit; with
+    save_fld the images are also written as .fld files holding the same
+    values under the reference Frame header."""
+    s = synth.small_case(n=(18, 16, 14), pml=5, nt=60, seed=9, shot_idx=[(5, 6, 2), (11, 8, 3)])
+    dg, dr = str(tmp_path / "gms") + "/", str(tmp_path / "raw") + "/"
+    project.write_project(dg, s)
+    project.write_project(dr, s, raw_model=True, save_fld=True)
+    for d in (dg, dr):
+        with jv.Context.open(d) as ctx:
+            ctx.run_project()
+    a, b = _read_outputs(project, dg, s), _read_outputs(project, dr, s)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    for nm in ("image_pp_0", "image_pp_laplace_0", "image_ps_0", "image_sp_0", "image_ss_0", "image_ipfd_0"):
+        fr, img = project.read_fld(f"{dr}out/{nm}.fld")
+        assert fr["type"] == 30 and (fr["n_rows"], fr["n_cols"], fr["n_slices"]) == (s.nx, s.ny, s.nz)
+        assert fr["d"][0] == np.float32(s.dx) and fr["r"][2] == np.float32((s.nz - 1) * np.float32(s.dz))
+        assert np.array_equal(img.reshape(-1), b[nm]), nm
