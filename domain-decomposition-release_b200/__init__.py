@@ -48,7 +48,10 @@ EXPORTS = (
     "jv_submit", "jv_poll", "jv_wait", "jv_cancel",
     "jv_footprint", "jv_server_create", "jv_server_submit", "jv_server_poll", "jv_server_wait", "jv_server_cancel",
     "jv_server_get_stats", "jv_server_close", "jv_frame_make", "jv_fld_write", "jv_fld_read", "jv_raw_read",
+    "jv_rtm_forward_pass", "jv_rtm_reverse_begin", "jv_rtm_reverse_op", "jv_rtm_reverse_end",
 )
+(OP_INJECT_RECEIVERS, OP_BACKWARD_STRESS, OP_REVERSE_VEL_PML, OP_REVERSE_VEL, OP_INJECT_BOUNDARY_STRESS,
+ OP_BACKWARD_VEL_IMAGE, OP_REVERSE_STRESS_PML, OP_REVERSE_STRESS, OP_INJECT_BOUNDARY_VEL) = range(9)
 JOB_FORWARD, JOB_RTM = 0, 1
 JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELLED = 0, 1, 2, 3
 
@@ -222,6 +225,10 @@ def lib() -> C.CDLL:
     L.jv_fld_write.argtypes = [C.c_char_p, C.POINTER(Frame), fp]
     L.jv_fld_read.argtypes = [C.c_char_p, C.POINTER(Frame), fp, C.c_size_t]
     L.jv_raw_read.argtypes = [C.c_char_p, C.c_size_t, fp]
+    L.jv_rtm_forward_pass.argtypes = [ctxp, C.c_int]
+    L.jv_rtm_reverse_begin.argtypes = [ctxp, C.c_int, vp, vp, vp]
+    L.jv_rtm_reverse_op.argtypes = [ctxp, C.c_int, C.c_int]
+    L.jv_rtm_reverse_end.argtypes = [ctxp]
     L.jv_last_timing.argtypes = [ctxp, dp]
     L.jv_sync.argtypes = [ctxp]
     L.jv_close.argtypes = [ctxp]

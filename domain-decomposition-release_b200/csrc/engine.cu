@@ -682,7 +682,8 @@ Status Engine::check_shot(int shot, long long *src) const {
 }
 
 Status Engine::set_state(int it, long long src, float *const tr[3], const float *const obs[3]) {
-    StepState h{};
+    StepState &h = h_state_;
+    h = StepState{};
     h.it = it;
     h.src = src;
     for (int q = 0; q < 3; q++) {
@@ -969,11 +970,10 @@ Status Engine::forward(int shot, float *d_vx, float *d_vy, float *d_vz) {
     return Status{};
 }
 
-Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
-    JV_CU(cudaSetDevice(dev_));
-    long long src;
-    JV_TRY(check_shot(shot, &src));
-    if (nrec_ > 0 && (!d_ox || !d_oy || !d_oz)) return bad(JV_EINVAL, "observed traces must not be NULL");
+// Device memory the RTM passes need beyond modelling, allocated with the
+// first RTM shot: the receiver wavefield, the FP32 shot image, the VOWR
+// boundary store and the two energies of the reconstruction check.
+Status Engine::rtm_prepare() {
     // lazily allocate the receiver wavefield and the boundary store
     if (!R_.f[0]) {
         void *p;
@@ -1045,32 +1045,115 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
             vowr_.store = store_;
         }
     }
-    const float *obs[3] = {d_ox, d_oy, d_oz};
-    JV_CU(cudaEventRecord(ev0_, stream_));
-    // forward with boundary store (rtm_forward)
-    JV_TRY(zero_wave(F_, kNumFld));
-    JV_TRY(zero_psi(cpF_));
-    JV_TRY(set_state(0, src, nullptr, obs));
-    JV_TRY(run_loop(kStepRtmFwd, nt_));
-    // reconstruction check: the source wavefield's FP64 energy over gridphy
-    // where the reconstruction starts, and what is left of it when the
-    // reverse loop has carried it back to its zero initial state
     if (!energy_d_) {
         void *p;
         JV_TRY(alloc(&p, 2 * sizeof(double)));
         energy_d_ = (double *)p;
     }
+    return Status{};
+}
+
+Status Engine::rtm_forward_pass(int shot) {
+    JV_CU(cudaSetDevice(dev_));
+    long long src;
+    JV_TRY(check_shot(shot, &src));
+    JV_TRY(rtm_prepare());
+    // forward with boundary store (rtm_forward)
+    JV_TRY(zero_wave(F_, kNumFld));
+    JV_TRY(zero_psi(cpF_));
+    JV_TRY(set_state(0, src, nullptr, nullptr));
+    JV_TRY(run_loop(kStepRtmFwd, nt_));
+    // reconstruction check: the source wavefield's FP64 energy over gridphy
+    // where the reconstruction starts (and, at the end of the reverse loop,
+    // what is left of it once carried back to its zero initial state)
     JV_CU(cudaMemsetAsync(energy_d_, 0, 2 * sizeof(double), stream_));
     JV_K(k_wave_energy(g_, F_, energy_d_, stream_));
+    fwd_shot_ = shot;
+    return Status{};
+}
+
+Status Engine::rtm_reverse_begin(int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
+    JV_CU(cudaSetDevice(dev_));
+    long long src;
+    JV_TRY(check_shot(shot, &src));
+    if (nrec_ > 0 && (!d_ox || !d_oy || !d_oz)) return bad(JV_EINVAL, "observed traces must not be NULL");
+    if (fwd_shot_ != shot) return bad(JV_ESTATE, "the time-reverse loop needs the forward pass of the same shot first");
+    const float *obs[3] = {d_ox, d_oy, d_oz};
     // time reverse: backward (reconstruction) + reverse (receivers) + image
     JV_TRY(zero_wave(R_, kNumFld));
     JV_TRY(zero_psi(cpR_));
     JV_TRY(set_state(nt_ - 1, src, nullptr, obs));
     JV_CU(cudaMemsetAsync(shot_img_.ip, 0, 5 * shot_img_pitch_ * sizeof(float), stream_));
-    JV_TRY(run_loop(kStepRtmRev, nt_));
+    rev_open_ = true;
+    return Status{};
+}
+
+// One kernel of the time-reverse loop at time index `it` (for the boundary
+// replays, the index of the record replayed), launched directly; the loop
+// of rtm_shot launches the same kernels per step (launch_step kStepRtmRev).
+Status Engine::rtm_reverse_op(int op, int it) {
+    if (!rev_open_) return bad(JV_ESTATE, "no time-reverse loop is open (jv_rtm_reverse_begin)");
+    JV_CU(cudaSetDevice(dev_));
+    h_state_.it = it;
+    JV_CU(cudaMemcpyAsync(st_, &h_state_, sizeof(h_state_), cudaMemcpyHostToDevice, stream_));
+    void *s = (void *)stream_;
+    const float dt = dt_;
+    const int rw = opt_.rec_width;
+    switch (op) {
+    case JV_OP_INJECT_RECEIVERS: JV_K(k_inject_rec(R_, rec_d_, nrec_, nt_, st_, 0, s)); break;
+    case JV_OP_BACKWARD_STRESS:
+        JV_K(k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, 0, kc_, s, &mapsF_));
+        break;
+    case JV_OP_REVERSE_VEL_PML: JV_K(k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s)); break;
+    case JV_OP_REVERSE_VEL: JV_K(k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s)); break;
+    case JV_OP_INJECT_BOUNDARY_STRESS: JV_K(k_vowr(g_, F_, vowr_, st_, 0, 0, 2, s)); break;
+    case JV_OP_BACKWARD_VEL_IMAGE: JV_K(k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s)); break;
+    case JV_OP_REVERSE_STRESS_PML:
+        // folded into the full-gridext stress kernel where that one runs
+        if (!fullR_.ok) JV_K(k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
+        break;
+    case JV_OP_REVERSE_STRESS:
+        if (fullR_.ok) JV_K(k_stress_full(kRev, g_, R_, dt, wavelet_, st_, 0, fullR_, s));
+        else JV_K(k_stress_phy(kRev, g_, R_, lam_, mu_, dt, rw, wavelet_, st_, 0, kc_, s, &mapsR_));
+        break;
+    case JV_OP_INJECT_BOUNDARY_VEL: JV_K(k_vowr(g_, F_, vowr_, st_, 0, 0, 1, s)); break;
+    default: return bad(JV_EINVAL, "unknown time-reverse operation");
+    }
+    return Status{};
+}
+
+// the end of the time-reverse loop, queued: the reconstruction check's
+// second energy, the shot image added to the FP64 stacks, both energies
+// copied to the host
+Status Engine::reverse_end_launch() {
+    if (!rev_open_) return bad(JV_ESTATE, "no time-reverse loop is open (jv_rtm_reverse_begin)");
+    JV_CU(cudaSetDevice(dev_));
+    rev_open_ = false;
     JV_K(k_wave_energy(g_, F_, energy_d_ + 1, stream_));
     JV_K(k_image_stack(g_, shot_img_, img_, stream_));
     JV_CU(cudaMemcpyAsync(recon_energy_, energy_d_, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    return Status{};
+}
+
+Status Engine::rtm_reverse_end() {
+    JV_TRY(reverse_end_launch());
+    JV_CU(cudaStreamSynchronize(stream_));
+    JV_CU(cudaGetLastError());
+    JV_TRY(check_zm_err());
+    return Status{};
+}
+
+Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
+    JV_CU(cudaSetDevice(dev_));
+    long long src;
+    JV_TRY(check_shot(shot, &src));
+    if (nrec_ > 0 && (!d_ox || !d_oy || !d_oz)) return bad(JV_EINVAL, "observed traces must not be NULL");
+    JV_TRY(rtm_prepare());
+    JV_CU(cudaEventRecord(ev0_, stream_));
+    JV_TRY(rtm_forward_pass(shot));
+    JV_TRY(rtm_reverse_begin(shot, d_ox, d_oy, d_oz));
+    JV_TRY(run_loop(kStepRtmRev, nt_));
+    JV_TRY(reverse_end_launch());
     JV_CU(cudaEventRecord(ev1_, stream_));
     JV_CU(cudaEventSynchronize(ev1_));
     JV_CU(cudaGetLastError());

@@ -81,6 +81,14 @@ class Engine {
     Status set_model(const float *vp, const float *vs, const float *rho);
     Status forward(int shot, float *d_vx, float *d_vy, float *d_vz);
     Status rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz);
+    // the phases of rtm_shot, for drivers that run them one by one: the
+    // forward pass with the boundary store, the opening of the time-reverse
+    // loop, one of its kernels (jv_rtm_op) at a time index, and its end
+    // (reconstruction check, the shot image added to the stacks)
+    Status rtm_forward_pass(int shot);
+    Status rtm_reverse_begin(int shot, const float *d_ox, const float *d_oy, const float *d_oz);
+    Status rtm_reverse_op(int op, int it);
+    Status rtm_reverse_end();
     Status image_reset();
     Status image_get(int kind, double *host_out);
     Status image_finalize(float *host_out[8]);
@@ -133,6 +141,11 @@ class Engine {
     Status zero_wave(const WaveDev &w, int nfld);
     Status zero_psi(const CpmlDev &c);
     Status set_state(int it, long long src, float *const tr[3], const float *const obs[3]);
+    Status rtm_prepare();
+    Status reverse_end_launch();
+    StepState h_state_{};   // host copy of the last step state written
+    int fwd_shot_ = -1;     // shot of the last RTM forward pass
+    bool rev_open_ = false;  // a time-reverse loop is open
 
     jv_grid grid_{};
     jv_options opt_{};

@@ -369,6 +369,26 @@ jv_status jv_set_geometry(jv_ctx *c, int n_shot, const float *shot_xyz, int n_re
     return ret(s);
 }
 
+jv_status jv_rtm_forward_pass(jv_ctx *c, int shot) {
+    JV_IDLE(c);
+    return ret(c->eng->rtm_forward_pass(shot));
+}
+
+jv_status jv_rtm_reverse_begin(jv_ctx *c, int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
+    JV_IDLE(c);
+    return ret(c->eng->rtm_reverse_begin(shot, d_ox, d_oy, d_oz));
+}
+
+jv_status jv_rtm_reverse_op(jv_ctx *c, int op, int it) {
+    JV_IDLE(c);
+    return ret(c->eng->rtm_reverse_op(op, it));
+}
+
+jv_status jv_rtm_reverse_end(jv_ctx *c) {
+    JV_IDLE(c);
+    return ret(c->eng->rtm_reverse_end());
+}
+
 jv_status jv_set_model(jv_ctx *c, const float *vp, const float *vs, const float *rho) {
     JV_IDLE(c);
     return ret(c->eng->set_model(vp, vs, rho));

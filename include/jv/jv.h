@@ -400,6 +400,46 @@ jv_status jv_server_close(jv_server *s);
  * with CUDA events around its kernels. */
 jv_status jv_last_timing(const jv_ctx *c, double *ms);
 
+/* The RTM shot in the phases of the reference's drivers, for callers that
+ * drive the time loops themselves (the C++ front end jarvis_compat.hpp
+ * runs the reference's rtm_forward / rtm_backward / rtm_reverse modules on
+ * them).  jv_rtm_shot_device is
+ *   jv_rtm_forward_pass(shot)                 fdtd3d_blend_elastic_model_mpi_module<rtm_forward>::
+ *                                             mpi_sub_forward_for_restruct (FD/fdtd3d_3_model_mpi_blend/
+ *                                             fdtd3d_blend_elastic_model_mpi_meat.hpp:125-155): modelling
+ *                                             with the VOWR boundary store, graph-captured
+ *   jv_rtm_reverse_begin(shot, d_obs)         rtm_backward / rtm_reverse reset_for_next_shot (:185-214):
+ *                                             cleared receiver wavefield and shot image, the adjoint
+ *                                             sources d_ox/d_oy/d_oz (device, [n_recv][nt])
+ *   for it = nt-1 .. 0: jv_rtm_reverse_op     one kernel each, in the order of the reference's time-reverse
+ *                                             loop (RTM/rtm3d_1_model_mpi_blend/
+ *                                             rtm3d_blend_elastic_model_mpi_meat.hpp:64-113)
+ *   jv_rtm_reverse_end                        the shot image added to the FP64 stacks, the reconstruction
+ *                                             check (jv_reconstruction_energy)
+ * The per-op path launches kernels one at a time (no graphs), so it is
+ * slower than jv_rtm_shot_device; the results are the same, bit for bit.
+ * Time indices: `it` is the time step of the loop; for the two boundary
+ * replays it is the index of the record replayed (the reference passes
+ * it - 1; records outside 0..nt-2 replay nothing). */
+typedef enum jv_rtm_op {
+    JV_OP_INJECT_RECEIVERS = 0,       /* adjoint sources at it (sub_rtm_reverse_add_vel_source)       */
+    JV_OP_BACKWARD_STRESS = 1,        /* source wavefield, stress backward in time, its source
+                                         subtracted at it (cuda_subtract_stress_source fused)         */
+    JV_OP_REVERSE_VEL_PML = 2,        /* receiver wavefield, absorbing layers of the velocity update  */
+    JV_OP_REVERSE_VEL = 3,            /* receiver wavefield, velocity update of gridphy               */
+    JV_OP_INJECT_BOUNDARY_STRESS = 4, /* stored stress boundary layers of record it                   */
+    JV_OP_BACKWARD_VEL_IMAGE = 5,     /* source wavefield, velocity backward in time, with the
+                                         zero-lag imaging condition fused (cal_correlation_from_wave) */
+    JV_OP_REVERSE_STRESS_PML = 6,     /* receiver wavefield, absorbing layers of the stress update
+                                         (nothing where they run inside JV_OP_REVERSE_STRESS)          */
+    JV_OP_REVERSE_STRESS = 7,         /* receiver wavefield, stress update                            */
+    JV_OP_INJECT_BOUNDARY_VEL = 8     /* stored velocity boundary layers of record it                 */
+} jv_rtm_op;
+jv_status jv_rtm_forward_pass(jv_ctx *c, int shot);
+jv_status jv_rtm_reverse_begin(jv_ctx *c, int shot, const float *d_ox, const float *d_oy, const float *d_oz);
+jv_status jv_rtm_reverse_op(jv_ctx *c, int op, int it);
+jv_status jv_rtm_reverse_end(jv_ctx *c);
+
 /* Per-kernel timing: with profiling on, the time loops launch kernels
  * directly (no graphs) and bracket each launch with CUDA events on the
  * context's stream; jv_profile_entry returns, for entry idx, the kernel

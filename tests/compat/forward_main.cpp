@@ -14,9 +14,11 @@ int main(int argc, char *argv[]) {
     fwd.initialize();
     fwd.reset_for_next_shot();
     fwd.mpi_sub_forward(0);
+    fwd.seis_record_p->copy_seis_into_host(0);
+    const std::vector<float> &vz = fwd.seis_record_p->vz_host_vec[0];
     FILE *f = std::fopen(argv[2], "wb");
     if (!f) return 3;
-    std::fwrite(fwd.vz_seis.data(), sizeof(float), fwd.vz_seis.size(), f);
+    std::fwrite(vz.data(), sizeof(float), vz.size(), f);
     std::fclose(f);
     std::printf("n_recv %d nt %d n_shot %d\n", fwd.n_recv, fwd.nt, fwd.n_shot);
     jarvis_mpi_final;

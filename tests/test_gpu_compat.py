@@ -139,3 +139,66 @@ def test_raw_model_project_matches_gms_project(tmp_path, project, synth):
         assert fr["type"] == 30 and (fr["n_rows"], fr["n_cols"], fr["n_slices"]) == (s.nx, s.ny, s.nz)
         assert fr["d"][0] == np.float32(s.dx) and fr["r"][2] == np.float32((s.nz - 1) * np.float32(s.dz))
         assert np.array_equal(img.reshape(-1), b[nm]), nm
+
+
+def test_rtm_modules_driver_matches_run_project(tmp_path, project):
+    """tests/compat/rtm_modules_main.cpp runs the job through the four module
+    specialisations (pure_forward, rtm_forward with
+    mpi_sub_forward_for_restruct, rtm_backward, rtm_reverse) and MigImage,
+    with the reference's time-reverse loop of component calls, each a kernel
+    launched on its own.  Its trace and image files equal jv_run_project's
+    (graph-captured loops), bit for bit; its .fld of image_pp holds the
+    same values."""
+    s = mg.case_survey("pin_w1")
+    d1, d2 = str(tmp_path / "a") + "/", str(tmp_path / "b") + "/"
+    project.write_project(d1, s)
+    project.write_project(d2, s)
+    exe = build_compat_driver("rtm_modules_main", str(tmp_path))
+    r = subprocess.run([exe, d1], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "geo_const: 4 2 1" in r.stdout
+    with jv.Context.open(d2) as ctx:
+        ctx.run_project()
+    a, b = _read_outputs(project, d1, s), _read_outputs(project, d2, s)
+    for k in b:
+        assert np.array_equal(a[k], b[k]), k
+    fr, img = project.read_fld(f"{d1}out/image_pp_0.fld")
+    assert fr["type"] == 30 and np.array_equal(img.reshape(-1), b["image_pp_0"])
+
+
+@pytest.mark.parametrize("w", [1, 3])
+def test_reverse_ops_match_rtm_shot(synth, w):
+    """The time-reverse loop driven one kernel at a time (jv_rtm_forward_pass,
+    jv_rtm_reverse_begin, jv_rtm_reverse_op in the reference's order,
+    jv_rtm_reverse_end) stacks the same images as jv_rtm_shot, bit for bit,
+    with the same reconstruction check."""
+    import torch
+
+    s = synth.small_case(n=(22, 18, 16), pml=6, nt=90, seed=21, rec_width=w)
+    with jv.Context.from_survey(s) as ctx:
+        obs = ctx.forward(0)
+        ctx.image_reset()
+        ctx.rtm_shot(0, obs)
+        want = ctx.images()
+        e_want = ctx.reconstruction_energy()
+        i = ctx.info()
+        dev = torch.from_numpy(np.stack(obs)).cuda()
+        L = jv.lib()
+        ctx.image_reset()
+        assert L.jv_rtm_reverse_op(ctx._h, jv.OP_REVERSE_VEL, 0) == jv.JV_ESTATE  # no loop open
+        assert L.jv_rtm_forward_pass(ctx._h, 0) == jv.JV_OK
+        p = [dev[q].data_ptr() for q in range(3)]
+        assert L.jv_rtm_reverse_begin(ctx._h, 0, p[0], p[1], p[2]) == jv.JV_OK
+        for it in range(i.nt - 1, -1, -1):
+            for op, t in ((jv.OP_INJECT_RECEIVERS, it), (jv.OP_REVERSE_VEL_PML, it), (jv.OP_BACKWARD_STRESS, it),
+                          (jv.OP_INJECT_BOUNDARY_STRESS, it - 1), (jv.OP_REVERSE_VEL, it),
+                          (jv.OP_BACKWARD_VEL_IMAGE, it), (jv.OP_INJECT_BOUNDARY_VEL, it - 1),
+                          (jv.OP_REVERSE_STRESS_PML, it), (jv.OP_REVERSE_STRESS, it)):
+                assert L.jv_rtm_reverse_op(ctx._h, op, t) == jv.JV_OK
+        assert L.jv_rtm_reverse_end(ctx._h) == jv.JV_OK
+        got = ctx.images()
+        e_got = ctx.reconstruction_energy()
+        assert L.jv_rtm_reverse_op(ctx._h, 99, 0) == jv.JV_ESTATE  # closed again
+    for k in want:
+        assert np.array_equal(got[k], want[k]), k
+    assert e_got == e_want
