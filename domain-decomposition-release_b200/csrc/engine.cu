@@ -358,7 +358,10 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
-    if (s && tune) s = E->autotune();
+    // measured at creation: the full choice with kernel_variant -1, else
+    // (autotune on, nothing fixed by hand) the result-neutral knobs only
+    const bool neutral = !tune && opt.autotune && opt.run_chunks <= 0 && opt.tile_gx <= 0 && opt.tile_gy <= 0;
+    if (s && (tune || neutral)) s = E->autotune(!tune);
     if (!s) {
         delete E;
         return s;
@@ -378,20 +381,20 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
 // float4 velocity update and the backward stress update (the forward step
 // of a one-tile grid does not run them).  The fastest wins; the choice is
 // kept per grid shape and device for the contexts that follow.
-Status Engine::autotune() {
+Status Engine::autotune(bool neutral) {
     struct Cand {
         int variant, pml_minb, q;  // q: variant 4's run chunks
         int gx = 0;                // float4 kernels' x groups per block (0: the default shape)
     };
     const bool shape_free = opt_.tile_gx <= 0 && opt_.tile_gy <= 0;
     static std::mutex mu;
-    static std::map<std::array<long long, 6>, Cand> cache;
+    static std::map<std::array<long long, 7>, Cand> cache;
     int dev = 0;
     JV_CU(cudaGetDevice(&dev));
     cudaDeviceProp prop{};
     JV_CU(cudaGetDeviceProperties(&prop, dev));
-    const std::array<long long, 6> key = {grid_.nx, grid_.ny, grid_.nz, grid_.pml, prop.multiProcessorCount,
-                                          (long long)prop.totalGlobalMem};
+    const std::array<long long, 7> key = {grid_.nx, grid_.ny, grid_.nz, grid_.pml, prop.multiProcessorCount,
+                                          (long long)prop.totalGlobalMem, neutral ? 1 : 0};
     Status st{};
     auto apply = [&](const Cand &c) {
         kc_.variant = c.variant;
@@ -425,18 +428,26 @@ Status Engine::autotune() {
                 if (fullF_.qcand[k] > 0) cands.push_back({4, 4, fullF_.qcand[k]});
         }
     }
-    if (mapsF_.ok) {
-        cands.push_back({3, 4, 0});
-        cands.push_back({3, 3, 0});
+    if (neutral) {
+        // only what cannot change a result: variant 4's run chunking (which
+        // CTA updates which cells) and, below, the float4 kernels' block
+        // shape (which thread updates which group)
+        if (cands.empty()) cands.push_back({kc_.variant, kc_.pml_minb, 0});
+    } else {
+        if (mapsF_.ok) {
+            cands.push_back({3, 4, 0});
+            cands.push_back({3, 3, 0});
+        }
+        cands.push_back({2, 4, 0});
+        cands.push_back({2, 3, 0});
     }
-    cands.push_back({2, 4, 0});
-    cands.push_back({2, 3, 0});
     const long long src = (long long)g_.xoff + (g_.m + g_.px / 2) + g_.sy * (g_.m + g_.py / 2) +
                           g_.sz * (g_.m + g_.pz / 2);
     float best = -1.f;
     Cand pick = cands[0];
     const int warm = 2, steps = 6;
     for (const Cand &c : cands) {
+        if (cands.size() == 1) break;  // nothing to choose between
         apply(c);
         JV_TRY(st);
         JV_TRY(zero_wave(F_, 9));

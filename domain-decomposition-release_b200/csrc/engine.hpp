@@ -120,7 +120,7 @@ class Engine {
     Status check_shot(int shot, long long *src) const;
     Status run_loop(int kind, int nsteps);
     Status launch_step(int kind, int off, bool advance);
-    Status autotune();
+    Status autotune(bool neutral);
 
   public:
     // the options this context runs with, the kernel choice as made

@@ -187,6 +187,7 @@ void jv_options_default(jv_options *o) {
     o->store_budget = 0;
     o->kernel_variant = 4;
     o->zchunk = 0;
+    o->autotune = 1;
 }
 
 jv_status jv_create(const jv_grid *grid, const float *vp, const float *vs, const float *rho, float dt, float fm,

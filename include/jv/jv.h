@@ -100,6 +100,12 @@ typedef struct jv_options {
                            persistent kernels' run schedule (0 -> the cost model's
                            choice; with kernel_variant -1 the measured choice among the
                            cost model's three best); jv_get_kernel_config reports it */
+    int autotune;       /* 1 (default): at creation, time the knobs that cannot change a result --
+                           variant 4's run chunking among the cost model's three best and the
+                           float4 kernels' block shape -- on this grid and keep the fastest, per
+                           grid shape and device for the process (skipped when run_chunks,
+                           tile_gx or tile_gy fix them, or kernel_variant is -1, which makes the
+                           wider choice); 0: the cost model's chunking and the default shape */
 } jv_options;
 
 /* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,

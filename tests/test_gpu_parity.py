@@ -445,7 +445,7 @@ def test_run_chunks_change_no_result(synth, chunks):
     s = synth.small_case(n=(24, 20, 18), pml=6, nt=60, seed=3)
     out = {}
     for q in (0, chunks):
-        with jv.Context.from_survey(s, run_chunks=q) as ctx:
+        with jv.Context.from_survey(s, run_chunks=q, autotune=0) as ctx:
             cfg = ctx.kernel_config()
             tr = ctx.forward(0)
             ctx.rtm_shot(0, tr)
@@ -456,6 +456,31 @@ def test_run_chunks_change_no_result(synth, chunks):
         assert np.array_equal(a, b)
     for k in out[0][1]:
         assert np.array_equal(out[0][1][k], out[chunks][1][k]), k
+
+
+def test_default_autotune_is_result_neutral(synth):
+    """By default a context times the knobs that cannot change a result
+    (variant 4's run chunking among the cost model's best, the float4
+    kernels' block shape) at creation: its traces and images equal those of
+    a context with the cost model's fixed choice, bit for bit; the choice
+    is reported and reused by the next context of the same shape."""
+    s = synth.small_case(n=(40, 24, 20), pml=8, nt=80, seed=62)
+    out, cfgs = {}, []
+    for tune in (0, 1, 1):
+        with jv.Context.from_survey(s, autotune=tune) as ctx:
+            cfg = ctx.kernel_config()
+            tr = ctx.forward(0)
+            ctx.rtm_shot(0, tr)
+            out[tune] = (tr, ctx.images())
+        if tune:
+            cfgs.append((cfg["run_chunks"], cfg["tile_gx"]))
+        assert cfg["kernel_variant"] == 4 and cfg["run_chunks"] > 0 and cfg["autotune"] == tune
+        assert cfg["tile_gx"] in (0, 5, 10) and cfg["tile_gy"] == 0
+    assert cfgs[0] == cfgs[1], cfgs
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    for k in out[0][1]:
+        assert np.array_equal(out[0][1][k], out[1][1][k]), k
 
 
 @pytest.mark.parametrize("variant", [4, 2])
