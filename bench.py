@@ -217,34 +217,67 @@ def cpu_sample(s, oracle, seconds_target=20.0, max_steps=200):
     return {"shots_per_h": 3600.0 / sec_per_shot, "gcells": cells / dt / 1e9, "steps": steps2, "seconds": dt}
 
 
-def serve_leg(jv, synth, n_req):
+def _outputs(jv, plan):
+    """Output arrays of every request, allocated and touched before timing
+    (a serving loop reuses its buffers; first-touch page faults are the
+    caller's allocator, not the server)."""
+    outs = []
+    for sv, k in plan:
+        if k == jv.JOB_FORWARD:
+            o = tuple(np.empty((sv.recvs.shape[0], sv.nt), np.float32) for _ in range(3))
+        else:
+            o = tuple(np.empty((sv.nz, sv.ny, sv.nx), np.float64) for _ in range(5))
+        for a in o:
+            a.fill(0)
+        outs.append(o)
+    return outs
+
+
+def _served(jv, plan, outs, slots, timeout):
+    """All requests submitted at once to a new server of `slots` slots;
+    (seconds from the first submission to the last completion, stats)."""
+    with jv.Server(slots=slots) as srv:
+        t0 = time.perf_counter()
+        subs = [srv.submit_survey(k, sv, outs=o) for (sv, k), o in zip(plan, outs)]
+        for rid, _ in subs:
+            if srv.wait(rid, timeout=timeout) != 0:
+                raise RuntimeError("served request failed")
+        dt = time.perf_counter() - t0
+        st = srv.stats()
+    return dt, st
+
+
+def _repeat(jv, plan, outs, timeout, repeats):
+    """1 slot and 4 slots, alternating, `repeats` times each; per config the
+    median run (by time) and every run's requests/h."""
+    runs = {1: [], 4: []}
+    for _ in range(repeats):
+        for slots in (1, 4):
+            runs[slots].append(_served(jv, plan, outs, slots, timeout))
+    med = {}
+    for slots, rs in runs.items():
+        rs = sorted(rs, key=lambda r: r[0])
+        med[slots] = rs[len(rs) // 2]
+    return runs, med
+
+
+def serve_leg(jv, synth, n_req, repeats=3):
     """Heterogeneous requests through jv_server: grids of 48..112 cells per
     axis (+10 CPML), 400 steps, forward and RTM (the RTM requests model
     their own traces first), each with its own model and a full receiver
-    plane; host buffers in and out.  Served with 4 slots against the same
-    requests one at a time (1 slot); requests/h and p50/p99 latency from
-    the server's own statistics (submission to completion)."""
+    plane; host buffers in and out, allocated before timing.  Served with 4
+    slots against the same requests one at a time (1 slot), `repeats` runs
+    of each, alternating, every run on a new server (its context pool
+    starts empty); requests/h and p50/p99 latency from the server's own
+    statistics (submission to completion) of the median run."""
     sizes = [48, 64, 80, 96, 112]
     surveys = {n: synth.scaled_cfg2(n, 400, pml=10, seed=30 + n) for n in sizes}
     plan = [(surveys[sizes[i % len(sizes)]], jv.JOB_RTM if i % 3 else jv.JOB_FORWARD) for i in range(n_req)]
+    outs = _outputs(jv, plan)
 
-    with jv.Server(slots=2) as srv:  # warm-up requests (module load, allocator pools), not counted
-        for rid, _ in [srv.submit_survey(k, sv) for sv, k in plan[:2]]:
-            srv.wait(rid, timeout=300.0)
-
-    def run(slots):
-        with jv.Server(slots=slots) as srv:
-            t0 = time.perf_counter()
-            subs = [srv.submit_survey(k, sv) for sv, k in plan]
-            for rid, _ in subs:
-                if srv.wait(rid, timeout=600.0) != 0:
-                    raise RuntimeError("served request failed")
-            dt = time.perf_counter() - t0
-            st = srv.stats()
-        return dt, st
-
-    t1, st1 = run(1)
-    t4, st4 = run(4)
+    _served(jv, plan[:2], outs[:2], 2, 300.0)  # warm-up (module load, allocator pools), not counted
+    runs, med = _repeat(jv, plan, outs, 600.0, repeats)
+    (t1, st1), (t4, st4) = med[1], med[4]
     cells = sum((sv.nx + 2 * sv.pml) * (sv.ny + 2 * sv.pml) * (sv.nz + 2 * sv.pml) * sv.nt * (3 if k else 1)
                 for sv, k in plan)
 
@@ -256,12 +289,12 @@ def serve_leg(jv, synth, n_req):
             t0 = time.perf_counter()
             due = 0.0
             subs = []
-            for sv, k in plan:
+            for (sv, k), o in zip(plan, outs):
                 due += rng.exponential(1.0 / rate)
                 pause = t0 + due - time.perf_counter()
                 if pause > 0:
                     time.sleep(pause)
-                subs.append(srv.submit_survey(k, sv))
+                subs.append(srv.submit_survey(k, sv, outs=o))
             for rid, _ in subs:
                 if srv.wait(rid, timeout=600.0) != 0:
                     raise RuntimeError("served request failed")
@@ -277,12 +310,16 @@ def serve_leg(jv, synth, n_req):
             "mix": f"grids {sizes}^3 +10 CPML, nt 400, 2/3 RTM (own modelling first), 1/3 forward",
             "slots4": round(n_req / t4 * 3600.0, 1), "slots1": round(n_req / t1 * 3600.0, 1),
             "speedup": round(t1 / t4, 3),
+            "runs": {"slots1": [round(n_req / t * 3600.0, 1) for t, _ in runs[1]],
+                     "slots4": [round(n_req / t * 3600.0, 1) for t, _ in runs[4]]},
+            "contexts_reused": {"slots1": st1["reused"], "slots4": st4["reused"]},
             "p50_ms": {"slots4": round(st4["p50_ms"], 1), "slots1": round(st1["p50_ms"], 1)},
             "p99_ms": {"slots4": round(st4["p99_ms"], 1), "slots1": round(st1["p99_ms"], 1)},
             "gcell_updates_per_s": {"slots4": round(cells / t4 / 1e9, 2), "slots1": round(cells / t1 / 1e9, 2)},
-            "note": "latency counts from submission; slots4/slots1: all requests submitted at once; "
-                    "poisson_4slots: seeded exponential arrival gaps at 0.5 and 0.9 of the slots4 rate; two "
-                    "warm-up requests on a server of their own are not counted"}
+            "note": f"median of {repeats} runs per slot count (alternating, each on a new server whose context pool "
+                    "starts empty); latency counts from submission; all requests submitted at once; "
+                    "poisson_4slots: seeded exponential arrival gaps at 0.5 and 0.9 of the slots4 rate; output "
+                    "buffers allocated before timing; two warm-up requests on a server of their own are not counted"}
 
 
 def serve_config_leg(jv, synth, n_req, nt, rate):
@@ -320,7 +357,7 @@ def serve_config_leg(jv, synth, n_req, nt, rate):
                     "steps and 1-50 requests/s cut to one step count and the lowest rate"}
 
 
-def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
+def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed, repeats=3):
     """The batched configuration, bounded in shots and steps.
 
     (a) n_shots shots at seeded surface positions (depth 5 cells) on one
@@ -332,7 +369,8 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
     (b) n_models independent seeded models with interior sizes drawn
     uniformly from {80, 96, 120, 160, 200}^3 (+16 CPML), nt_mixed steps, one
     RTM request each (modelling its own traces) through jv_server with 4
-    slots, against the same requests one at a time (1 slot)."""
+    slots, against the same requests one at a time (1 slot), `repeats` runs
+    of each."""
     import dataclasses
     rng = np.random.default_rng(64)
     base = synth.scaled_cfg2(160, nt, pml=16, seed=64)
@@ -372,44 +410,39 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed):
     models = [synth.scaled_cfg2(n, nt_mixed, pml=16, seed=200 + k) for k, n in enumerate(sizes)]
     cells = sum(nt_mixed * (3 * m.n_ext) for m in models)  # own modelling + source and receiver propagations
 
-    def run(slots):
-        with jv.Server(slots=slots) as srv:
-            t0 = time.perf_counter()
-            subs = [srv.submit_survey(jv.JOB_RTM, m) for m in models]
-            for rid, _ in subs:
-                if srv.wait(rid, timeout=900.0) != 0:
-                    raise RuntimeError("mixed-batch request failed")
-            dt = time.perf_counter() - t0
-            st = srv.stats()
-        return dt, st
-
-    with jv.Server(slots=2) as srv:  # warm-up requests (one of each size), not counted
-        warm = {}
-        for m in models:
-            warm.setdefault(m.nx, m)
-        for rid, _ in [srv.submit_survey(jv.JOB_RTM, m) for m in warm.values()]:
-            srv.wait(rid, timeout=900.0)
-    t1, st1 = run(1)
-    t4, st4 = run(4)
+    plan = [(m, jv.JOB_RTM) for m in models]
+    outs = _outputs(jv, plan)
+    warm = {}
+    for (m, k), o in zip(plan, outs):
+        warm.setdefault(m.nx, ((m, k), o))
+    _served(jv, [w[0] for w in warm.values()], [w[1] for w in warm.values()], 2, 900.0)  # warm-up, not counted
+    runs, med = _repeat(jv, plan, outs, 900.0, repeats)
+    (t1, st1), (t4, st4) = med[1], med[4]
     out["mixed_models"] = {
         "models": n_models, "sizes": {str(n): sizes.count(n) for n in sorted(set(sizes))}, "pml": 16,
         "nt": nt_mixed, "unit": "RTM shots/h", "slots1": round(n_models / t1 * 3600.0, 1),
         "slots4": round(n_models / t4 * 3600.0, 1), "speedup": round(t1 / t4, 3),
+        "runs": {"slots1": [round(n_models / t * 3600.0, 1) for t, _ in runs[1]],
+                 "slots4": [round(n_models / t * 3600.0, 1) for t, _ in runs[4]]},
+        "contexts_reused": {"slots1": st1["reused"], "slots4": st4["reused"]},
         "gcell_updates_per_s": {"slots1": round(cells / t1 / 1e9, 2), "slots4": round(cells / t4 / 1e9, 2)},
         "p50_ms": {"slots1": round(st1["p50_ms"], 1), "slots4": round(st4["p50_ms"], 1)},
         "p99_ms": {"slots1": round(st1["p99_ms"], 1), "slots4": round(st4["p99_ms"], 1)},
-        "note": "each request models its own traces, then migrates; all submitted at once; latency from "
-                "submission; one warm-up request of each size on a server of its own is not counted; the "
-                "configured 64 shots / 48 models are cut in steps (and shots) to keep the bench short"}
+        "note": f"median of {repeats} runs per slot count (alternating, each on a new server whose context pool "
+                "starts empty); each request models its own traces, then migrates; all submitted at once; latency "
+                "from submission; output buffers allocated before timing; one warm-up request of each size on a "
+                "server of its own is not counted; the configured 48 models run "
+                f"{nt_mixed} steps each"}
     return out
 
 
 def extra_configs(jv, synth, torch, device):
     """The other configurations, one short measurement each (not the
-    headline): cfg1 plain forward modelling in full, and the large cfg3
-    grid's RTM shot with the FP16 boundary store, cut to a few time steps,
-    with the measured kernel choice (kernel_variant -1, made when the
-    context is created)."""
+    headline): cfg1 plain forward modelling in full, cfg2's RTM shot at
+    rec_width 4 in full (with its accuracy against the size fixtures), and
+    the large cfg3 grid's RTM shot with the FP16 boundary store, cut to a
+    few time steps, with the measured kernel choice (kernel_variant -1, made
+    when the context is created)."""
     out = {}
     s = synth.cfg1()
     with jv.Context.from_survey(s, device=device) as ctx:
@@ -425,6 +458,30 @@ def extra_configs(jv, synth, torch, device):
         out["cfg1_forward"] = {"grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt, "n_recv": i.n_recv,
                                "ms_per_shot": round(1000 * t, 2), "shots_per_h": round(3600.0 / t, 1),
                                "gcell_updates_per_s": round(i.n_ext * s.nt / t / 1e9, 2)}
+    # cfg2 at rec_width 4: the VOWR store keeps 4 layers per face (47 GB
+    # of HBM in FP32), and the reconstruction is exact
+    s = synth.cfg2(rec_width=4)
+    with jv.Context.from_survey(s, device=device) as ctx:
+        i = ctx.info()
+        tr = torch.empty((3, i.n_recv, i.nt), dtype=torch.float32, device=f"cuda:{device}")
+        ptrs = [tr[q].data_ptr() for q in range(3)]
+        ctx.forward_device(0, ptrs)
+        ctx.rtm_shot_device(0, ptrs)  # warm-up (graph capture, store allocation)
+        ms = []
+        for _ in range(2):
+            ctx.rtm_shot_device(0, ptrs)
+            ms.append(ctx.last_ms())
+        t = min(ms) / 1000.0
+        e0, e1 = ctx.reconstruction_energy()
+        acc = accuracy_leg(ctx, s, tr, ptrs, 4)
+        out["cfg2_rtm_w4"] = {
+            "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt, "rec_width": 4, "n_recv": i.n_recv,
+            "shots_per_h": round(3600.0 / t, 1), "ms_per_shot": round(1000 * t, 1),
+            "gcell_updates_per_s": round(s.nt * (2 * i.n_ext + i.n_phy) / t / 1e9, 2),
+            "store_bytes": int(i.store_bytes_per_step) * (s.nt - 1), "store_on_device": bool(i.store_on_device),
+            "reconstruction_residual_ratio": e1 / e0 if e0 > 0 else None, "accuracy": acc,
+            "note": "best of 2 shots after one warm-up shot"}
+        del tr
     nt3 = 40
     s = synth.cfg3(nt=nt3)
     with jv.Context.from_survey(s, device=device, precision=jv.JV_FP16, kernel_variant=-1) as ctx:
@@ -446,6 +503,63 @@ def extra_configs(jv, synth, torch, device):
             "note": "the configured 3000 steps cut to 40 to keep the bench short; per-step cost is constant"}
         del tr
     return out
+
+
+SIZE_FIXTURES = {("cfg2_rtm_200_w1", 1): "size_cfg2_w1", ("cfg2_rtm_200_w4", 4): "size_cfg2_w4"}
+
+
+def accuracy_leg(ctx, s, obs, ptrs, rec_width):
+    """The timed configuration's accuracy, measured on this run: one RTM
+    shot's five raw images on the planes z = 100 and y = 100 and the traces
+    of a 4 x 4 receiver subset, against the FP64 oracle's and the reference
+    binary's outputs of the same shot (tests/golden/size_cfg2_w*.npz, made
+    by tests/golden/make_size_pins.py on a B200); plus the whole-field
+    figures that script measured (tests/golden/size_pins.json)."""
+    name = SIZE_FIXTURES.get((s.name, rec_width))
+    gold = os.path.join(ROOT, "tests", "golden")
+    path = os.path.join(gold, f"{name}.npz") if name else None
+    if not path or not os.path.exists(path):
+        return {"unavailable": f"no size fixture for {s.name} at rec_width {rec_width}"}
+    f = np.load(path)
+    sub = f["subset"]
+    ctx.image_reset()
+    ctx.rtm_shot_device(0, ptrs)
+    img = ctx.images()
+    ctx.image_reset()
+
+    def rl2(a, b):
+        a = np.asarray(a, np.float64)
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    import torch
+    planes = {"z100": lambda a: a[100], "y100": lambda a: a[:, 100]}
+    idx = torch.as_tensor(np.asarray(sub, dtype=np.int64), device=obs.device)
+    tr = [obs[q].index_select(0, idx).cpu().numpy() for q in range(3)]
+    out = {}
+    for src in ("oracle", "ref"):
+        t = max(rl2(tr[q], f[f"{src}_tr_{c}"]) for q, c in enumerate(("vx", "vy", "vz")))
+        im = {}
+        for k in ("ip", "pp", "ps", "sp", "ss"):
+            a = np.concatenate([planes[pk](img[k]).ravel() for pk in planes])
+            b = np.concatenate([f[f"{src}_{k}_{pk}"].ravel() for pk in planes])
+            im[k] = rl2(a, b)
+        out["vs_fp64_oracle" if src == "oracle" else "vs_reference_binary"] = {"traces": t, "images": im}
+    worst = max(out["vs_fp64_oracle"]["images"].values())
+    res = {"metric": "relative L2", **out, "image_bound_vs_fp64": 1e-3, "within_bound": worst <= 1e-3,
+           "sample": "this run's RTM shot: traces of 16 receivers (4 x 4 grid) x all steps; the five raw (stacked, "
+                     "uncompensated) images on the planes z = 100 and y = 100 (80 000 of 8 M cells)"}
+    summ = os.path.join(gold, "size_pins.json")
+    key = name[len("size_"):]
+    if os.path.exists(summ):
+        with open(summ) as fh:
+            d = json.load(fh).get(key)
+        if d:
+            res["full_field"] = {"traces": d["traces"], "raw_images": d["raw_images"],
+                                 "laplacian_pp": d["laplacian_pp"], "compensated": d["compensated"],
+                                 "source": "tests/golden/size_pins.json (tests/golden/make_size_pins.py --run on "
+                                           "one B200: every trace sample and every gridphy cell)"}
+    return res
 
 
 def spawn_ranks(args) -> int:
@@ -545,10 +659,11 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--no-extra", action="store_true", help="skip the cfg1 / cfg3 side measurements")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-configuration leg")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the accuracy leg")
     ap.add_argument("--serve-config-requests", type=int, default=6,
                     help="requests of the configured-grid serving sample (0 skips it)")
     ap.add_argument("--serve-config-nt", type=int, default=1500)
-    ap.add_argument("--batch-shots", type=int, default=8, help="shots of the one-model batch (160^3)")
+    ap.add_argument("--batch-shots", type=int, default=64, help="shots of the one-model batch (160^3)")
     ap.add_argument("--batch-nt", type=int, default=600, help="time steps of the one-model batch")
     ap.add_argument("--mixed-models", type=int, default=48, help="models of the mixed batch")
     ap.add_argument("--mixed-nt", type=int, default=200, help="time steps of each mixed-batch request")
@@ -671,6 +786,10 @@ def main():
                     "traffic": tr, "algorithmic_bytes_per_launch": b, "avg_launch_us": round(avg_s * 1e6, 2),
                     "share": round(ms / tot, 4) if tot > 0 else None}
 
+    accuracy = None
+    if rank == 0 and not args.no_accuracy:
+        accuracy = accuracy_leg(ctx, s, obs, ptrs, args.rec_width)
+
     # end to end through the host-pointer ABI: pinned H2D of the traces,
     # D2H of the 8 finalized images, every step
     e2e = None
@@ -779,7 +898,7 @@ def main():
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
                    "boundary_store": args.store,
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "modes": modes, "serving": serving,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "accuracy": accuracy, "modes": modes, "serving": serving,
         "batched_config": batched_cfg,
         "other_configs": extra, "clocks": clk,
         "gpu_launches": launches * args.steps if launches else None,

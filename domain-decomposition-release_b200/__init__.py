@@ -569,12 +569,23 @@ class Server:
         self._refs[rid.value] = refs
         return rid.value
 
-    def submit_survey(self, kind, s, shot: int = 0, obs=None, precision=JV_FP32):
+    def submit_survey(self, kind, s, shot: int = 0, obs=None, precision=JV_FP32, outs=None):
         """Queues shot `shot` of a synth.Survey-like object; returns (id,
         outputs): the three trace arrays [n_recv][nt] of a FORWARD request,
         or the five image arrays (ip, pp, ps, sp, ss; gridphy, float64) of an
-        RTM request, filled when the request is done."""
+        RTM request, filled when the request is done.  outs: those arrays,
+        allocated by the caller (e.g. reused), instead of new ones."""
         rv = np.ascontiguousarray(s.recvs, dtype=np.float32).reshape(-1, 3)
+        if outs is not None:
+            want = (np.float32, (rv.shape[0], s.nt), 3) if kind == JOB_FORWARD else (np.float64, (s.nz, s.ny, s.nx), 5)
+            outs = tuple(outs)
+            if len(outs) != want[2] or any(o.dtype != want[0] or o.shape != want[1] or not o.flags.c_contiguous
+                                           for o in outs):
+                raise JvError(JV_EINVAL, "outs do not match the request's outputs")
+            rid = self.submit(kind, s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt,
+                              s.shots[shot], rv, rec_width=s.rec_width, obs=obs,
+                              **({"out": outs} if kind == JOB_FORWARD else {"image": outs, "precision": precision}))
+            return rid, outs
         if kind == JOB_FORWARD:
             outs = tuple(np.zeros((rv.shape[0], s.nt), np.float32) for _ in range(3))
             rid = self.submit(kind, s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.vp, s.vs, s.rho, s.dt, s.fm, s.nt,
