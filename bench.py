@@ -322,39 +322,52 @@ def serve_leg(jv, synth, n_req, repeats=3):
                     "buffers allocated before timing; two warm-up requests on a server of their own are not counted"}
 
 
-def serve_config_leg(jv, synth, n_req, nt, rate):
-    """Serving at the configured grid sizes, bounded: n_req RTM requests
-    (each modelling its own traces first) on grids drawn (seeded) from
-    {120^3, 200^3, 320^3, 480 x 480 x 200} + 20 CPML, nt steps, seeded
+def serve_config_leg(jv, synth, n_req, nt, rate, seed=5, nt_max=None, forward_share=0.0):
+    """Serving at the configured grid sizes: n_req requests on grids drawn
+    (seeded) from {120^3, 200^3, 320^3, 480 x 480 x 200} + 20 CPML, seeded
     layered models and source positions, arriving as a Poisson stream at
-    `rate` requests/s (the low end of the configured 1-50/s; it already
-    exceeds what these grids allow, so latency is mostly queueing), served
-    with 4 slots under the default HBM budget."""
+    `rate` requests/s, served with 4 slots under the default HBM budget.
+    Step counts: nt, or drawn uniformly from [nt, nt_max]; a share of
+    forward_share of the requests is forward modelling, the others RTM
+    (each modelling its own traces first)."""
     grids = [(120, 120, 120), (200, 200, 200), (320, 320, 320), (480, 480, 200)]
-    rng = np.random.default_rng(5)
+    rng = np.random.default_rng(seed)
     picks = [grids[int(k)] for k in rng.permutation(np.arange(n_req) % len(grids))]
-    reqs = [synth.serving_grid(*g, nt, seed=300 + k) for k, g in enumerate(picks)]
-    cells = sum(nt * (2 * r.n_ext + r.n_phy + r.n_ext) for r in reqs)  # own modelling + migration
+    nts = [int(rng.integers(nt, nt_max + 1)) if nt_max else nt for _ in picks]
+    kinds = [jv.JOB_FORWARD if rng.random() < forward_share else jv.JOB_RTM for _ in picks]
+    reqs = [synth.serving_grid(*g, n, seed=300 + k) for k, (g, n) in enumerate(zip(picks, nts))]
+    plan = list(zip(reqs, kinds))
+    outs = _outputs(jv, plan)
+    # forward: one pass; RTM: own modelling + forward pass + reverse loop
+    cells = sum(r.nt * (r.n_ext if k == jv.JOB_FORWARD else 3 * r.n_ext + r.n_phy) for r, k in plan)
     with jv.Server(slots=4) as srv:
         t0 = time.perf_counter()
         due, subs = 0.0, []
-        for r in reqs:
+        for (r, k), o in zip(plan, outs):
             due += rng.exponential(1.0 / rate)
             pause = t0 + due - time.perf_counter()
             if pause > 0:
                 time.sleep(pause)
-            subs.append(srv.submit_survey(jv.JOB_RTM, r))
+            subs.append(srv.submit_survey(k, r, outs=o))
         for rid, _ in subs:
-            if srv.wait(rid, timeout=1200.0) != 0:
+            if srv.wait(rid, timeout=1800.0) != 0:
                 raise RuntimeError("served request failed")
         dt = time.perf_counter() - t0
         st = srv.stats()
-    return {"requests": n_req, "grids": ["x".join(map(str, g)) for g in picks], "pml": 20, "nt": nt,
-            "offered_per_s": rate, "unit": "RTM requests/h", "value": round(n_req / dt * 3600.0, 1),
+    return {"requests": n_req, "grids": ["x".join(map(str, g)) for g in picks], "pml": 20,
+            "nt": nts if nt_max else nt, "kinds": ["forward" if k == jv.JOB_FORWARD else "rtm" for _, k in plan],
+            "offered_per_s": rate, "unit": "requests/h", "value": round(n_req / dt * 3600.0, 1),
             "gcell_updates_per_s": round(cells / dt / 1e9, 2), "p50_ms": round(st["p50_ms"], 1),
-            "p99_ms": round(st["p99_ms"], 1), "seconds": round(dt, 2),
-            "note": "4 slots; each request models its own traces, then migrates; the configured 1500-3000 "
-                    "steps and 1-50 requests/s cut to one step count and the lowest rate"}
+            "p99_ms": round(st["p99_ms"], 1), "seconds": round(dt, 2), "contexts_reused": st["reused"],
+            "note": "4 slots; RTM requests model their own traces, then migrate; latency from submission"}
+
+
+def serve_sweep(jv, synth, n_req, rates):
+    """The serving configuration as specified, opt-in (--serve-sweep): a
+    Poisson stream at each rate, nt drawn from 1500-3000, half forward
+    modelling and half RTM, grids from the configured four."""
+    return [serve_config_leg(jv, synth, n_req, 1500, r, seed=50 + i, nt_max=3000, forward_share=0.5)
+            for i, r in enumerate(rates)]
 
 
 def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed, repeats=3):
@@ -663,6 +676,10 @@ def main():
     ap.add_argument("--serve-config-requests", type=int, default=6,
                     help="requests of the configured-grid serving sample (0 skips it)")
     ap.add_argument("--serve-config-nt", type=int, default=1500)
+    ap.add_argument("--serve-sweep", default="",
+                    help="comma-separated arrival rates (requests/s) of the full serving sweep, e.g. 1,5,20,50 "
+                         "(nt 1500-3000, half forward, half RTM); off by default")
+    ap.add_argument("--serve-sweep-requests", type=int, default=8)
     ap.add_argument("--batch-shots", type=int, default=64, help="shots of the one-model batch (160^3)")
     ap.add_argument("--batch-nt", type=int, default=600, help="time steps of the one-model batch")
     ap.add_argument("--mixed-models", type=int, default=48, help="models of the mixed batch")
@@ -853,6 +870,9 @@ def main():
         if args.serve_config_requests > 0:
             serving["configured_grids"] = serve_config_leg(jv, jv.synth, args.serve_config_requests,
                                                            args.serve_config_nt, 1.0)
+        if args.serve_sweep:
+            serving["sweep"] = serve_sweep(jv, jv.synth, args.serve_sweep_requests,
+                                           [float(r) for r in args.serve_sweep.split(",")])
     extra = None
     if world == 1 and not args.no_extra:
         extra = extra_configs(jv, jv.synth, torch, local)

@@ -300,7 +300,6 @@ size_t footprint_bytes(const jv_grid &grid, int nt, int rec_width, bool rtm, int
         b += (size_t)per * nslot * (s16 ? sizeof(uint16_t) : sizeof(float));      // boundary store
         if (s16) b += (nslot + 2) * segs.size() * sizeof(float);                    // its per-box scales
         b += 5 * ((nphy + 63) / 64 * 64) * sizeof(float);                           // shot image
-        b += (size_t)blk * sizeof(int) + 64 * sizeof(SegDev);
     }
     return b;
 }
@@ -327,6 +326,8 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread < 0 || opt.planes_per_thread > 2 || opt.pml_planes_per_thread < 0 ||
         opt.pml_planes_per_thread > 2)
         return bad(JV_EINVAL, "planes_per_thread and pml_planes_per_thread must be 0, 1 or 2");
+    if (opt.fuse_min_blocks != 0 && (opt.fuse_min_blocks < 2 || opt.fuse_min_blocks > 4))
+        return bad(JV_EINVAL, "fuse_min_blocks must be 0, 2, 3 or 4");
     if (opt.kernel_variant < -1 || opt.kernel_variant > 4)
         return bad(JV_EINVAL, "kernel_variant must be 0..4, or -1 (measured choice)");
     if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
@@ -355,6 +356,8 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread) E->kc_.zp = opt.planes_per_thread;
     if (opt.pml_planes_per_thread) E->kc_.pml_zp = opt.pml_planes_per_thread;
     if (opt.run_chunks > 0) E->kc_.fzq = opt.run_chunks;
+    E->kc_.both = opt.fuse_velocity ? 1 : 0;
+    if (opt.fuse_min_blocks) E->kc_.both_minb = opt.fuse_min_blocks;
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
@@ -591,20 +594,12 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         vowr_.prec = opt_.precision;
         vowr_.nseg = (int)segs_h_.size();
         vowr_.all_blocks = (int)blk;
-        std::vector<int> blk_seg((size_t)blk);
+        if (segs_h_.size() > (size_t)kVowrMaxSegs) return bad(JV_EINVAL, "too many boundary boxes");
         for (size_t q = 0; q < segs_h_.size(); q++) {
             const SegDev &S = segs_h_[q];
+            vowr_.seg[q] = S;
             const long long nb = ((long long)S.nxb * S.nyb * S.nzb + 256LL * S.vw - 1) / (256LL * S.vw);
-            for (long long b = 0; b < nb; b++) blk_seg[(size_t)(S.nblk_first + b)] = (int)q;
             if (S.fld <= VZ) vowr_.vel_blocks = (int)(S.nblk_first + nb);
-        }
-        if (!segs_h_.empty()) {
-            JV_TRY(alloc(&p, segs_h_.size() * sizeof(SegDev)));
-            vowr_.segs = (const SegDev *)p;
-            JV_CU(cudaMemcpy(p, segs_h_.data(), segs_h_.size() * sizeof(SegDev), cudaMemcpyHostToDevice));
-            JV_TRY(alloc(&p, blk_seg.size() * sizeof(int)));
-            vowr_.blk_seg = (const int *)p;
-            JV_CU(cudaMemcpy(p, blk_seg.data(), blk_seg.size() * sizeof(int), cudaMemcpyHostToDevice));
         }
     }
     JV_CU(cudaStreamSynchronize(stream_));
@@ -880,15 +875,24 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // injection + reverse velocity, stress boundary layers of step it-1
         JV_L("inject_rec", k_inject_rec(R_, rec_d_, nrec_, nt_, st_, off, s));
         JV_L("stress_phy_bwd", k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, off, kc_, s, &mapsF_));
-        // the receiver side's velocity update keeps the split kernels: with
-        // its P-wave velocities it measured no faster fused (cfg2), slower
-        // on x-tiled grids
+        // the receiver side's velocity update: absorbing layers, then gridphy
+        // (with its P-wave velocities, the full-gridext form measured no
+        // faster on cfg2 and slower on x-tiled grids)
         JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
-        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-        JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
-        // UPDATE 2: backward velocity with the imaging condition fused,
-        // reverse stress, velocity boundary layers of step it-1
-        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
+        if (both_vel()) {
+            // the stress boundary layers of step it-1 first: the backward
+            // velocity update reads them
+            JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
+            // UPDATE 1's receiver velocities of gridphy and UPDATE 2's
+            // backward velocities with the imaging condition, one pass
+            JV_L("vel_both_image", k_vel_both(g_, F_, R_, rho_, -dt, dt, rw, shot_img_, kc_, s));
+        } else {
+            JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+            JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
+            // UPDATE 2: backward velocity with the imaging condition fused,
+            // reverse stress, velocity boundary layers of step it-1
+            JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
+        }
         if (fullR_.ok) {
             JV_L("stress_fz_rev", k_stress_full(kRev, g_, R_, dt, wavelet_, st_, off, fullR_, s));
         } else {

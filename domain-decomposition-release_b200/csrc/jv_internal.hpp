@@ -88,13 +88,18 @@ struct SegDev {          // one VOWR face box
 
 // The VOWR boundary store and its face boxes.  Boxes of the velocity
 // fields come first; each box is cut into blocks of 256 threads of vw
-// cells each and blk_seg maps a block to its box.
+// cells each, and a block's box is the last one whose first block is not
+// after it.
 // boundary-store precision (the values of jv_precision)
 constexpr int kStoreF32 = 0, kStoreBF16 = 1, kStoreFP16 = 2;
 
+constexpr int kVowrMaxSegs = 64;  // face boxes of a record: at most 10 fields x 6 faces
+
 struct VowrDev {
-    const SegDev *segs;
-    const int *blk_seg;
+    // the face boxes, in block order, passed to the kernels in their
+    // (constant-bank) parameters: a block finds its box without a load from
+    // global memory
+    SegDev seg[kVowrMaxSegs];
     int vel_blocks, all_blocks;
     long long per_step;  // values of one step's record
     int nslot;           // records in the store
@@ -206,6 +211,8 @@ struct KCfg {
     int zp = 1;          // variant 2: z planes per thread (1 or 2)
     int pml_zp = 1;      // CPML kernels: the same
     int fzq = 0;         // variant 4: run chunks per tile (0: the cost model's choice)
+    int both = 1;        // variants 2-4: the reverse loop's two velocity updates of gridphy in one kernel
+    int both_minb = 3;   // that kernel's register budget: blocks per SM (2, 3 or 4)
 };
 
 // kernels.cu ------------------------------------------------------------
@@ -215,6 +222,11 @@ int k_zero_range(float *p, size_t n, void *stream);
 
 int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w,
               const WaveDev *rev, const ImageDev *img, const KCfg &kc, void *stream);
+// the receiver wavefield's velocity update of gridphy (rev, step dt_rev) and
+// the source wavefield's backward one (src, dt_src) with the imaging
+// condition, in one pass (variants 2-4)
+int k_vel_both(const GridDev &g, const WaveDev &src, const WaveDev &rev, const float *rho, float dt_src, float dt_rev,
+               int rec_w, const ImageDev &img, const KCfg &kc, void *stream);
 // it_off: the kernels of a step read the time step as st->it + it_off (a
 // captured chunk of steps advances st->it once, at its end)
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,

@@ -515,12 +515,14 @@ __device__ __forceinline__ void st4(float *f, int i0, const float *v, int nvalid
     }
 }
 
-// One 4-cell group (x cells pi0..pi0+3 of row pj, plane pk) of the
-// velocity update.
-template <int MODE, bool IMG>
-__device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
-                                           float dt, int rec_w, const WaveDev &rv, const ImageDev &img, int pi0,
-                                           int pj, int pk) {
+// The velocity update of one 4-cell group (x cells pi0..pi0+3 of row pj,
+// plane pk) of wavefield w, stored, with the updated velocities left in
+// v[3][4] and, for the modes that carry them, the P-wave velocities in
+// p[3][4].
+template <int MODE>
+__device__ __forceinline__ void vel_update4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
+                                            float dt, int rec_w, int pi0, int pj, int pk, float v[3][4],
+                                            float p[3][4]) {
     constexpr bool kP = (MODE == kBwd || MODE == kRev);
     const int nvalid = min(4, g.px - pi0);
     const int sy = (int)g.sy, sz = (int)g.sz;
@@ -570,81 +572,101 @@ __device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, c
         const float4 r4 = ld4(rho, i0);
         dtr[0] = dt / r4.x; dtr[1] = dt / r4.y; dtr[2] = dt / r4.z; dtr[3] = dt / r4.w;
     }
-    float vx[4], vy[4], vz[4];
-    f4a(vx, ldw4(w.f[VX], i0));
-    f4a(vy, ldw4(w.f[VY], i0));
-    f4a(vz, ldw4(w.f[VZ], i0));
+    f4a(v[0], ldw4(w.f[VX], i0));
+    f4a(v[1], ldw4(w.f[VY], i0));
+    f4a(v[2], ldw4(w.f[VZ], i0));
 #pragma unroll
     for (int c = 0; c < 4; c++) {
-        vx[c] += dtr[c] * Dx[c];
-        vy[c] += dtr[c] * Dy[c];
-        vz[c] += dtr[c] * Dz[c];
+        v[0][c] += dtr[c] * Dx[c];
+        v[1][c] += dtr[c] * Dy[c];
+        v[2][c] += dtr[c] * Dz[c];
     }
-    st4(w.f[VX], i0, vx, nvalid);
-    st4(w.f[VY], i0, vy, nvalid);
-    st4(w.f[VZ], i0, vz, nvalid);
+    st4(w.f[VX], i0, v[0], nvalid);
+    st4(w.f[VY], i0, v[1], nvalid);
+    st4(w.f[VZ], i0, v[2], nvalid);
     if (kP) {
         // P-wave velocity from the pressure-like field sau (Dp on every axis)
-        float px[4], py[4], pz[4];
         xwin(w.f[SAU], i0, win);
         xdp(win, cx, t);
-        f4a(px, ldw4(w.f[VXP], i0));
+        f4a(p[0], ldw4(w.f[VXP], i0));
 #pragma unroll
-        for (int c = 0; c < 4; c++) px[c] += dtr[c] * (t[c] * rdx);
+        for (int c = 0; c < 4; c++) p[0][c] += dtr[c] * (t[c] * rdx);
         sdp(w.f[SAU], i0, sy, cy, t);
-        f4a(py, ldw4(w.f[VYP], i0));
+        f4a(p[1], ldw4(w.f[VYP], i0));
 #pragma unroll
-        for (int c = 0; c < 4; c++) py[c] += dtr[c] * (t[c] * rdy);
+        for (int c = 0; c < 4; c++) p[1][c] += dtr[c] * (t[c] * rdy);
         sdp(w.f[SAU], i0, sz, cz, t);
-        f4a(pz, ldw4(w.f[VZP], i0));
+        f4a(p[2], ldw4(w.f[VZP], i0));
 #pragma unroll
-        for (int c = 0; c < 4; c++) pz[c] += dtr[c] * (t[c] * rdz);
-        st4(w.f[VXP], i0, px, nvalid);
-        st4(w.f[VYP], i0, py, nvalid);
-        st4(w.f[VZP], i0, pz, nvalid);
-        if (IMG) {
-            float rvx[4], rvy[4], rvz[4], rpx[4], rpy[4], rpz[4];
-            f4a(rvx, ld4(rv.f[VX], i0));
-            f4a(rvy, ld4(rv.f[VY], i0));
-            f4a(rvz, ld4(rv.f[VZ], i0));
-            f4a(rpx, ld4(rv.f[VXP], i0));
-            f4a(rpy, ld4(rv.f[VYP], i0));
-            f4a(rpz, ld4(rv.f[VZP], i0));
-            const long long o0 = pi0 + (long long)g.px * (pj + (long long)g.py * pk);
-            float a[5][4];
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const float rsx = rvx[c] - rpx[c], rsy = rvy[c] - rpy[c], rsz = rvz[c] - rpz[c];
-                const float ssx = vx[c] - px[c], ssy = vy[c] - py[c], ssz = vz[c] - pz[c];
-                a[0][c] = px[c] * px[c] + py[c] * py[c] + pz[c] * pz[c];
-                a[1][c] = px[c] * rpx[c] + py[c] * rpy[c] + pz[c] * rpz[c];
-                a[2][c] = px[c] * rsx + py[c] * rsy + pz[c] * rsz;
-                a[3][c] = ssx * rpx[c] + ssy * rpy[c] + ssz * rpz[c];
-                a[4][c] = ssx * rsx + ssy * rsy + ssz * rsz;
-            }
-            float *dst[5] = {img.ip, img.pp, img.ps, img.sp, img.ss};
-            bool al = nvalid == 4;
-#pragma unroll
-            for (int q = 0; q < 5; q++) al = al && ((reinterpret_cast<uintptr_t>(dst[q] + o0) & 15) == 0);
-            if (al) {
-#pragma unroll
-                for (int q = 0; q < 5; q++) {
-                    float4 *p4 = reinterpret_cast<float4 *>(dst[q] + o0);
-                    float4 v = *p4;
-                    v.x += a[q][0]; v.y += a[q][1]; v.z += a[q][2]; v.w += a[q][3];
-                    *p4 = v;
-                }
-            } else {
-#pragma unroll
-                for (int q = 0; q < 5; q++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        if (c < nvalid) dst[q][o0 + c] += a[q][c];
-            }
-        }
+        for (int c = 0; c < 4; c++) p[2][c] += dtr[c] * (t[c] * rdz);
+        st4(w.f[VXP], i0, p[0], nvalid);
+        st4(w.f[VYP], i0, p[1], nvalid);
+        st4(w.f[VZP], i0, p[2], nvalid);
     }
 }
 
+// Zero-lag imaging condition of one group (RTM/rtm3d_0_image_module/
+// rtm3d_iamge_kernel.hpp:6-51): P = p, S = v - p of the reconstructed
+// source (v, p) and of the receiver wavefield (rv, rp), added into the
+// shot's FP32 images.
+__device__ __forceinline__ void image4(const GridDev &g, const ImageDev &img, int pi0, int pj, int pk,
+                                       const float v[3][4], const float p[3][4], const float rv[3][4],
+                                       const float rp[3][4]) {
+    const int nvalid = min(4, g.px - pi0);
+    const long long o0 = pi0 + (long long)g.px * (pj + (long long)g.py * pk);
+    float a[5][4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const float rsx = rv[0][c] - rp[0][c], rsy = rv[1][c] - rp[1][c], rsz = rv[2][c] - rp[2][c];
+        const float ssx = v[0][c] - p[0][c], ssy = v[1][c] - p[1][c], ssz = v[2][c] - p[2][c];
+        a[0][c] = p[0][c] * p[0][c] + p[1][c] * p[1][c] + p[2][c] * p[2][c];
+        a[1][c] = p[0][c] * rp[0][c] + p[1][c] * rp[1][c] + p[2][c] * rp[2][c];
+        a[2][c] = p[0][c] * rsx + p[1][c] * rsy + p[2][c] * rsz;
+        a[3][c] = ssx * rp[0][c] + ssy * rp[1][c] + ssz * rp[2][c];
+        a[4][c] = ssx * rsx + ssy * rsy + ssz * rsz;
+    }
+    float *dst[5] = {img.ip, img.pp, img.ps, img.sp, img.ss};
+    bool al = nvalid == 4;
+#pragma unroll
+    for (int q = 0; q < 5; q++) al = al && ((reinterpret_cast<uintptr_t>(dst[q] + o0) & 15) == 0);
+    if (al) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            float4 *p4 = reinterpret_cast<float4 *>(dst[q] + o0);
+            float4 s4 = *p4;
+            s4.x += a[q][0]; s4.y += a[q][1]; s4.z += a[q][2]; s4.w += a[q][3];
+            *p4 = s4;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 5; q++)
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                if (c < nvalid) dst[q][o0 + c] += a[q][c];
+    }
+}
+
+// One 4-cell group of the velocity update of wavefield w; with IMG (the
+// backward update) the imaging condition against the receiver wavefield rv
+// follows.
+template <int MODE, bool IMG>
+__device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
+                                           float dt, int rec_w, const WaveDev &rv, const ImageDev &img, int pi0,
+                                           int pj, int pk) {
+    const int i0 = (int)g.xoff + (pi0 + g.m) + (int)g.sy * (pj + g.m) + (int)g.sz * (pk + g.m);
+    float v[3][4], p[3][4];
+    vel_update4<MODE>(g, w, rho, dt, rec_w, pi0, pj, pk, v, p);
+    if (IMG) {
+        float r[3][4], rp[3][4];
+        f4a(r[0], ld4(rv.f[VX], i0));
+        f4a(r[1], ld4(rv.f[VY], i0));
+        f4a(r[2], ld4(rv.f[VZ], i0));
+        f4a(rp[0], ld4(rv.f[VXP], i0));
+        f4a(rp[1], ld4(rv.f[VYP], i0));
+        f4a(rp[2], ld4(rv.f[VZP], i0));
+        image4(g, img, pi0, pj, pk, v, p, r, rp);
+    }
+}
 
 // Blocks of blockDim.x groups x blockDim.y rows x ZP planes; a thread
 // updates its group in ZP consecutive planes.
@@ -659,6 +681,31 @@ __global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, co
         const int pk = blockIdx.z * ZP + zz;
         if (pk < g.pz) vel_group4<MODE, IMG>(g, w, rho, dt, rec_w, rv, img, pi0, pj, pk);
     }
+}
+
+// The reverse loop's two velocity updates of gridphy in one pass: per
+// group the receiver wavefield's update (rev, time forward, P-wave
+// velocities included), then the source wavefield's backward update with
+// the rtm_backward rim orders (src), then the imaging condition from both
+// sets of updated velocities, still in registers.  The
+// arithmetic of each update is that of vel_group4<kRev> and
+// vel_group4<kBwd, true>, so the results are the same, bit for bit; the
+// receiver velocities are not read back and rho comes from DRAM once (196
+// instead of 224 bytes a cell).
+// The two updates touch different arrays and neither reads what the other
+// writes, so their order within a step is free.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) vel_phy_v4_both(GridDev g, WaveDev src, WaveDev rev,
+                                                            const float *__restrict__ rho, float dt_src, float dt_rev,
+                                                            int rec_w, ImageDev img) {
+    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
+    const int pk = blockIdx.z;
+    if (pi0 >= g.px || pj >= g.py || pk >= g.pz) return;
+    float rv[3][4], rp[3][4], v[3][4], p[3][4];
+    vel_update4<kRev>(g, rev, rho, dt_rev, rec_w, pi0, pj, pk, rv, rp);
+    vel_update4<kBwd>(g, src, rho, dt_src, rec_w, pi0, pj, pk, v, p);
+    image4(g, img, pi0, pj, pk, v, p, rv, rp);
 }
 
 // One 4-cell group of the stress update (source fused).
@@ -2366,16 +2413,28 @@ __global__ void inject_rec(WaveDev w, const long long *__restrict__ rec, int nre
 
 // ---------------------------------------------------------------- VOWR
 
-// One block per 256 elements of one face box; the block finds its box by
-// the prefix of block counts.  pack: field -> store[slot]; else the
-// reverse.  which: 0 all fields, 1 velocities only, 2 stresses only.
-// blocks [b0, b0 + gridDim.x) of the face boxes; one cell per thread
-__global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, VowrDev v, const StepState *__restrict__ st,
+// The box of block b: the last box whose first block is not after b (a
+// binary search over the table in the kernel parameters, block-uniform).
+__device__ __forceinline__ int vowr_box(const VowrDev &v, int b) {
+    int lo = 0, hi = v.nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if ((int)v.seg[mid].nblk_first <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One block per 256 (x vw) elements of one face box.  pack: field ->
+// store[slot]; else the reverse.  Blocks [b0, b0 + gridDim.x) of the face
+// boxes (all of them, the velocity boxes or the stress boxes).
+__global__ void __launch_bounds__(256) vowr(GridDev g, const __grid_constant__ WaveDev w,
+                                            const __grid_constant__ VowrDev v, const StepState *__restrict__ st,
                                             int slot_shift, int pack, int b0) {
     const int slot = st->it + slot_shift;
     if (slot < 0 || slot >= v.nslot) return;
     const int b = b0 + (int)blockIdx.x;
-    const SegDev &S = v.segs[v.blk_seg[b]];
+    const SegDev &S = v.seg[vowr_box(v, b)];
     const int e = ((b - (int)S.nblk_first) * 256 + (int)threadIdx.x) * S.vw;
     const int cnt = S.nxb * S.nyb * S.nzb;
     if (e >= cnt) return;
@@ -2400,16 +2459,17 @@ __global__ void __launch_bounds__(256) vowr(GridDev g, WaveDev w, VowrDev v, con
 // step (amax[parity][box], atomic max of the float bits, non-negative);
 // the other parity's row, last read by the previous step's pass 2, is
 // cleared for the next step.
-__global__ void __launch_bounds__(256) vowr_amax(GridDev g, WaveDev w, VowrDev v, const StepState *__restrict__ st,
-                                                 int slot_shift) {
+__global__ void __launch_bounds__(256) vowr_amax(GridDev g, const __grid_constant__ WaveDev w,
+                                                 const __grid_constant__ VowrDev v,
+                                                 const StepState *__restrict__ st, int slot_shift) {
     const int slot = st->it + slot_shift;
     if (slot < 0 || slot >= v.nslot) return;
     unsigned *cur = v.amax + (slot & 1) * v.nseg, *nxt = v.amax + ((slot + 1) & 1) * v.nseg;
     if (blockIdx.x == 0)
         for (int q = threadIdx.x; q < v.nseg; q += blockDim.x) nxt[q] = 0u;
     const int b = (int)blockIdx.x;
-    const int sg = v.blk_seg[b];
-    const SegDev &S = v.segs[sg];
+    const int sg = vowr_box(v, b);
+    const SegDev &S = v.seg[sg];
     const int e = (b - (int)S.nblk_first) * 256 + (int)threadIdx.x;
     float a = 0.f;
     if (e < S.nxb * S.nyb * S.nzb) {
@@ -2426,13 +2486,14 @@ __global__ void __launch_bounds__(256) vowr_amax(GridDev g, WaveDev w, VowrDev v
 
 // Pass 2 (pack) and the unpack of a 16-bit store: value = q * scale.
 template <int PREC>
-__global__ void __launch_bounds__(256) vowr16(GridDev g, WaveDev w, VowrDev v, const StepState *__restrict__ st,
+__global__ void __launch_bounds__(256) vowr16(GridDev g, const __grid_constant__ WaveDev w,
+                                              const __grid_constant__ VowrDev v, const StepState *__restrict__ st,
                                               int slot_shift, int pack, int b0) {
     const int slot = st->it + slot_shift;
     if (slot < 0 || slot >= v.nslot) return;
     const int b = b0 + (int)blockIdx.x;
-    const int sg = v.blk_seg[b];
-    const SegDev &S = v.segs[sg];
+    const int sg = vowr_box(v, b);
+    const SegDev &S = v.seg[sg];
     const int e = (b - (int)S.nblk_first) * 256 + (int)threadIdx.x;
     if (e >= S.nxb * S.nyb * S.nzb) return;
     const int t = e / S.nxb;
@@ -2672,6 +2733,19 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
         break;
     default: return (int)cudaErrorInvalidValue;
     }
+    return cerr();
+}
+
+int k_vel_both(const GridDev &g, const WaveDev &src, const WaveDev &rev, const float *rho, float dt_src, float dt_rev,
+               int rec_w, const ImageDev &img, const KCfg &kc, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    KCfg k1 = kc;
+    k1.zp = 1;
+    dim3 b, gr;
+    v4_shape(g, k1, &b, &gr);
+    if (kc.both_minb == 4) vel_phy_v4_both<4><<<gr, b, 0, s>>>(g, src, rev, rho, dt_src, dt_rev, rec_w, img);
+    else if (kc.both_minb == 2) vel_phy_v4_both<2><<<gr, b, 0, s>>>(g, src, rev, rho, dt_src, dt_rev, rec_w, img);
+    else vel_phy_v4_both<3><<<gr, b, 0, s>>>(g, src, rev, rho, dt_src, dt_rev, rec_w, img);
     return cerr();
 }
 
