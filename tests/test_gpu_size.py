@@ -1,0 +1,79 @@
+"""Parity at the workload sizes, on the GPU.
+
+* cfg1 in full (100^3 + 10 CPML, 1000 steps, 8 receivers): the traces
+  against the FP64 oracle run here on every host core (about 10 s on 16
+  cores) and against the reference binary's own run of the same inputs
+  (tests/golden/size_cfg1.npz).  Measured: <= 7.4e-7 and <= 7.9e-7.
+* cfg2 in full (200^3 + 20 CPML, 2000 steps, 40 000 receivers), VOWR
+  rec_width 1 and 4: one RTM shot; the traces of a 4 x 4 receiver subset
+  and the five raw images on the planes z = 100 and y = 100 against the
+  FP64 oracle's and the reference binary's outputs
+  (tests/golden/size_cfg2_w*.npz, made by tests/golden/make_size_pins.py on
+  a B200, which also measured the whole fields: traces <= 2.8e-6 vs FP64
+  and <= 3.5e-6 vs the reference; raw images 4.3e-6 .. 3.3e-5 vs FP64 and
+  8e-6 .. 2.3e-5 vs the reference, whose own FP32 error against the FP64
+  oracle is 4e-6 .. 2.4e-5).
+
+Bounds: traces 1e-5; raw images 1e-4 against both (the workload's image
+bound is 1e-3 against FP64); rec_width 4 reconstructs the source wavefield
+exactly, so its reconstruction residual is at the FP32 floor.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import pkg, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+jv = pkg()
+synth = pkg("synth")
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+KINDS = ("ip", "pp", "ps", "sp", "ss")
+
+
+def test_cfg1_full_vs_fp64_oracle_and_reference(oracle):
+    s = synth.cfg1()
+    with jv.Context.from_survey(s) as ctx:
+        tr = ctx.forward(0)
+    p = oracle.Problem(s.nx, s.ny, s.nz, s.pml, s.dx, s.dy, s.dz, s.dt, s.fm, s.T, s.rec_width, s.shots, s.recvs,
+                       s.vp, s.vs, s.rho, nthreads=os.cpu_count() or 1)
+    ref64 = oracle.forward(p)
+    f = np.load(os.path.join(GOLD, "size_cfg1.npz"))
+    for q, c in enumerate(("vx", "vy", "vz")):
+        assert tr[q].shape == (8, 1000)
+        assert rel_l2(tr[q], ref64[q]) <= 5e-6, (c, rel_l2(tr[q], ref64[q]))
+        assert rel_l2(tr[q], f[f"ref_tr_{c}"]) <= 5e-6, (c, rel_l2(tr[q], f[f"ref_tr_{c}"]))
+        # the fixture's oracle traces are this oracle's (rounded to FP32)
+        assert rel_l2(f[f"oracle_tr_{c}"], ref64[q]) <= 1e-7
+
+
+@pytest.mark.parametrize("w", [1, 4])
+def test_cfg2_full_vs_fp64_oracle_and_reference(w):
+    import torch
+
+    s = synth.cfg2(rec_width=w)
+    f = np.load(os.path.join(GOLD, f"size_cfg2_w{w}.npz"))
+    sub = torch.as_tensor(f["subset"].astype(np.int64), device="cuda:0")
+    with jv.Context.from_survey(s) as ctx:
+        i = ctx.info()
+        obs = torch.empty((3, i.n_recv, i.nt), dtype=torch.float32, device="cuda:0")
+        ptrs = [obs[q].data_ptr() for q in range(3)]
+        ctx.forward_device(0, ptrs)
+        ctx.image_reset()
+        ctx.rtm_shot_device(0, ptrs)
+        img = ctx.images()
+        e0, e1 = ctx.reconstruction_energy()
+        tr = [obs[q].index_select(0, sub).cpu().numpy() for q in range(3)]
+    for src in ("oracle", "ref"):
+        for q, c in enumerate(("vx", "vy", "vz")):
+            e = rel_l2(tr[q], f[f"{src}_tr_{c}"])
+            assert e <= 1e-5, (src, c, e)
+        for k in KINDS:
+            a = np.concatenate([img[k][100].ravel(), img[k][:, 100].ravel()])
+            b = np.concatenate([f[f"{src}_{k}_z100"].ravel(), f[f"{src}_{k}_y100"].ravel()])
+            e = rel_l2(a, b)
+            assert e <= 1e-4, (src, k, e)
+    if w == 4:
+        assert e1 / e0 < 1e-5, e1 / e0  # exact reconstruction, up to FP32 rounding
