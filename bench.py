@@ -523,8 +523,9 @@ SIZE_FIXTURES = {("cfg2_rtm_200_w1", 1): "size_cfg2_w1", ("cfg2_rtm_200_w4", 4):
 
 def accuracy_leg(ctx, s, obs, ptrs, rec_width):
     """The timed configuration's accuracy, measured on this run: one RTM
-    shot's five raw images on the planes z = 100 and y = 100 and the traces
-    of a 4 x 4 receiver subset, against the FP64 oracle's and the reference
+    shot's five raw images sampled at every 4th cell of every axis and on the
+    plane y = 100, and the traces of 16 receivers around the source, against
+    the FP64 oracle's and the reference
     binary's outputs of the same shot (tests/golden/size_cfg2_w*.npz, made
     by tests/golden/make_size_pins.py on a B200); plus the whole-field
     figures that script measured (tests/golden/size_pins.json)."""
@@ -546,7 +547,7 @@ def accuracy_leg(ctx, s, obs, ptrs, rec_width):
         return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
     import torch
-    planes = {"z100": lambda a: a[100], "y100": lambda a: a[:, 100]}
+    planes = {"d4": lambda a: a[2::4, 2::4, 2::4], "y100": lambda a: a[:, 100]}
     idx = torch.as_tensor(np.asarray(sub, dtype=np.int64), device=obs.device)
     tr = [obs[q].index_select(0, idx).cpu().numpy() for q in range(3)]
     out = {}
@@ -560,8 +561,9 @@ def accuracy_leg(ctx, s, obs, ptrs, rec_width):
         out["vs_fp64_oracle" if src == "oracle" else "vs_reference_binary"] = {"traces": t, "images": im}
     worst = max(out["vs_fp64_oracle"]["images"].values())
     res = {"metric": "relative L2", **out, "image_bound_vs_fp64": 1e-3, "within_bound": worst <= 1e-3,
-           "sample": "this run's RTM shot: traces of 16 receivers (4 x 4 grid) x all steps; the five raw (stacked, "
-                     "uncompensated) images on the planes z = 100 and y = 100 (80 000 of 8 M cells)"}
+           "sample": "this run's RTM shot: traces of 16 receivers around the source x all steps; the five raw "
+                     "(stacked, uncompensated) images at every 4th cell of every axis and on the vertical plane "
+                     "y = 100 through the source (165 000 of 8 M cells)"}
     summ = os.path.join(gold, "size_pins.json")
     key = name[len("size_"):]
     if os.path.exists(summ):

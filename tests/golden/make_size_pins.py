@@ -21,10 +21,11 @@ core, and writes
                          images, the Laplacian and the compensated images)
                          between each pair of the three, with run times;
   OUT/size_<case>.npz    a compact fixture for the GPU tests and the bench:
-                         the FP64 oracle's and the reference's traces of a
-                         4 x 4 receiver subset (cfg2) or of every receiver
-                         (cfg1), and their raw images on the planes z = 100
-                         and y = 100 (cfg2).
+                         the FP64 oracle's and the reference's traces of 16
+                         receivers around the source (cfg2) or of every
+                         receiver (cfg1), and their raw images sampled at
+                         every 4th cell of every axis and on the vertical
+                         plane y = 100 through the source (cfg2).
 
 ``--collect OUT`` copies the fixtures and one summary (size_pins.json,
 every case's figures) into tests/golden/.  Inputs are regenerated from
@@ -56,8 +57,11 @@ synth = importlib.import_module("domain-decomposition-release_b200.synth")
 project = importlib.import_module("domain-decomposition-release_b200.project")
 
 KINDS = ("ip", "pp", "ps", "sp", "ss")
-PLANES = {"z100": (0, 100), "y100": (1, 100)}  # (axis of (nz, ny, nx), index)
-SUBSET = [j * 200 + i for j in (25, 75, 125, 175) for i in (25, 75, 125, 175)]  # cfg2 receiver indices
+# image samples: every 4th cell of every axis (a uniform sample of the whole
+# volume) and the vertical plane y = 100 through the source
+SAMPLES = ("d4", "y100")
+# cfg2 receiver indices (j * 200 + i): 16 receivers around the source
+SUBSET = [j * 200 + i for j in (85, 95, 105, 115) for i in (85, 95, 105, 115)]
 
 
 def case_survey(name: str):
@@ -85,9 +89,11 @@ def read_traces_fast(path: str, nrec: int, nt: int) -> np.ndarray:
     return a.reshape(nrec, nt)
 
 
-def plane(a: np.ndarray, key: str) -> np.ndarray:
-    ax, i = PLANES[key]
-    return np.ascontiguousarray(np.take(a, i, axis=ax))
+def sample(a: np.ndarray, key: str) -> np.ndarray:
+    """An image sample of (nz, ny, nx) gridphy: 'd4' or 'y100'."""
+    if key == "d4":
+        return np.ascontiguousarray(a[2::4, 2::4, 2::4])
+    return np.ascontiguousarray(a[:, 100, :])
 
 
 def host_mem_gb() -> float:
@@ -124,7 +130,9 @@ def run_reference(s, d: str) -> dict:
     raw = {k: comp[k].astype(np.float64) * np.where(ip > 3.4e-38, ip, 1.0) for k in comp}
     raw["ip"] = ip
     with open(os.path.join(d, "ref.log")) as f:
-        tail = f.read()[-2000:]
+        lines = f.read().splitlines()
+    # the reference's own timers (cuda_toc lines) and the end of its log
+    tail = "\n".join([ln for ln in lines if "time" in ln] + lines[-5:])[-4000:]
     return {"traces": tr, "raw": raw, "comp": comp, "lap_pp": img["lap_pp"], "wall_s": wall, "log_tail": tail}
 
 
@@ -194,10 +202,10 @@ def fixture(name: str, s, o: dict, r: dict) -> dict:
         fx[f"oracle_tr_{c}"] = t[SUBSET].astype(np.float32)
     for c, t in zip(("vx", "vy", "vz"), r["traces"]):
         fx[f"ref_tr_{c}"] = t[SUBSET].astype(np.float32)
-    for pk in PLANES:
+    for pk in SAMPLES:
         for k in KINDS:
-            fx[f"oracle_{k}_{pk}"] = plane(o["raw"][k], pk).astype(np.float32)
-            fx[f"ref_{k}_{pk}"] = plane(r["raw"][k], pk).astype(np.float32)
+            fx[f"oracle_{k}_{pk}"] = sample(o["raw"][k], pk).astype(np.float32)
+            fx[f"ref_{k}_{pk}"] = sample(r["raw"][k], pk).astype(np.float32)
     return fx
 
 
@@ -222,7 +230,7 @@ def run_case(name: str, out: str) -> None:
                           "gpu_forward_ms": round(g["forward_ms"], 2), "gpu_rtm_ms": round(g.get("rtm_ms", 0.0), 2),
                           "oracle_forward_s": round(o["forward_s"], 2), "oracle_rtm_s": round(o.get("rtm_s", 0.0), 2),
                           "oracle_cores": o["cores"]},
-                "reference_log_tail": r["log_tail"][-600:]})
+                "reference_log_tail": r["log_tail"]})
     with open(os.path.join(out, name + ".json"), "w") as f:
         json.dump(res, f, indent=1)
     np.savez_compressed(os.path.join(out, f"size_{name}.npz"), **fixture(name, s, o, r))
@@ -236,7 +244,8 @@ def collect(out: str) -> None:
         if fn.endswith(".json") and fn[:-5] in ("cfg1", "cfg2_w1", "cfg2_w4"):
             with open(os.path.join(out, fn)) as f:
                 d = json.load(f)
-            d.pop("reference_log_tail", None)
+            log = d.pop("reference_log_tail", "")
+            d["reference_timers"] = [ln.strip() for ln in log.splitlines() if "time" in ln][:20]
             summary[fn[:-5]] = d
         if fn.startswith("size_") and fn.endswith(".npz"):
             shutil.copy(os.path.join(out, fn), os.path.join(HERE, fn))

@@ -90,7 +90,7 @@ def test_oracle_matches_reference_at_size(w):
     for c in ("vx", "vy", "vz"):
         assert rel_l2(f[f"oracle_tr_{c}"], f[f"ref_tr_{c}"]) <= 1e-5
     for k in ("ip", "pp", "ps", "sp", "ss"):
-        for pk in ("z100", "y100"):
+        for pk in ("d4", "y100"):
             assert rel_l2(f[f"oracle_{k}_{pk}"], f[f"ref_{k}_{pk}"]) <= 1e-4, (k, pk)
     with open(f"{gold}/size_pins.json") as fh:
         d = json.load(fh)[f"cfg2_w{w}"]
