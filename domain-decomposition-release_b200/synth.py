@@ -158,6 +158,22 @@ def cfg3(nt: int = 3000, seed: int = 3, rec_step: int = 4) -> Survey:
                   _pos(rec, d), name="cfg3_large_676x676x210", seed=seed)
 
 
+def cfg3_half(seed: int = 3) -> Survey:
+    """cfg3 at half resolution, for the FP64 oracle: the same 6760 x 6760 x
+    2100 m model (cfg3's generator on 338 x 338 x 105 cells of 20 m), 10
+    CPML cells, dt = 1.6 ms (cfg3's Courant number), 1500 steps (its 2.4 s)
+    and a 10 Hz Ricker (its points per wavelength); source at the surface
+    centre at depth 3 cells, receivers every 2 cells (40 m, as cfg3's) at z = 3."""
+    nx, ny, nz = 338, 338, 105
+    vp = layered_vp(nx, ny, nz, seed, n_layers=4, vmin=1800, vmax=4500, dip=True)
+    vp, vs, rho = gardner(vp)
+    d = (20.0, 20.0, 20.0)
+    jj, ii = np.meshgrid(np.arange(0, ny, 2), np.arange(0, nx, 2), indexing="ij")
+    rec = np.stack([ii.ravel(), jj.ravel(), np.full(ii.size, 3)], axis=1)
+    return Survey(nx, ny, nz, 10, 20.0, 20.0, 20.0, 1.6e-3, 10.0, 1500, vp, vs, rho,
+                  _pos([(nx // 2, ny // 2, 3)], d), _pos(rec, d), name="cfg3_half_338x338x105", seed=seed)
+
+
 def scaled_cfg2(n: int, nt: int, rec_width: int = 1, seed: int = 2, pml: int = 20) -> Survey:
     """cfg2's construction at another size (same spacing, source at the
     centre of the surface at depth 5 cells, full receiver plane at z=5)."""

@@ -10,6 +10,9 @@ quoted, on a GPU box:
             VOWR rec_width 1
   cfg2_w4   the same at rec_width 4 (the FP64 oracle's boundary store alone
             takes about 94 GB of host memory; skipped when the host has less)
+  cfg3_half the precision configuration at half resolution (synth.cfg3_half:
+            338 x 338 x 105 + 10 CPML, 20 m, 1500 steps): the GPU path with
+            the FP32, FP16 and BF16 boundary stores
 
 For each case, ``--run OUT`` writes the reference project, runs the
 reference binary (oracle/_ref/jvref_rtm_w{1,4}, built by oracle/build_ref.sh),
@@ -71,7 +74,16 @@ def case_survey(name: str):
         return synth.cfg2(rec_width=1)
     if name == "cfg2_w4":
         return synth.cfg2(rec_width=4)
+    if name == "cfg3_half":
+        return synth.cfg3_half()
     raise KeyError(name)
+
+
+def subset_of(name: str) -> list:
+    """16 receivers around the source (indices into the survey's list)."""
+    if name == "cfg3_half":  # a 169 x 169 receiver grid, the source under (84.5, 84.5)
+        return [j * 169 + i for j in (76, 82, 88, 94) for i in (76, 82, 88, 94)]
+    return SUBSET
 
 
 def rel_l2(a, b) -> float:
@@ -136,14 +148,14 @@ def run_reference(s, d: str) -> dict:
     return {"traces": tr, "raw": raw, "comp": comp, "lap_pp": img["lap_pp"], "wall_s": wall, "log_tail": tail}
 
 
-def run_gpu(s) -> dict:
+def run_gpu(s, precision: int = 0) -> dict:
     jv = importlib.import_module("domain-decomposition-release_b200")
-    with jv.Context.from_survey(s) as ctx:
+    with jv.Context.from_survey(s, precision=precision) as ctx:
         t0 = time.time()
         tr = ctx.forward(0)
         fwd_ms = ctx.last_ms()
         out = {"traces": [np.asarray(t) for t in tr], "forward_ms": fwd_ms}
-        if s.name.startswith("cfg2"):
+        if not s.name.startswith("cfg1"):
             ctx.image_reset()
             ctx.rtm_shot(0, tr)
             out["rtm_ms"] = ctx.last_ms()
@@ -163,7 +175,7 @@ def run_oracle(s) -> dict:
     t0 = time.time()
     tr = O.forward(p)
     out = {"traces": list(tr), "forward_s": time.time() - t0}
-    if s.name.startswith("cfg2"):
+    if not s.name.startswith("cfg1"):
         t1 = time.time()
         raw = O.rtm_shot(p, tr)
         out["rtm_s"] = time.time() - t1
@@ -189,6 +201,21 @@ def compare(s, g: dict, o: dict, r: dict) -> dict:
     return res
 
 
+def precision_study(g: dict, extra: dict, o: dict, r: dict) -> dict:
+    """16-bit boundary stores (extra: "fp16" / "bf16" GPU runs) against the
+    FP64 oracle, the reference and the FP32-store GPU run."""
+    out = {}
+    for tag, a in extra.items():
+        out[tag] = {
+            "raw_images_vs_oracle": {k: rel_l2(a["raw"][k], o["raw"][k]) for k in KINDS},
+            "raw_images_vs_reference": {k: rel_l2(a["raw"][k], r["raw"][k]) for k in KINDS},
+            "raw_images_vs_fp32_store": {k: rel_l2(a["raw"][k], g["raw"][k]) for k in KINDS},
+            "laplacian_pp_vs_oracle": rel_l2(a["lap"]["pp"], o["lap"]["pp"]),
+            "traces_vs_fp32_store": {c: rel_l2(x, y) for c, x, y in zip(("vx", "vy", "vz"), a["traces"], g["traces"])},
+            "rtm_ms": round(a["rtm_ms"], 2)}
+    return out
+
+
 def fixture(name: str, s, o: dict, r: dict) -> dict:
     fx = {"case": np.array(name)}
     if name == "cfg1":
@@ -197,11 +224,12 @@ def fixture(name: str, s, o: dict, r: dict) -> dict:
         for c, t in zip(("vx", "vy", "vz"), r["traces"]):
             fx[f"ref_tr_{c}"] = t.astype(np.float32)
         return fx
-    fx["subset"] = np.array(SUBSET, dtype=np.int32)
+    sub = subset_of(name)
+    fx["subset"] = np.array(sub, dtype=np.int32)
     for c, t in zip(("vx", "vy", "vz"), o["traces"]):
-        fx[f"oracle_tr_{c}"] = t[SUBSET].astype(np.float32)
+        fx[f"oracle_tr_{c}"] = t[sub].astype(np.float32)
     for c, t in zip(("vx", "vy", "vz"), r["traces"]):
-        fx[f"ref_tr_{c}"] = t[SUBSET].astype(np.float32)
+        fx[f"ref_tr_{c}"] = t[sub].astype(np.float32)
     for pk in SAMPLES:
         for k in KINDS:
             fx[f"oracle_{k}_{pk}"] = sample(o["raw"][k], pk).astype(np.float32)
@@ -211,7 +239,7 @@ def fixture(name: str, s, o: dict, r: dict) -> dict:
 
 def run_case(name: str, out: str) -> None:
     s = case_survey(name)
-    need = {"cfg2_w4": 150.0, "cfg2_w1": 40.0}.get(name, 4.0)
+    need = {"cfg2_w4": 150.0, "cfg2_w1": 40.0, "cfg3_half": 40.0}.get(name, 4.0)
     if host_mem_gb() < need:
         print(f"{name}: skipped, {host_mem_gb():.0f} GB of host memory available, {need:.0f} needed", flush=True)
         return
@@ -220,10 +248,15 @@ def run_case(name: str, out: str) -> None:
     r = run_reference(s, d)
     print(f"{name}: reference {r['wall_s']:.1f} s; gpu ...", flush=True)
     g = run_gpu(s)
+    extra = {}
+    if name == "cfg3_half":
+        extra = {"fp16_store": run_gpu(s, 2), "bf16_store": run_gpu(s, 1)}
     print(f"{name}: gpu {g['wall_s']:.1f} s; oracle ...", flush=True)
     o = run_oracle(s)
     print(f"{name}: oracle {o.get('forward_s', 0) + o.get('rtm_s', 0):.1f} s", flush=True)
     res = compare(s, g, o, r)
+    if extra:
+        res["boundary_store_precision"] = precision_study(g, extra, o, r)
     res.update({"case": name, "grid_phy": [s.nx, s.ny, s.nz], "pml": s.pml, "nt": s.nt, "rec_width": s.rec_width,
                 "n_recv": int(s.recvs.shape[0]), "seed": s.seed,
                 "times": {"reference_binary_wall_s": round(r["wall_s"], 2),
@@ -239,9 +272,15 @@ def run_case(name: str, out: str) -> None:
 
 
 def collect(out: str) -> None:
+    """Adds the cases run into OUT to tests/golden/ (the fixtures, and their
+    figures merged into size_pins.json)."""
+    dst = os.path.join(HERE, "size_pins.json")
     summary = {}
+    if os.path.exists(dst):
+        with open(dst) as f:
+            summary = json.load(f)
     for fn in sorted(os.listdir(out)):
-        if fn.endswith(".json") and fn[:-5] in ("cfg1", "cfg2_w1", "cfg2_w4"):
+        if fn.endswith(".json") and fn[:-5] in ("cfg1", "cfg2_w1", "cfg2_w4", "cfg3_half"):
             with open(os.path.join(out, fn)) as f:
                 d = json.load(f)
             log = d.pop("reference_log_tail", "")
@@ -250,7 +289,7 @@ def collect(out: str) -> None:
         if fn.startswith("size_") and fn.endswith(".npz"):
             shutil.copy(os.path.join(out, fn), os.path.join(HERE, fn))
             print("copied", fn)
-    with open(os.path.join(HERE, "size_pins.json"), "w") as f:
+    with open(dst, "w") as f:
         json.dump(summary, f, indent=1)
     print("wrote size_pins.json with", sorted(summary))
 
