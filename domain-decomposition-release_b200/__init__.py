@@ -74,8 +74,7 @@ class Options(C.Structure):
                 ("use_graphs", C.c_int), ("graph_steps", C.c_int), ("store_budget", C.c_size_t),
                 ("kernel_variant", C.c_int), ("zchunk", C.c_int), ("tile_gx", C.c_int), ("tile_gy", C.c_int),
                 ("min_blocks", C.c_int), ("pml_min_blocks", C.c_int), ("planes_per_thread", C.c_int),
-                ("pml_planes_per_thread", C.c_int), ("run_chunks", C.c_int), ("autotune", C.c_int),
-                ("fuse_velocity", C.c_int), ("fuse_min_blocks", C.c_int)]
+                ("pml_planes_per_thread", C.c_int), ("run_chunks", C.c_int), ("autotune", C.c_int)]
 
 
 class Job(C.Structure):

@@ -326,8 +326,6 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread < 0 || opt.planes_per_thread > 2 || opt.pml_planes_per_thread < 0 ||
         opt.pml_planes_per_thread > 2)
         return bad(JV_EINVAL, "planes_per_thread and pml_planes_per_thread must be 0, 1 or 2");
-    if (opt.fuse_min_blocks != 0 && (opt.fuse_min_blocks < 2 || opt.fuse_min_blocks > 4))
-        return bad(JV_EINVAL, "fuse_min_blocks must be 0, 2, 3 or 4");
     if (opt.kernel_variant < -1 || opt.kernel_variant > 4)
         return bad(JV_EINVAL, "kernel_variant must be 0..4, or -1 (measured choice)");
     if (opt.tile_gx < 0 || opt.tile_gy < 0 || opt.tile_gx * std::max(opt.tile_gy, 1) > 256)
@@ -356,8 +354,6 @@ Status Engine::create(const jv_grid &grid, const float *vp, const float *vs, con
     if (opt.planes_per_thread) E->kc_.zp = opt.planes_per_thread;
     if (opt.pml_planes_per_thread) E->kc_.pml_zp = opt.pml_planes_per_thread;
     if (opt.run_chunks > 0) E->kc_.fzq = opt.run_chunks;
-    E->kc_.both = opt.fuse_velocity ? 1 : 0;
-    if (opt.fuse_min_blocks) E->kc_.both_minb = opt.fuse_min_blocks;
     const char *cf = std::getenv("JV_CHECK_FINITE");
     E->check_finite_ = cf && cf[0] == '1';
     Status s = E->alloc_all(vp, vs, rho);
@@ -879,20 +875,11 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // (with its P-wave velocities, the full-gridext form measured no
         // faster on cfg2 and slower on x-tiled grids)
         JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
-        if (both_vel()) {
-            // the stress boundary layers of step it-1 first: the backward
-            // velocity update reads them
-            JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
-            // UPDATE 1's receiver velocities of gridphy and UPDATE 2's
-            // backward velocities with the imaging condition, one pass
-            JV_L("vel_both_image", k_vel_both(g_, F_, R_, rho_, -dt, dt, rw, shot_img_, kc_, s));
-        } else {
-            JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
-            JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
-            // UPDATE 2: backward velocity with the imaging condition fused,
-            // reverse stress, velocity boundary layers of step it-1
-            JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
-        }
+        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
+        // UPDATE 2: backward velocity with the imaging condition fused,
+        // reverse stress, velocity boundary layers of step it-1
+        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
         if (fullR_.ok) {
             JV_L("stress_fz_rev", k_stress_full(kRev, g_, R_, dt, wavelet_, st_, off, fullR_, s));
         } else {

@@ -134,8 +134,6 @@ class Engine {
         o->run_chunks = use_full_ ? fullF_.geo.Q : 0;
         o->tile_gx = kc_.gx;
         o->tile_gy = kc_.gy;
-        o->fuse_velocity = kc_.both;
-        o->fuse_min_blocks = kc_.both_minb;
     }
 
   private:
@@ -176,8 +174,6 @@ class Engine {
     }
 
   private:
-    // the reverse loop's gridphy velocity updates run as one kernel (float4 variants)
-    bool both_vel() const { return kc_.both && kc_.variant >= 2; }
     bool use_full_ = false;                        // the stress update of absorbing steps runs in stress_fz
     bool vel_full_ = false;                        // the forward passes' velocity update runs in vel_fz
     int *zm_err_ = nullptr;       // device flag of variant 3's bounded waits

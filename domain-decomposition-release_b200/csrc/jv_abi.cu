@@ -188,8 +188,6 @@ void jv_options_default(jv_options *o) {
     o->kernel_variant = 4;
     o->zchunk = 0;
     o->autotune = 1;
-    o->fuse_velocity = 1;
-    o->fuse_min_blocks = 0;
 }
 
 jv_status jv_create(const jv_grid *grid, const float *vp, const float *vs, const float *rho, float dt, float fm,

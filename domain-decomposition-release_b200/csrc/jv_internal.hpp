@@ -211,8 +211,6 @@ struct KCfg {
     int zp = 1;          // variant 2: z planes per thread (1 or 2)
     int pml_zp = 1;      // CPML kernels: the same
     int fzq = 0;         // variant 4: run chunks per tile (0: the cost model's choice)
-    int both = 1;        // variants 2-4: the reverse loop's two velocity updates of gridphy in one kernel
-    int both_minb = 3;   // that kernel's register budget: blocks per SM (2, 3 or 4)
 };
 
 // kernels.cu ------------------------------------------------------------
@@ -222,11 +220,7 @@ int k_zero_range(float *p, size_t n, void *stream);
 
 int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w,
               const WaveDev *rev, const ImageDev *img, const KCfg &kc, void *stream);
-// the receiver wavefield's velocity update of gridphy (rev, step dt_rev) and
-// the source wavefield's backward one (src, dt_src) with the imaging
-// condition, in one pass (variants 2-4)
-int k_vel_both(const GridDev &g, const WaveDev &src, const WaveDev &rev, const float *rho, float dt_src, float dt_rev,
-               int rec_w, const ImageDev &img, const KCfg &kc, void *stream);
+
 // it_off: the kernels of a step read the time step as st->it + it_off (a
 // captured chunk of steps advances st->it once, at its end)
 int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam, const float *mu, float dt,

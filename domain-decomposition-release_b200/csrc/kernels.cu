@@ -683,31 +683,6 @@ __global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, co
     }
 }
 
-// The reverse loop's two velocity updates of gridphy in one pass: per
-// group the receiver wavefield's update (rev, time forward, P-wave
-// velocities included), then the source wavefield's backward update with
-// the rtm_backward rim orders (src), then the imaging condition from both
-// sets of updated velocities, still in registers.  The
-// arithmetic of each update is that of vel_group4<kRev> and
-// vel_group4<kBwd, true>, so the results are the same, bit for bit; the
-// receiver velocities are not read back and rho comes from DRAM once (196
-// instead of 224 bytes a cell).
-// The two updates touch different arrays and neither reads what the other
-// writes, so their order within a step is free.
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) vel_phy_v4_both(GridDev g, WaveDev src, WaveDev rev,
-                                                            const float *__restrict__ rho, float dt_src, float dt_rev,
-                                                            int rec_w, ImageDev img) {
-    const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
-    const int pj = blockIdx.y * blockDim.y + threadIdx.y;
-    const int pk = blockIdx.z;
-    if (pi0 >= g.px || pj >= g.py || pk >= g.pz) return;
-    float rv[3][4], rp[3][4], v[3][4], p[3][4];
-    vel_update4<kRev>(g, rev, rho, dt_rev, rec_w, pi0, pj, pk, rv, rp);
-    vel_update4<kBwd>(g, src, rho, dt_src, rec_w, pi0, pj, pk, v, p);
-    image4(g, img, pi0, pj, pk, v, p, rv, rp);
-}
-
 // One 4-cell group of the stress update (source fused).
 template <int MODE>
 __device__ __forceinline__ void stress_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ lam,
@@ -2733,19 +2708,6 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
         break;
     default: return (int)cudaErrorInvalidValue;
     }
-    return cerr();
-}
-
-int k_vel_both(const GridDev &g, const WaveDev &src, const WaveDev &rev, const float *rho, float dt_src, float dt_rev,
-               int rec_w, const ImageDev &img, const KCfg &kc, void *stream) {
-    cudaStream_t s = (cudaStream_t)stream;
-    KCfg k1 = kc;
-    k1.zp = 1;
-    dim3 b, gr;
-    v4_shape(g, k1, &b, &gr);
-    if (kc.both_minb == 4) vel_phy_v4_both<4><<<gr, b, 0, s>>>(g, src, rev, rho, dt_src, dt_rev, rec_w, img);
-    else if (kc.both_minb == 2) vel_phy_v4_both<2><<<gr, b, 0, s>>>(g, src, rev, rho, dt_src, dt_rev, rec_w, img);
-    else vel_phy_v4_both<3><<<gr, b, 0, s>>>(g, src, rev, rho, dt_src, dt_rev, rec_w, img);
     return cerr();
 }
 

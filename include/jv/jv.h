@@ -106,11 +106,6 @@ typedef struct jv_options {
                            grid shape and device for the process (skipped when run_chunks,
                            tile_gx or tile_gy fix them, or kernel_variant is -1, which makes the
                            wider choice); 0: the cost model's chunking and the default shape */
-    int fuse_velocity;  /* variants 2-4: the reverse loop's receiver and backward velocity updates of
-                           gridphy as one kernel, the imaging condition reading the receiver
-                           velocities from registers (1, default) or as two kernels (0); the
-                           results are the same, bit for bit */
-    int fuse_min_blocks;/* that kernel's register budget: 2, 3 or 4 blocks per SM (0: default) */
 } jv_options;
 
 /* Fills `o` with the defaults (device 0, rec_width 1, FP32, auto store,

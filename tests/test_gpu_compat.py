@@ -171,7 +171,8 @@ def test_reverse_ops_match_rtm_shot(synth, w):
     """The time-reverse loop driven one kernel at a time (jv_rtm_forward_pass,
     jv_rtm_reverse_begin, jv_rtm_reverse_op in the reference's order,
     jv_rtm_reverse_end) stacks the same images as jv_rtm_shot, bit for bit,
-    with the same reconstruction check."""
+    with the same reconstruction check (its FP64 sums are atomic, so
+    equal to rounding)."""
     import torch
 
     s = synth.small_case(n=(22, 18, 16), pml=6, nt=90, seed=21, rec_width=w)
@@ -201,4 +202,5 @@ def test_reverse_ops_match_rtm_shot(synth, w):
         assert L.jv_rtm_reverse_op(ctx._h, 99, 0) == jv.JV_ESTATE  # closed again
     for k in want:
         assert np.array_equal(got[k], want[k]), k
-    assert e_got == e_want
+    for a, b in zip(e_got, e_want):
+        assert abs(a - b) <= 1e-12 * abs(b), (e_got, e_want)
