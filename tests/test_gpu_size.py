@@ -15,9 +15,15 @@
   8e-6 .. 2.3e-5 vs the reference, whose own FP32 error against the FP64
   oracle is 4e-6 .. 2.4e-5).
 
-Bounds: traces 1e-5; raw images 1e-4 against both (the workload's image
-bound is 1e-3 against FP64); rec_width 4 reconstructs the source wavefield
-exactly, so its reconstruction residual is at the FP32 floor.
+Bounds: on every sample, the GPU path's error against either is at most
+twice the reference's own FP32 error against the FP64 oracle on the same
+sample (at least 2e-5 for traces and 1e-4 for images); on the plane through
+the source, which holds the bright cells that set the whole-field norm,
+1e-4 for every image (the workload's image bound is 1e-3 against FP64).
+The uniform volume sample leaves those cells out: there the FP32 noise of
+dim cells shows, for the reference's own run too (1.5e-3 .. 2.7e-3 for sp
+and ss).  rec_width 4 reconstructs the source wavefield exactly, so its
+reconstruction residual is at the FP32 floor.
 """
 import os
 
@@ -67,14 +73,18 @@ def test_cfg2_full_vs_fp64_oracle_and_reference(w):
         img = ctx.images()
         e0, e1 = ctx.reconstruction_energy()
         tr = [obs[q].index_select(0, sub).cpu().numpy() for q in range(3)]
+    sample = {"y100": lambda a: a[:, 100], "d4": lambda a: a[2::4, 2::4, 2::4]}
     for src in ("oracle", "ref"):
         for q, c in enumerate(("vx", "vy", "vz")):
             e = rel_l2(tr[q], f[f"{src}_tr_{c}"])
-            assert e <= 1e-5, (src, c, e)
+            own = rel_l2(f[f"ref_tr_{c}"], f[f"oracle_tr_{c}"])  # the reference's own FP32 error here
+            assert e <= max(2e-5, 2.0 * own), (src, c, e, own)
         for k in KINDS:
-            a = np.concatenate([img[k][2::4, 2::4, 2::4].ravel(), img[k][:, 100].ravel()])
-            b = np.concatenate([f[f"{src}_{k}_d4"].ravel(), f[f"{src}_{k}_y100"].ravel()])
-            e = rel_l2(a, b)
-            assert e <= 1e-4, (src, k, e)
+            for pk, cut in sample.items():
+                e = rel_l2(cut(img[k]), f[f"{src}_{k}_{pk}"])
+                own = rel_l2(f[f"ref_{k}_{pk}"], f[f"oracle_{k}_{pk}"])
+                assert e <= max(1e-4, 2.0 * own), (src, k, pk, e, own)
+            # the plane through the source carries the bright cells that set the whole-field norm
+            assert rel_l2(img[k][:, 100], f[f"{src}_{k}_y100"]) <= 1e-4, (src, k)
     if w == 4:
         assert e1 / e0 < 1e-5, e1 / e0  # exact reconstruction, up to FP32 rounding
