@@ -320,7 +320,12 @@ class Field : public Frame {
     // host_single_field::save of the host storage
     void save(const string &_file_path, SaveFormat _format) const { save_values(_file_path, _format, host_); }
     // Field<.., device>::cu_save: the device storage, through a host copy
+    // (a field without device storage saves its host values)
     void cu_save(const string &_file_path, SaveFormat _format) const {
+        if (!kDevice) {
+            save(_file_path, _format);
+            return;
+        }
         std::vector<elem_type> h(n_elem);
         if (n_elem)
             jarvis_handle_cuda_error(cudaMemcpy(h.data(), dev_, bytes(), cudaMemcpyDeviceToHost));
@@ -489,6 +494,9 @@ struct jv_compat_job {
     int it = 0;                      // time index of the current reverse step
     bool begin_pending = false, reverse_open = false;
 
+    jv_compat_job() = default;
+    jv_compat_job(const jv_compat_job &) = delete;  // it owns the context
+    jv_compat_job &operator=(const jv_compat_job &) = delete;
     ~jv_compat_job() {
         if (ctx) jv_close(ctx);
     }
