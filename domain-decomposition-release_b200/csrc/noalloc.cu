@@ -81,11 +81,16 @@ jv_status device_setup(int dev, unsigned char **out) {
     if (dev < 0 || dev >= kMaxDevices) return fail(JV_EINVAL, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceSetup &d = g_setup[dev];
-    // binds (and if need be creates) the device's primary context on this
-    // thread, so that the context recorded below is the one the set-up uses
-    cudaError_t e0 = cudaSetDevice(dev);
-    if (e0 != cudaSuccess) return fail(JV_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e0));
     void *ctx = current_context();
+    if (!ctx) {
+        // no context bound to this thread yet: bind (and if need be create)
+        // the device's primary context, the one the set-up below uses, so
+        // that the context recorded is that one (a context the caller has
+        // made current is left as it is)
+        cudaError_t e0 = cudaSetDevice(dev);
+        if (e0 != cudaSuccess) return fail(JV_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e0));
+        ctx = current_context();
+    }
     if (!d.addr || ctx != d.ctx) {
         d.addr = nullptr;
         void *p = nullptr;
