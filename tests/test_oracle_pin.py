@@ -102,3 +102,24 @@ def test_oracle_matches_reference_at_size(w):
         assert max(d["traces"][pair].values()) <= 1e-5, pair
         assert max(d["raw_images"][pair].values()) <= 1e-4, pair
         assert d["laplacian_pp"][pair] <= 1e-4, pair
+
+
+def test_boundary_store_precision_at_size():
+    """cfg3 at half resolution (338 x 338 x 105 + 10 CPML, 1500 steps), the
+    whole fields as make_size_pins.py measured them on a B200: with the FP32,
+    FP16 and BF16 boundary stores the raw images stay within the workload's
+    1e-3 bound against the FP64 oracle, and within 1e-4 of the FP32 store;
+    the traces do not depend on the store."""
+    import json
+    import os
+
+    with open(os.path.join(os.path.dirname(mg.__file__), "size_pins.json")) as fh:
+        d = json.load(fh)["cfg3_half"]
+    assert d["grid_phy"] == [338, 338, 105] and d["nt"] == 1500
+    assert max(d["raw_images"]["gpu_vs_oracle"].values()) <= 1e-4
+    assert max(d["raw_images"]["oracle_vs_reference"].values()) <= 1e-4
+    for tag in ("fp16_store", "bf16_store"):
+        p = d["boundary_store_precision"][tag]
+        assert max(p["raw_images_vs_oracle"].values()) <= 1e-3, tag
+        assert max(p["raw_images_vs_fp32_store"].values()) <= 1e-4, tag
+        assert max(p["traces_vs_fp32_store"].values()) == 0.0, tag
