@@ -149,6 +149,28 @@ BYTES_PER_CELL = {
 }
 
 
+# (arrays read, arrays written) per interior cell of each kernel: the
+# footprint whose pointwise pass (jv_stream_probe) bounds what the kernel
+# can move; the full-gridext kernels add CPML memory variables at the rim
+FOOTPRINT = {
+    "vel_phy_bwd_image": (25, 11), "vel_phy_rev": (14, 6), "vel_phy_rtmfwd": (10, 3), "vel_phy_fwd": (10, 3),
+    "vel_fz_rtmfwd": (10, 3), "vel_fz_fwd": (10, 3),
+    "stress_phy_bwd": (12, 7), "stress_phy_rev": (12, 7), "stress_phy_rtmfwd": (12, 7),
+    "stress_fz_rev": (12, 7), "stress_fz_rtmfwd": (12, 7),
+}
+
+
+def attainable(jv, names, n, reps=5):
+    """GB/s of the pointwise pass of each named kernel's footprint over n
+    floats per array (arrays larger than L2): {footprint: GB/s}."""
+    out = {}
+    for k in names:
+        fp = FOOTPRINT.get(k)
+        if fp is not None and fp not in out:
+            out[fp] = jv.stream_probe(fp[0], fp[1], n - n % 4, reps=reps)
+    return out
+
+
 def pml_bytes(s, name):
     """Algorithmic bytes of one CPML launch: per slab cell the fields, plus
     3 memory variables read+written per axis on which the cell absorbs."""
@@ -421,7 +443,10 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed, repea
 
     sizes = [int(n) for n in rng.choice([80, 96, 120, 160, 200], n_models)]
     models = [synth.scaled_cfg2(n, nt_mixed, pml=16, seed=200 + k) for k, n in enumerate(sizes)]
-    cells = sum(nt_mixed * (3 * m.n_ext) for m in models)  # own modelling + source and receiver propagations
+    # own modelling (gridext), the RTM forward pass (gridext), the reverse
+    # loop's receiver (gridext) and source (gridphy) propagations: the
+    # count of the single-shot and serving figures
+    cells = sum(nt_mixed * (3 * m.n_ext + m.n_phy) for m in models)
 
     plan = [(m, jv.JOB_RTM) for m in models]
     outs = _outputs(jv, plan)
@@ -790,17 +815,21 @@ def main():
         name, (ms, n) = max(prof.items(), key=lambda kv: kv[1][0])
         b = kernel_bytes(s, name)
         peak, peak_kind = load_peaks()
+        att = attainable(jv, prof.keys(), info.n_ext)
         if rank == 0:
             print(f"per-kernel device time, one instrumented RTM shot ({s.name}, CUDA events on the library stream):",
                   file=sys.stderr)
             print(f"  {'kernel':22s} {'launches':>8s} {'us/launch':>10s} {'share':>7s} {'alg. bytes':>12s} "
-                  f"{'GB/s':>8s} {'of peak':>8s}", file=sys.stderr)
+                  f"{'GB/s':>8s} {'of peak':>8s} {'of attainable':>14s}", file=sys.stderr)
             for k, (kms, kn) in sorted(prof.items(), key=lambda kv: -kv[1][0]):
                 kb = kernel_bytes(s, k)
                 us = 1000.0 * kms / max(kn, 1)
                 gbs = kb / (us * 1e-6) / 1e9 if kb else float("nan")
+                a = att.get(FOOTPRINT.get(k))
                 print(f"  {k:22s} {kn:8d} {us:10.1f} {kms / tot:7.1%} {kb or 0:12.4g} {gbs:8.0f} "
-                      f"{gbs / peak:8.1%}", file=sys.stderr)
+                      f"{gbs / peak:8.1%} {(gbs / a) if a else float('nan'):14.1%}", file=sys.stderr)
+            print("  attainable: " + ", ".join(f"{r} read + {w} written {g:.0f} GB/s" for (r, w), g in att.items()),
+                  file=sys.stderr)
         if b is not None and n > 0:
             avg_s = ms / n / 1000.0
             ach = b / avg_s / 1e9
@@ -810,6 +839,14 @@ def main():
                     "peak_nominal": NOMINAL_HBM_GBS, "frac_nominal": round(ach / NOMINAL_HBM_GBS, 4),
                     "traffic": tr, "algorithmic_bytes_per_launch": b, "avg_launch_us": round(avg_s * 1e6, 2),
                     "share": round(ms / tot, 4) if tot > 0 else None}
+            fp = FOOTPRINT.get(name)
+            if fp in att:
+                roof["attainable"] = {
+                    "footprint": {"read": fp[0], "written": fp[1]}, "gbs": round(att[fp], 1),
+                    "frac": round(ach / att[fp], 4),
+                    "note": "jv_stream_probe: a pointwise float4 pass over the kernel's arrays (each "
+                            f"{info.n_ext} floats, larger than L2), median of 5 launches; the bound of a pass "
+                            "with that many arrays, which a two-array copy does not give"}
 
     accuracy = None
     if rank == 0 and not args.no_accuracy:

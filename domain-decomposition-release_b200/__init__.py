@@ -48,7 +48,7 @@ EXPORTS = (
     "jv_submit", "jv_poll", "jv_wait", "jv_cancel",
     "jv_footprint", "jv_server_create", "jv_server_submit", "jv_server_poll", "jv_server_wait", "jv_server_cancel",
     "jv_server_get_stats", "jv_server_close", "jv_frame_make", "jv_fld_write", "jv_fld_read", "jv_raw_read",
-    "jv_rtm_forward_pass", "jv_rtm_reverse_begin", "jv_rtm_reverse_op", "jv_rtm_reverse_end",
+    "jv_rtm_forward_pass", "jv_rtm_reverse_begin", "jv_rtm_reverse_op", "jv_rtm_reverse_end", "jv_stream_probe",
 )
 (OP_INJECT_RECEIVERS, OP_BACKWARD_STRESS, OP_REVERSE_VEL_PML, OP_REVERSE_VEL, OP_INJECT_BOUNDARY_STRESS,
  OP_BACKWARD_VEL_IMAGE, OP_REVERSE_STRESS_PML, OP_REVERSE_STRESS, OP_INJECT_BOUNDARY_VEL) = range(9)
@@ -230,6 +230,7 @@ def lib() -> C.CDLL:
     L.jv_rtm_reverse_op.argtypes = [ctxp, C.c_int, C.c_int]
     L.jv_rtm_reverse_end.argtypes = [ctxp]
     L.jv_last_timing.argtypes = [ctxp, dp]
+    L.jv_stream_probe.argtypes = [C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_int, dp]
     L.jv_sync.argtypes = [ctxp]
     L.jv_close.argtypes = [ctxp]
     L.jv_last_error.argtypes = []
@@ -502,6 +503,15 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def stream_probe(n_read: int, n_write: int, n: int, reps: int = 5, device: int = 0) -> float:
+    """GB/s of a pointwise pass over n_read + n_write arrays of n floats
+    (jv_stream_probe): the attainable bandwidth of a kernel with that
+    footprint."""
+    g = C.c_double()
+    _check(lib().jv_stream_probe(device, n_read, n_write, n, reps, C.byref(g)))
+    return g.value
 
 
 def footprint(nx, ny, nz, pml, nt, rec_width=1, kind=JOB_RTM, n_recv=0) -> int:

@@ -478,6 +478,17 @@ jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, const float
                              float fm, int nt, const float *src_xyz, int n_recv, const float *recv_xyz, float *d_vx,
                              float *d_vy, float *d_vz, int *n_kept, void *stream);
 
+/* Attainable HBM bandwidth of a pointwise pass that reads n_read and writes
+ * n_write arrays of n floats each (n a multiple of 4; one float4 of every
+ * array per thread, every load issued before the stores), in GB/s of bytes
+ * moved, from the median device time of `reps` launches after one warm-up.
+ * The supported (n_read, n_write) pairs are the footprints of this
+ * library's kernels and a copy: (1,1) (2,1) (10,3) (12,7) (14,6) (25,11).
+ * Allocates its arrays on `device` and frees them before it returns.  A
+ * diagnostic for the roofline of many-array kernels; no counterpart in the
+ * reference. */
+jv_status jv_stream_probe(int device, int n_read, int n_write, size_t n, int reps, double *gbs);
+
 /* Waits for all work of the context. */
 jv_status jv_sync(jv_ctx *c);
 

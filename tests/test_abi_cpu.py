@@ -139,3 +139,13 @@ def test_traces_format(tmp_path, project):
 
 def test_size_info_matches_reference_naming(project):
     assert project.size_info(30, 26, 22) == "_30_26_22_0.000000_0.000000_0.000000"
+
+
+def test_stream_probe_rejects_bad_arguments_without_device():
+    jv = pkg()
+    L = jv.lib()
+    g = C.c_double()
+    for nr, nw, n, reps in ((3, 3, 1024, 1), (1, 1, 1022, 1), (1, 1, 0, 1), (25, 11, 1024, 0)):
+        assert L.jv_stream_probe(0, nr, nw, n, reps, C.byref(g)) == jv.JV_EINVAL
+    assert L.jv_stream_probe(0, 1, 1, 1024, 1, None) == jv.JV_EINVAL
+    assert b"(25,11)" in L.jv_last_error() or b"bad argument" in L.jv_last_error()
