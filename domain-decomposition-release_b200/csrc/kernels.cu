@@ -1303,6 +1303,38 @@ __device__ __forceinline__ void vel_pml_group(const GridDev &g, const CpmlDev &P
                                               const PmlPos &q) {
     const int sy = (int)g.sy, sz = (int)g.sz;
     const int i0 = (int)g.xoff + q.xs + sy * q.y + sz * q.z;
+    {
+        // the group's DRAM-new lines (slab blocks run in plane order), as in
+        // vel_prefetch4: pointwise arrays, fields read in their own plane, the
+        // leading plane of each z difference, and the memory variables of the
+        // axes on which the group absorbs
+        pf_l2(rho, i0);
+        pf_l2(vpm, i0);
+        pf_l2(w.f[VX], i0);
+        pf_l2(w.f[VY], i0);
+        pf_l2(w.f[VZ], i0);
+        pf_l2(w.f[SXX], i0);
+        pf_l2(w.f[SXY], i0);
+        pf_l2(w.f[SYY], i0);
+        pf_l2(w.f[SXZ], i0 + sz);
+        pf_l2(w.f[SYZ], i0 + sz);
+        pf_l2(w.f[SZZ], i0 + 2 * sz);
+        const float *psi = P.psi + q.psi;
+        const long long n = q.stride;
+        bool anyx = false;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+            if (q.mask & (1u << c)) anyx |= P.ax[0][q.xs + c].x > 0.f;
+        if (anyx)
+#pragma unroll
+            for (int a = 0; a < 3; a++) pf_l2(psi + a * n, 0);
+        if (P.ax[1][q.y].x > 0.f)
+#pragma unroll
+            for (int a = 3; a < 6; a++) pf_l2(psi + a * n, 0);
+        if (P.ax[2][q.z].x > 0.f)
+#pragma unroll
+            for (int a = 6; a < 9; a++) pf_l2(psi + a * n, 0);
+    }
     const float c0 = c_dc2[0], c1 = c_dc2[1];
     const float rdx = 1.0f / g.dx, rdy = 1.0f / g.dy, rdz = 1.0f / g.dz;
     float win[12], sxx_x[4], syx_x[4], szx_x[4], sxy_y[4], syy_y[4], szy_y[4], sxz_z[4], syz_z[4], szz_z[4];
