@@ -300,8 +300,9 @@ def serve_leg(jv, synth, n_req, repeats=3):
     _served(jv, plan[:2], outs[:2], 2, 300.0)  # warm-up (module load, allocator pools), not counted
     runs, med = _repeat(jv, plan, outs, 600.0, repeats)
     (t1, st1), (t4, st4) = med[1], med[4]
-    cells = sum((sv.nx + 2 * sv.pml) * (sv.ny + 2 * sv.pml) * (sv.nz + 2 * sv.pml) * sv.nt * (3 if k else 1)
-                for sv, k in plan)
+    # forward: gridext; RTM: its own modelling, the forward pass and the
+    # receiver propagation on gridext, the source reconstruction on gridphy
+    cells = sum(sv.nt * (3 * sv.n_ext + sv.n_phy if k else sv.n_ext) for sv, k in plan)
 
     # a Poisson stream: requests arrive (seeded exponential gaps) while
     # others run, at half and at 0.9 of the 4-slot capacity just measured
@@ -335,6 +336,7 @@ def serve_leg(jv, synth, n_req, repeats=3):
             "runs": {"slots1": [round(n_req / t * 3600.0, 1) for t, _ in runs[1]],
                      "slots4": [round(n_req / t * 3600.0, 1) for t, _ in runs[4]]},
             "contexts_reused": {"slots1": st1["reused"], "slots4": st4["reused"]},
+            "device_busy_slots1": round(st1["device_ms"] / (1000.0 * t1), 4),
             "p50_ms": {"slots4": round(st4["p50_ms"], 1), "slots1": round(st1["p50_ms"], 1)},
             "p99_ms": {"slots4": round(st4["p99_ms"], 1), "slots1": round(st1["p99_ms"], 1)},
             "gcell_updates_per_s": {"slots4": round(cells / t4 / 1e9, 2), "slots1": round(cells / t1 / 1e9, 2)},
@@ -464,6 +466,10 @@ def batched_leg(jv, synth, torch, device, n_shots, nt, n_models, nt_mixed, repea
                  "slots4": [round(n_models / t * 3600.0, 1) for t, _ in runs[4]]},
         "contexts_reused": {"slots1": st1["reused"], "slots4": st4["reused"]},
         "gcell_updates_per_s": {"slots1": round(cells / t1 / 1e9, 2), "slots4": round(cells / t4 / 1e9, 2)},
+        # the requests' propagation kernels' device time against the wall
+        # time of the one-slot run: what a launch over several models could
+        # still fill is the rest
+        "device_busy_slots1": round(st1["device_ms"] / (1000.0 * t1), 4),
         "p50_ms": {"slots1": round(st1["p50_ms"], 1), "slots4": round(st4["p50_ms"], 1)},
         "p99_ms": {"slots1": round(st1["p99_ms"], 1), "slots4": round(st4["p99_ms"], 1)},
         "note": f"median of {repeats} runs per slot count (alternating, each on a new server whose context pool "

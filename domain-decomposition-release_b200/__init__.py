@@ -96,7 +96,7 @@ class ServerStats(C.Structure):
                 ("cancelled", C.c_longlong), ("running", C.c_longlong), ("queued", C.c_longlong),
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("bytes_in_use", C.c_size_t), ("budget", C.c_size_t), ("reused", C.c_longlong),
-                ("pooled", C.c_longlong)]
+                ("pooled", C.c_longlong), ("device_ms", C.c_double)]
 
 
 class ArgFileC(C.Structure):

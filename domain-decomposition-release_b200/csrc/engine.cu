@@ -404,7 +404,7 @@ Status Engine::autotune(bool neutral) {
         }
         if (c.variant == 4 && fullF_.ok && c.q > 0 && c.q != fullF_.geo.Q) {
             kc_.fzq = c.q;
-            const int e = k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_);
+            const int e = k_make_full_maps(g_, F_, lam_, mu_, vp_, bdt_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_);
             if (e != 0 || !fullF_.ok) st = bad(JV_ECUDA, "variant-4 descriptors for the measured choice");
         }
         use_full_ = c.variant == 4 && fullF_.ok;
@@ -479,7 +479,7 @@ Status Engine::autotune(bool neutral) {
             JV_TRY(set_state(0, src, nullptr, nullptr));
             for (int i = 0; i < warm + steps; i++) {
                 if (i == warm) JV_CU(cudaEventRecord(ev0_, stream_));
-                JV_K(k_vel_phy(kRev, g_, F_, rho_, dt_, opt_.rec_width, nullptr, nullptr, kc_, stream_));
+                JV_K(k_vel_phy(kRev, g_, F_, bdt_, dt_, opt_.rec_width, nullptr, nullptr, kc_, stream_));
                 JV_K(k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt_, opt_.rec_width, wavelet_, st_, 0, kc_, stream_,
                                   &mapsF_));
             }
@@ -521,7 +521,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
     JV_TRY(alloc(&p, (4 * field_elems_ + kGuard) * sizeof(float)));
     JV_CU(cudaMemsetAsync(p, 0, (4 * field_elems_ + kGuard) * sizeof(float), stream_));
     float *mb = (float *)p + kGuard;
-    vp_ = mb; rho_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
+    vp_ = mb; bdt_ = mb + field_elems_; lam_ = mb + 2 * field_elems_; mu_ = mb + 3 * field_elems_;
     const size_t nphy = (size_t)g_.px * g_.py * g_.pz;
     JV_TRY(upload_model(vp, vs, rho));
 
@@ -555,7 +555,7 @@ Status Engine::alloc_all(const float *vp, const float *vs, const float *rho) {
         fz_psi_total_ = 2 * fz_psi_floats(g_);  // velocity and stress sets
         JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
         fzpsiF_ = (float *)p;
-        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, rho_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_));
+        JV_K(k_make_full_maps(g_, F_, lam_, mu_, vp_, bdt_, axis_d_, fzpsiF_, zm_err_, kc_.fzq, &fullF_));
         // the fused velocity update runs on one-tile grids, where it measured
         // faster than the split kernels; x-tiled grids keep the split ones
         use_full_ = fullF_.ok;
@@ -612,7 +612,7 @@ Status Engine::upload_model(const float *vp, const float *vs, const float *rho) 
     cudaError_t e1 = cudaMemcpyAsync(tmp, vp, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
     cudaError_t e2 = cudaMemcpyAsync(tmp + nphy, vs, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
     cudaError_t e3 = cudaMemcpyAsync(tmp + 2 * nphy, rho, nphy * sizeof(float), cudaMemcpyHostToDevice, stream_);
-    int ek = k_model_prep(g_, tmp, tmp + nphy, tmp + 2 * nphy, vp_, rho_, lam_, mu_, stream_);
+    int ek = k_model_prep(g_, tmp, tmp + nphy, tmp + 2 * nphy, dt_, vp_, bdt_, lam_, mu_, stream_);
     cudaFreeAsync(tmp, stream_);
     cudaError_t e4 = cudaStreamSynchronize(stream_);
     JV_CU(e1); JV_CU(e2); JV_CU(e3); JV_K(ek); JV_CU(e4);
@@ -834,8 +834,8 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         if (vel_full_) {
             JV_L("vel_fz_fwd", k_vel_full(g_, F_, dt, fullF_, s));
         } else {
-            JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
-            JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+            JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, bdt_, vp_, kc_, s));
+            JV_L("vel_phy_fwd", k_vel_phy(kFwd, g_, F_, bdt_, dt, rw, nullptr, nullptr, kc_, s));
         }
         if (use_full_) {
             JV_L("stress_fz_fwd", k_stress_full(kFwd, g_, F_, dt, wavelet_, st_, off, fullF_, s));
@@ -851,8 +851,8 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         if (vel_full_) {
             JV_L("vel_fz_rtmfwd", k_vel_full(g_, F_, dt, fullF_, s));
         } else {
-            JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, rho_, vp_, kc_, s));
-            JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+            JV_L("vel_pml", k_vel_pml(g_, cpF_, F_, bdt_, vp_, kc_, s));
+            JV_L("vel_phy_rtmfwd", k_vel_phy(kRtmFwd, g_, F_, bdt_, dt, rw, nullptr, nullptr, kc_, s));
         }
         if (use_full_) {
             // the boundary boxes lie in the absorbing layers: pack them after their update
@@ -874,12 +874,12 @@ Status Engine::launch_step(int kind, int off, bool advance) {
         // the receiver side's velocity update: absorbing layers, then gridphy
         // (with its P-wave velocities, the full-gridext form measured no
         // faster on cfg2 and slower on x-tiled grids)
-        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s));
-        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s));
+        JV_L("vel_pml", k_vel_pml(g_, cpR_, R_, bdt_, vp_, kc_, s));
+        JV_L("vel_phy_rev", k_vel_phy(kRev, g_, R_, bdt_, dt, rw, nullptr, nullptr, kc_, s));
         JV_L("vowr_unpack", k_vowr(g_, F_, vowr_, st_, off - 1, 0, 2, s));
         // UPDATE 2: backward velocity with the imaging condition fused,
         // reverse stress, velocity boundary layers of step it-1
-        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s));
+        JV_L("vel_phy_bwd_image", k_vel_phy(kBwd, g_, F_, bdt_, -dt, rw, &R_, &shot_img_, kc_, s));
         if (fullR_.ok) {
             JV_L("stress_fz_rev", k_stress_full(kRev, g_, R_, dt, wavelet_, st_, off, fullR_, s));
         } else {
@@ -988,7 +988,7 @@ Status Engine::rtm_prepare() {
         if (kc_.variant == 4) {
             JV_TRY(alloc(&p, (size_t)fz_psi_total_ * sizeof(float)));
             fzpsiR_ = (float *)p;
-            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, rho_, axis_d_, fzpsiR_, zm_err_, kc_.fzq, &fullR_));
+            JV_K(k_make_full_maps(g_, R_, lam_, mu_, vp_, bdt_, axis_d_, fzpsiR_, zm_err_, kc_.fzq, &fullR_));
         }
     }
     if (!shot_img_.ip) {
@@ -1106,10 +1106,10 @@ Status Engine::rtm_reverse_op(int op, int it) {
     case JV_OP_BACKWARD_STRESS:
         JV_K(k_stress_phy(kBwd, g_, F_, lam_, mu_, -dt, rw, wavelet_, st_, 0, kc_, s, &mapsF_));
         break;
-    case JV_OP_REVERSE_VEL_PML: JV_K(k_vel_pml(g_, cpR_, R_, rho_, vp_, kc_, s)); break;
-    case JV_OP_REVERSE_VEL: JV_K(k_vel_phy(kRev, g_, R_, rho_, dt, rw, nullptr, nullptr, kc_, s)); break;
+    case JV_OP_REVERSE_VEL_PML: JV_K(k_vel_pml(g_, cpR_, R_, bdt_, vp_, kc_, s)); break;
+    case JV_OP_REVERSE_VEL: JV_K(k_vel_phy(kRev, g_, R_, bdt_, dt, rw, nullptr, nullptr, kc_, s)); break;
     case JV_OP_INJECT_BOUNDARY_STRESS: JV_K(k_vowr(g_, F_, vowr_, st_, 0, 0, 2, s)); break;
-    case JV_OP_BACKWARD_VEL_IMAGE: JV_K(k_vel_phy(kBwd, g_, F_, rho_, -dt, rw, &R_, &shot_img_, kc_, s)); break;
+    case JV_OP_BACKWARD_VEL_IMAGE: JV_K(k_vel_phy(kBwd, g_, F_, bdt_, -dt, rw, &R_, &shot_img_, kc_, s)); break;
     case JV_OP_REVERSE_STRESS_PML:
         // folded into the full-gridext stress kernel where that one runs
         if (!fullR_.ok) JV_K(k_stress_pml(g_, cpR_, R_, lam_, mu_, vp_, 1, kc_, s));
@@ -1145,7 +1145,7 @@ Status Engine::rtm_reverse_end() {
     return Status{};
 }
 
-Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz) {
+Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz, cudaEvent_t obs_ready) {
     JV_CU(cudaSetDevice(dev_));
     long long src;
     JV_TRY(check_shot(shot, &src));
@@ -1153,6 +1153,7 @@ Status Engine::rtm_shot(int shot, const float *d_ox, const float *d_oy, const fl
     JV_TRY(rtm_prepare());
     JV_CU(cudaEventRecord(ev0_, stream_));
     JV_TRY(rtm_forward_pass(shot));
+    if (obs_ready) JV_CU(cudaStreamWaitEvent(stream_, obs_ready, 0));
     JV_TRY(rtm_reverse_begin(shot, d_ox, d_oy, d_oz));
     JV_TRY(run_loop(kStepRtmRev, nt_));
     JV_TRY(reverse_end_launch());
@@ -1220,11 +1221,6 @@ Status Engine::image_set(int kind, const double *src, bool src_on_device) {
     return Status{};
 }
 
-Status Engine::wait_event(cudaEvent_t e) {
-    JV_CU(cudaSetDevice(dev_));
-    JV_CU(cudaStreamWaitEvent(stream_, e, 0));
-    return Status{};
-}
 
 Status Engine::check_zm_err() {
     if (!zm_err_) return Status{};

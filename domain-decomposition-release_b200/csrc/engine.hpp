@@ -80,7 +80,11 @@ class Engine {
     // maps and captured graphs stay as they are
     Status set_model(const float *vp, const float *vs, const float *rho);
     Status forward(int shot, float *d_vx, float *d_vy, float *d_vz);
-    Status rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz);
+    // obs_ready: an event the observed traces' copy records; the reverse
+    // loop, the first user of the traces, waits for it, so the copy runs
+    // beside the forward pass
+    Status rtm_shot(int shot, const float *d_ox, const float *d_oy, const float *d_oz,
+                    cudaEvent_t obs_ready = nullptr);
     // the phases of rtm_shot, for drivers that run them one by one: the
     // forward pass with the boundary store, the opening of the time-reverse
     // loop, one of its kernels (jv_rtm_op) at a time index, and its end
@@ -107,8 +111,6 @@ class Engine {
     int nt() const { return nt_; }
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
-    // the next kernels of this context wait for `e` (recorded on another stream)
-    Status wait_event(cudaEvent_t e);
 
     // project bookkeeping (jv_open)
     std::string output_path;
@@ -182,7 +184,7 @@ class Engine {
     std::vector<void *> allocs_;
     size_t dev_bytes_ = 0;
 
-    float *vp_ = nullptr, *rho_ = nullptr, *lam_ = nullptr, *mu_ = nullptr;
+    float *vp_ = nullptr, *bdt_ = nullptr, *lam_ = nullptr, *mu_ = nullptr;  // bdt_: dt / rho
     WaveDev F_{}, R_{};
     CpmlDev cpF_{}, cpR_{};
     CpmlDev cpml_proto_{};     // slab table shared by both wavefields

@@ -146,18 +146,37 @@ static jv_status forward_host(jv_ctx *c, int shot, float *vx, float *vy, float *
     return JV_OK;
 }
 
+// the copy stream of host-pointer RTM calls and its two events, made once
+static jv_status ensure_copy_stream(jv_ctx *c) {
+    if (c->copy_stream) return JV_OK;
+    cudaSetDevice(c->eng->device());
+    cudaError_t e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaEventCreateWithFlags(&c->ev_copy[b], cudaEventDisableTiming);
+    if (e != cudaSuccess) return fail(JV_ECUDA, std::string("copy stream: ") + cudaGetErrorString(e));
+    return JV_OK;
+}
+
+// One shot from host traces: they are copied on the copy stream while the
+// forward pass runs (it does not read them); the reverse loop waits for the
+// copy.  The previous call has finished with the buffer, since every call
+// returns after its shot.
 static jv_status rtm_host(jv_ctx *c, int shot, const float *ox, const float *oy, const float *oz) {
     const size_t per = (size_t)c->eng->nrec() * c->eng->nt();
     if (per && (!ox || !oy || !oz)) return fail(JV_EINVAL, "observed traces must not be NULL");
     jv_status st = ensure_traces(c, 3 * per);
+    if (st == JV_OK) st = ensure_copy_stream(c);
     if (st != JV_OK) return st;
     const float *h[3] = {ox, oy, oz};
     for (int q = 0; q < 3 && per; q++) {
         cudaError_t e = cudaMemcpyAsync(c->d_tr[0] + q * per, h[q], per * sizeof(float), cudaMemcpyHostToDevice,
-                                        c->eng->stream());
+                                        c->copy_stream);
         if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
     }
-    return ret(c->eng->rtm_shot(shot, c->d_tr[0], c->d_tr[0] + per, c->d_tr[0] + 2 * per));
+    cudaError_t e = cudaEventRecord(c->ev_copy[0], c->copy_stream);
+    if (e != cudaSuccess) return fail(JV_ECUDA, cudaGetErrorString(e));
+    st = ret(c->eng->rtm_shot(shot, c->d_tr[0], c->d_tr[0] + per, c->d_tr[0] + 2 * per, c->ev_copy[0]));
+    if (st != JV_OK) cudaStreamSynchronize(c->copy_stream);  // the buffer is free when the call returns
+    return st;
 }
 
 namespace jv {
@@ -169,7 +188,10 @@ jv_status rtm_self_modelled(jv_ctx *c, int shot) {
     float *d = c->d_tr[0];
     st = ret(c->eng->forward(shot, d, d + per, d + 2 * per));
     if (st != JV_OK) return st;
-    return ret(c->eng->rtm_shot(shot, d, d + per, d + 2 * per));
+    const double fwd_ms = c->eng->last_ms();
+    st = ret(c->eng->rtm_shot(shot, d, d + per, d + 2 * per));
+    if (st == JV_OK) c->eng->set_last_ms(fwd_ms + c->eng->last_ms());  // both propagations
+    return st;
 }
 }  // namespace jv
 
@@ -444,11 +466,9 @@ jv_status jv_rtm_batch(jv_ctx *c, int n, const int *shots, const float *const *o
         jv_status st = ensure_traces(c, 3 * per, b);
         if (st != JV_OK) return st;
     }
-    cudaSetDevice(c->eng->device());
-    if (!c->copy_stream) {
-        cudaError_t e = cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking);
-        for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaEventCreateWithFlags(&c->ev_copy[b], cudaEventDisableTiming);
-        if (e != cudaSuccess) return fail(JV_ECUDA, std::string("batch stream: ") + cudaGetErrorString(e));
+    {
+        jv_status st = ensure_copy_stream(c);
+        if (st != JV_OK) return st;
     }
     // shot k's traces go to buffer k % 2 on the copy stream; buffer k % 2
     // is free once shot k - 2 has finished, which jv_rtm_shot waits for
@@ -468,10 +488,8 @@ jv_status jv_rtm_batch(jv_ctx *c, int n, const int *shots, const float *const *o
     for (int k = 0; k < n && st == JV_OK; k++) {
         if (k + 1 < n) st = issue(k + 1);
         if (st != JV_OK) break;
-        st = ret(c->eng->wait_event(c->ev_copy[k % 2]));
-        if (st != JV_OK) break;
         float *d = c->d_tr[k % 2];
-        st = ret(c->eng->rtm_shot(shots[k], d, d + per, d + 2 * per));
+        st = ret(c->eng->rtm_shot(shots[k], d, d + per, d + 2 * per, c->ev_copy[k % 2]));
         total += c->eng->last_ms();
     }
     cudaStreamSynchronize(c->copy_stream);

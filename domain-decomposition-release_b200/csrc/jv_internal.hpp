@@ -214,11 +214,12 @@ struct KCfg {
 };
 
 // kernels.cu ------------------------------------------------------------
-int k_model_prep(const GridDev &g, const float *d_vp_phy, const float *d_vs_phy, const float *d_rho_phy,
-                 float *vp, float *rho, float *lam, float *mu, void *stream);
+// vp, dt / rho (the velocity update's density term), lambda, mu on gridext
+int k_model_prep(const GridDev &g, const float *d_vp_phy, const float *d_vs_phy, const float *d_rho_phy, float dt,
+                 float *vp, float *bdt, float *lam, float *mu, void *stream);
 int k_zero_range(float *p, size_t n, void *stream);
 
-int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w,
+int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *bdt, float dt, int rec_w,
               const WaveDev *rev, const ImageDev *img, const KCfg &kc, void *stream);
 
 // it_off: the kernels of a step read the time step as st->it + it_off (a
@@ -240,7 +241,7 @@ int k_make_wave_maps(const GridDev &g, const WaveDev &w, const float *lam, const
 // row of more than 512 threads or a halo row wider than 256 floats, the
 // driver entry point missing).  Returns a cudaError_t.
 int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
-                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, int chunks,
+                     const float *bdt, float4 *const ax[3], float *psi, int *err_flag, int chunks,
                      FullMaps *maps);
 // Stress update of every updated cell of gridext, interior and absorbing
 // layers in one launch (modes kFwd, kRtmFwd, kRev).
@@ -248,7 +249,7 @@ int k_stress_full(int mode, const GridDev &g, const WaveDev &w, float dt, const 
                   int it_off, const FullMaps &maps, void *stream);
 // Velocity update of every updated cell of gridext (variant 4; vx, vy, vz)
 int k_vel_full(const GridDev &g, const WaveDev &w, float dt, const FullMaps &maps, void *stream);
-int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
+int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *bdt, const float *vp,
               const KCfg &kc, void *stream);
 int k_stress_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *lam, const float *mu,
                  const float *vp, int with_sau, const KCfg &kc, void *stream);

@@ -75,8 +75,12 @@ __device__ __forceinline__ int rim_order(int p, int np, int w) {
     return e < w ? w : e + 1;
 }
 
+// dt / rho of a cell for a step of signed length dt, from the stored
+// |dt| / rho (model_prep)
+__device__ __forceinline__ float signed_bdt(float b, float dt) { return dt < 0.f ? -b : b; }
+
 template <int MODE, bool IMG>
-__global__ void __launch_bounds__(kTX *kTY) vel_phy(GridDev g, WaveDev w, const float *__restrict__ rho, float dt,
+__global__ void __launch_bounds__(kTX *kTY) vel_phy(GridDev g, WaveDev w, const float *__restrict__ bdt, float dt,
                                                    int rec_w, WaveDev rv, ImageDev img) {
     const int pi = blockIdx.x * kTX + threadIdx.x;
     const int pj = blockIdx.y * kTY + threadIdx.y;
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(kTX *kTY) vel_phy(GridDev g, WaveDev w, const 
             sau_z = dp<4>(sau, i, sz, c);
         }
     }
-    const float dtr = dt / ld(rho, i);
+    const float dtr = signed_bdt(ld(bdt, i), dt);
     const float a = dtr / g.dx, b = dtr / g.dy, c = dtr / g.dz;
     const float vx = w.f[VX][i] + (a * sxx_x + b * sxy_y + c * sxz_z);
     const float vy = w.f[VY][i] + (a * syx_x + b * syy_y + c * syz_z);
@@ -238,7 +242,7 @@ __device__ __forceinline__ float win_dm(const float *w, const float *c, int o) {
 }
 
 template <int MODE, bool IMG>
-__global__ void __launch_bounds__(kTX *kTY) vel_phy_zm(GridDev g, WaveDev w, const float *__restrict__ rho, float dt,
+__global__ void __launch_bounds__(kTX *kTY) vel_phy_zm(GridDev g, WaveDev w, const float *__restrict__ bdt, float dt,
                                                       int rec_w, WaveDev rv, ImageDev img, int zc) {
     const int pi = blockIdx.x * kTX + threadIdx.x;
     const int pj = blockIdx.y * kTY + threadIdx.y;
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(kTX *kTY) vel_phy_zm(GridDev g, WaveDev w, con
         const float syz_z = win_dm(wyz, cz, oz);
         const float szz_z = win_dp(wzz, cz, oz);
         const float sau_z = kP ? win_dp(wau, cz, oz) : 0.f;
-        const float dtr = dt / ld(rho, i);
+        const float dtr = signed_bdt(ld(bdt, i), dt);
         const float a = dtr / g.dx, b = dtr / g.dy, c = dtr / g.dz;
         const float vx = w.f[VX][i] + (a * sxx_x + b * sxy_y + c * sxz_z);
         const float vy = w.f[VY][i] + (a * syx_x + b * syy_y + c * syz_z);
@@ -520,7 +524,7 @@ __device__ __forceinline__ void st4(float *f, int i0, const float *v, int nvalid
 // v[3][4] and, for the modes that carry them, the P-wave velocities in
 // p[3][4].
 template <int MODE>
-__device__ __forceinline__ void vel_update4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
+__device__ __forceinline__ void vel_update4(const GridDev &g, const WaveDev &w, const float *__restrict__ bdt,
                                             float dt, int rec_w, int pi0, int pj, int pk, float v[3][4],
                                             float p[3][4]) {
     constexpr bool kP = (MODE == kBwd || MODE == kRev);
@@ -569,8 +573,20 @@ __device__ __forceinline__ void vel_update4(const GridDev &g, const WaveDev &w, 
 
     float dtr[4];
     {
-        const float4 r4 = ld4(rho, i0);
-        dtr[0] = dt / r4.x; dtr[1] = dt / r4.y; dtr[2] = dt / r4.z; dtr[3] = dt / r4.w;
+        const float4 r4 = ld4(bdt, i0);
+        if (MODE == kBwd) {
+            // -b as b / -1 (exact): the backward update carries the imaging
+            // and runs at the 64-register cap, and with the division in place
+            // of a select ptxas keeps the schedule that spills least (24
+            // against 44 bytes; 255 against 267 us on cfg2)
+            float sg = dt < 0.f ? -1.0f : 1.0f;
+            asm("mov.b32 %0, %0;" : "+f"(sg));
+            dtr[0] = __fdiv_rn(r4.x, sg); dtr[1] = __fdiv_rn(r4.y, sg);
+            dtr[2] = __fdiv_rn(r4.z, sg); dtr[3] = __fdiv_rn(r4.w, sg);
+        } else {
+            dtr[0] = signed_bdt(r4.x, dt); dtr[1] = signed_bdt(r4.y, dt);
+            dtr[2] = signed_bdt(r4.z, dt); dtr[3] = signed_bdt(r4.w, dt);
+        }
     }
     f4a(v[0], ldw4(w.f[VX], i0));
     f4a(v[1], ldw4(w.f[VY], i0));
@@ -662,11 +678,11 @@ __device__ __forceinline__ void pf_l2(const float *f, int i) {
 // left out: their prefetch addresses spill at 64 registers and cost more
 // than they gain (337 us).
 template <int MODE>
-__device__ __forceinline__ void vel_prefetch4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
+__device__ __forceinline__ void vel_prefetch4(const GridDev &g, const WaveDev &w, const float *__restrict__ bdt,
                                               int i0) {
     constexpr bool kP = (MODE == kBwd || MODE == kRev);
     const int sz = (int)g.sz;
-    pf_l2(rho, i0);
+    pf_l2(bdt, i0);
     pf_l2(w.f[VX], i0);
     pf_l2(w.f[VY], i0);
     pf_l2(w.f[VZ], i0);
@@ -688,13 +704,13 @@ __device__ __forceinline__ void vel_prefetch4(const GridDev &g, const WaveDev &w
 // backward update) the imaging condition against the receiver wavefield rv
 // follows.
 template <int MODE, bool IMG>
-__device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ rho,
+__device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, const float *__restrict__ bdt,
                                            float dt, int rec_w, const WaveDev &rv, const ImageDev &img, int pi0,
                                            int pj, int pk) {
     const int i0 = (int)g.xoff + (pi0 + g.m) + (int)g.sy * (pj + g.m) + (int)g.sz * (pk + g.m);
-    vel_prefetch4<MODE>(g, w, rho, i0);
+    vel_prefetch4<MODE>(g, w, bdt, i0);
     float v[3][4], p[3][4];
-    vel_update4<MODE>(g, w, rho, dt, rec_w, pi0, pj, pk, v, p);
+    vel_update4<MODE>(g, w, bdt, dt, rec_w, pi0, pj, pk, v, p);
     if (IMG) {
         float r[3][4], rp[3][4];
         f4a(r[0], ld4(rv.f[VX], i0));
@@ -710,7 +726,7 @@ __device__ __forceinline__ void vel_group4(const GridDev &g, const WaveDev &w, c
 // Blocks of blockDim.x groups x blockDim.y rows x ZP planes; a thread
 // updates its group in ZP consecutive planes.
 template <int MODE, bool IMG, int MINB, int ZP>
-__global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ rho,
+__global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, const float *__restrict__ bdt,
                                                        float dt, int rec_w, WaveDev rv, ImageDev img) {
     const int pi0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int pj = blockIdx.y * blockDim.y + threadIdx.y;
@@ -718,7 +734,7 @@ __global__ void __launch_bounds__(256, MINB) vel_phy_v4(GridDev g, WaveDev w, co
 #pragma unroll
     for (int zz = 0; zz < ZP; zz++) {
         const int pk = blockIdx.z * ZP + zz;
-        if (pk < g.pz) vel_group4<MODE, IMG>(g, w, rho, dt, rec_w, rv, img, pi0, pj, pk);
+        if (pk < g.pz) vel_group4<MODE, IMG>(g, w, bdt, dt, rec_w, rv, img, pi0, pj, pk);
     }
 }
 
@@ -1299,7 +1315,7 @@ __device__ __forceinline__ void xcoef4(const CpmlDev &P, const PmlPos &q, float 
 // variables on the absorbing axes (z-slabs x,y,z; y-slabs x,y; x-slabs x)
 // (FD/fdtd3d_1_cpml_mpi_module/fdtd3d_cpml_mpi_2_kernel_device_{x,y,z}_meat.hpp)
 __device__ __forceinline__ void vel_pml_group(const GridDev &g, const CpmlDev &P, const WaveDev &w,
-                                              const float *__restrict__ rho, const float *__restrict__ vpm,
+                                              const float *__restrict__ bdt, const float *__restrict__ vpm,
                                               const PmlPos &q) {
     const int sy = (int)g.sy, sz = (int)g.sz;
     const int i0 = (int)g.xoff + q.xs + sy * q.y + sz * q.z;
@@ -1308,7 +1324,7 @@ __device__ __forceinline__ void vel_pml_group(const GridDev &g, const CpmlDev &P
         // vel_prefetch4: pointwise arrays, fields read in their own plane, the
         // leading plane of each z difference, and the memory variables of the
         // axes on which the group absorbs
-        pf_l2(rho, i0);
+        pf_l2(bdt, i0);
         pf_l2(vpm, i0);
         pf_l2(w.f[VX], i0);
         pf_l2(w.f[VY], i0);
@@ -1384,11 +1400,8 @@ __device__ __forceinline__ void vel_pml_group(const GridDev &g, const CpmlDev &P
         psi4(psi + 7 * n, B, A, syz_z);
         psi4(psi + 8 * n, Bh, Ah, szz_z);
     }
-    float r4[4], v[4];
-    f4a(r4, ld4(rho, i0));
-    float dtr[4];
-#pragma unroll
-    for (int c = 0; c < 4; c++) dtr[c] = P.dt / r4[c];
+    float dtr[4], v[4];
+    f4a(dtr, ld4(bdt, i0));  // P.dt > 0
     f4a(v, ldw4(w.f[VX], i0));
 #pragma unroll
     for (int c = 0; c < 4; c++) v[c] += dtr[c] * (sxx_x[c] + sxy_y[c] + sxz_z[c]);
@@ -1500,14 +1513,14 @@ __device__ __forceinline__ void stress_pml_group(const GridDev &g, const CpmlDev
 // Blocks of 256 threads over (slab, row block, plane block); a thread
 // updates its group in P.zp consecutive planes of its slab.
 template <int MINB, int ZP>
-__global__ void __launch_bounds__(256, MINB) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ rho,
+__global__ void __launch_bounds__(256, MINB) vel_pml(GridDev g, CpmlDev P, WaveDev w, const float *__restrict__ bdt,
                                                   const float *__restrict__ vpm) {
     PmlPos q;
     if (!pml_pos(P, q)) return;
 #pragma unroll
     for (int zz = 0; zz < ZP; zz++) {
         if (q.z >= q.z1) break;
-        vel_pml_group(g, P, w, rho, vpm, q);
+        vel_pml_group(g, P, w, bdt, vpm, q);
         q.z++;
         q.psi += q.plane;
     }
@@ -2047,7 +2060,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
 // z-marching kernel, with the tiling, thread layout, run schedule and
 // axis-major memory variables of stress_fz.  Per item TMA brings halo
 // planes (12 rows) of sxy, syy, syz; 4-row bands with the x halo of sxx
-// and sxz; the core tiles of rho, vp, vx, vy, vz; the window feed of sxz,
+// and sxz; the core tiles of dt/rho, vp, vx, vy, vz; the window feed of sxz,
 // syz, szz five planes ahead; the memory-variable boxes.  The z windows
 // hold sxz, syz, szz.  It serves the passes without P-wave velocities
 // (forward modelling, the RTM forward pass) on grids of one x tile; the
@@ -2059,7 +2072,7 @@ constexpr int kFvStage = 3 * kZmHB + 10 * kZmCB;  // halo planes, 2 bands, 5 cor
 struct FvMaps {
     CUtensorMap halo[3];  // sxy syy syz
     CUtensorMap band[2];  // sxx sxz
-    CUtensorMap core[5];  // rho vp vx vy vz
+    CUtensorMap core[5];  // dt/rho vp vx vy vz
     CUtensorMap feed[3];  // sxz syz szz (core boxes)
     CUtensorMap psi[3];
 };
@@ -2198,7 +2211,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
         if (live) {
             const float *H = base;                  // halo planes: sxy, syy, syz
             const float *BD = base + 3 * hb;         // bands: sxx, sxz
-            const float *C = base + 3 * hb + 2 * cb; // core: rho, vp, vx, vy, vz
+            const float *C = base + 3 * hb + 2 * cb; // core: dt/rho, vp, vx, vy, vz
             const float *FD = base + 3 * hb + 7 * cb;
             const int c0 = (r + kZmHalo) * boxw + hcol;  // a halo plane
             const int b0 = r * boxw + hcol;              // a band
@@ -2396,7 +2409,7 @@ __global__ void __launch_bounds__(kZmMaxThreads, 1)
                 }
             }
             const float2 rh = ld2(C, cc);
-            const float dtr[2] = {dt / rh.x, dt / rh.y};
+            const float dtr[2] = {signed_bdt(rh.x, dt), signed_bdt(rh.y, dt)};
             const float2 v0 = ld2(C, 2 * cb + cc), v1 = ld2(C, 3 * cb + cc), v2 = ld2(C, 4 * cb + cc);
             *reinterpret_cast<float2 *>(w.f[VX] + i0) = make_float2(v0.x + dtr[0] * Dx[0], v0.y + dtr[1] * Dx[1]);
             *reinterpret_cast<float2 *>(w.f[VY] + i0) = make_float2(v1.x + dtr[0] * Dy[0], v1.y + dtr[1] * Dy[1]);
@@ -2602,9 +2615,13 @@ __global__ void count_nonfinite_d(const double *p, size_t n, unsigned long long 
 // gridext model: nearest-cell extension of gridphy (the 26 regions of
 // FD/fdtd3d_0_base_module/fdtd3d_base_3_geomodel_meat.hpp:101-364) and
 // lambda = rho (vp^2 - 2 vs^2), mu = rho vs^2 with the reference's
-// float operation order (:454-460).
+// float operation order (:454-460).  Density enters the velocity update
+// only as dt / rho, so that quotient is stored (bdt, for dt > 0): the
+// velocity kernels take it, negated for the backward update, in place of a
+// division per cell and step.  IEEE division is sign-symmetric, so
+// -(dt / rho) equals (-dt) / rho bit for bit.
 __global__ void model_prep(GridDev g, const float *__restrict__ vp0, const float *__restrict__ vs0,
-                           const float *__restrict__ rho0, float *vp, float *rho, float *lam, float *mu) {
+                           const float *__restrict__ rho0, float dt, float *vp, float *bdt, float *lam, float *mu) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     const int z = blockIdx.z;
@@ -2616,7 +2633,7 @@ __global__ void model_prep(GridDev g, const float *__restrict__ vp0, const float
     const long long i = g.xoff + x + g.sy * y + g.sz * z;
     const float a = vp0[s], b = vs0[s], r = rho0[s];
     vp[i] = a;
-    rho[i] = r;
+    bdt[i] = __fdiv_rn(dt, r);
     const float b2 = __fmul_rn(b, b);
     lam[i] = __fmul_rn(r, __fsub_rn(__fmul_rn(a, a), __fmul_rn(2.0f, b2)));
     mu[i] = __fmul_rn(r, b2);
@@ -2672,10 +2689,10 @@ int upload_coefficients(const float list[5][4], const float dc2[2]) {
     return (int)cudaMemcpyToSymbol(c_dc2, dc2, sizeof(float) * 2);
 }
 
-int k_model_prep(const GridDev &g, const float *vp0, const float *vs0, const float *rho0, float *vp, float *rho,
-                 float *lam, float *mu, void *stream) {
+int k_model_prep(const GridDev &g, const float *vp0, const float *vs0, const float *rho0, float dt, float *vp,
+                 float *bdt, float *lam, float *mu, void *stream) {
     dim3 b(128), gr((g.nx + 127) / 128, g.ny, g.nz);
-    model_prep<<<gr, b, 0, (cudaStream_t)stream>>>(g, vp0, vs0, rho0, vp, rho, lam, mu);
+    model_prep<<<gr, b, 0, (cudaStream_t)stream>>>(g, vp0, vs0, rho0, dt, vp, bdt, lam, mu);
     return cerr();
 }
 
@@ -2709,15 +2726,15 @@ static void v4_shape(const GridDev &g, const KCfg &kc, dim3 *b, dim3 *gr) {
 
 template <int MINB, int ZP>
 static int launch_vel_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const GridDev &g, const WaveDev &w,
-                         const float *rho, float dt, int rec_w, const WaveDev *rev, const ImageDev *img,
+                         const float *bdt, float dt, int rec_w, const WaveDev *rev, const ImageDev *img,
                          const WaveDev &rv, const ImageDev &im) {
     switch (mode) {
-    case kFwd: vel_phy_v4<kFwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-    case kRtmFwd: vel_phy_v4<kRtmFwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-    case kRev: vel_phy_v4<kRev, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kFwd: vel_phy_v4<kFwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im); break;
+    case kRtmFwd: vel_phy_v4<kRtmFwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im); break;
+    case kRev: vel_phy_v4<kRev, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im); break;
     case kBwd:
-        if (img && rev) vel_phy_v4<kBwd, true, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
-        else vel_phy_v4<kBwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        if (img && rev) vel_phy_v4<kBwd, true, MINB, ZP><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im);
+        else vel_phy_v4<kBwd, false, MINB, ZP><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im);
         break;
     default: return (int)cudaErrorInvalidValue;
     }
@@ -2738,7 +2755,7 @@ static int launch_stress_v4(int mode, dim3 gr, dim3 b, cudaStream_t s, const Gri
     return cerr();
 }
 
-int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, float dt, int rec_w, const WaveDev *rev,
+int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *bdt, float dt, int rec_w, const WaveDev *rev,
               const ImageDev *img, const KCfg &kc, void *stream) {
     cudaStream_t s = (cudaStream_t)stream;
     WaveDev rv = rev ? *rev : WaveDev{};
@@ -2747,22 +2764,22 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
         dim3 b, gr;
         v4_shape(g, kc, &b, &gr);
         if (kc.zp == 2) {
-            if (kc.minb == 4) return launch_vel_v4<4, 2>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
-            return launch_vel_v4<3, 2>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+            if (kc.minb == 4) return launch_vel_v4<4, 2>(mode, gr, b, s, g, w, bdt, dt, rec_w, rev, img, rv, im);
+            return launch_vel_v4<3, 2>(mode, gr, b, s, g, w, bdt, dt, rec_w, rev, img, rv, im);
         }
-        if (kc.minb == 4) return launch_vel_v4<4, 1>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
-        return launch_vel_v4<3, 1>(mode, gr, b, s, g, w, rho, dt, rec_w, rev, img, rv, im);
+        if (kc.minb == 4) return launch_vel_v4<4, 1>(mode, gr, b, s, g, w, bdt, dt, rec_w, rev, img, rv, im);
+        return launch_vel_v4<3, 1>(mode, gr, b, s, g, w, bdt, dt, rec_w, rev, img, rv, im);
     }
     if (kc.variant == 1) {
         const int zc = kc.zchunk > 0 ? kc.zchunk : g.pz;
         dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, (g.pz + zc - 1) / zc);
         switch (mode) {
-        case kFwd: vel_phy_zm<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc); break;
-        case kRtmFwd: vel_phy_zm<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc); break;
-        case kRev: vel_phy_zm<kRev, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc); break;
+        case kFwd: vel_phy_zm<kFwd, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im, zc); break;
+        case kRtmFwd: vel_phy_zm<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im, zc); break;
+        case kRev: vel_phy_zm<kRev, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im, zc); break;
         case kBwd:
-            if (img && rev) vel_phy_zm<kBwd, true><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc);
-            else vel_phy_zm<kBwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im, zc);
+            if (img && rev) vel_phy_zm<kBwd, true><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im, zc);
+            else vel_phy_zm<kBwd, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im, zc);
             break;
         default: return (int)cudaErrorInvalidValue;
         }
@@ -2770,12 +2787,12 @@ int k_vel_phy(int mode, const GridDev &g, const WaveDev &w, const float *rho, fl
     }
     dim3 b(kTX, kTY), gr((g.px + kTX - 1) / kTX, (g.py + kTY - 1) / kTY, g.pz);
     switch (mode) {
-    case kFwd: vel_phy<kFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-    case kRtmFwd: vel_phy<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
-    case kRev: vel_phy<kRev, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im); break;
+    case kFwd: vel_phy<kFwd, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im); break;
+    case kRtmFwd: vel_phy<kRtmFwd, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im); break;
+    case kRev: vel_phy<kRev, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im); break;
     case kBwd:
-        if (img && rev) vel_phy<kBwd, true><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
-        else vel_phy<kBwd, false><<<gr, b, 0, s>>>(g, w, rho, dt, rec_w, rv, im);
+        if (img && rev) vel_phy<kBwd, true><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im);
+        else vel_phy<kBwd, false><<<gr, b, 0, s>>>(g, w, bdt, dt, rec_w, rv, im);
         break;
     default: return (int)cudaErrorInvalidValue;
     }
@@ -2869,7 +2886,7 @@ long long fz_psi_floats(const GridDev &g) {
 }
 
 int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const float *mu, const float *vp,
-                     const float *rho, float4 *const ax[3], float *psi, int *err_flag, int chunks,
+                     const float *bdt, float4 *const ax[3], float *psi, int *err_flag, int chunks,
                      FullMaps *maps) {
     maps->ok = false;
     const int m = g.m, xoff = (int)g.xoff;
@@ -3003,7 +3020,7 @@ int k_make_full_maps(const GridDev &g, const WaveDev &w, const float *lam, const
     // the velocity kernel's field boxes
     const cuuint32_t bbox[3] = {(cuuint32_t)kZmPitch, (cuuint32_t)kZmRows, 1};
     const int vh[3] = {SXY, SYY, SYZ}, vb[2] = {SXX, SXZ}, vf[3] = {SXZ, SYZ, SZZ};
-    const float *vc[5] = {rho, vp, w.f[VX], w.f[VY], w.f[VZ]};
+    const float *vc[5] = {bdt, vp, w.f[VX], w.f[VY], w.f[VZ]};
     for (int f = 0; f < 3; f++)
         if (!make(w.f[vh[f]], 3, fd, hbox, &maps->vhalo[f]) || !make(w.f[vf[f]], 3, fd, cbox, &maps->vfeed[f]))
             return 0;
@@ -3138,17 +3155,17 @@ int k_stress_phy(int mode, const GridDev &g, const WaveDev &w, const float *lam,
     return cerr();
 }
 
-int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *rho, const float *vp,
+int k_vel_pml(const GridDev &g, const CpmlDev &c, const WaveDev &w, const float *bdt, const float *vp,
               const KCfg &kc, void *stream) {
     if (c.nblocks <= 0) return 0;
     const unsigned blocks = (unsigned)c.nblocks;
     cudaStream_t s = (cudaStream_t)stream;
     if (c.zp == 2) {
-        if (kc.pml_minb == 4) vel_pml<4, 2><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
-        else vel_pml<3, 2><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+        if (kc.pml_minb == 4) vel_pml<4, 2><<<blocks, 256, 0, s>>>(g, c, w, bdt, vp);
+        else vel_pml<3, 2><<<blocks, 256, 0, s>>>(g, c, w, bdt, vp);
     } else {
-        if (kc.pml_minb == 4) vel_pml<4, 1><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
-        else vel_pml<3, 1><<<blocks, 256, 0, s>>>(g, c, w, rho, vp);
+        if (kc.pml_minb == 4) vel_pml<4, 1><<<blocks, 256, 0, s>>>(g, c, w, bdt, vp);
+        else vel_pml<3, 1><<<blocks, 256, 0, s>>>(g, c, w, bdt, vp);
     }
     return cerr();
 }

@@ -216,8 +216,8 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
     if (psi_total) NA_CK(cudaMemsetAsync(psi, 0, (size_t)psi_total * sizeof(float), s));
 
     float *mb = model + guard;
-    float *vp = mb, *rho = mb + fe, *lam = mb + 2 * fe, *mu = mb + 3 * fe;
-    NA_CK(k_model_prep(g, d_vp, d_vs, d_rho, vp, rho, lam, mu, s));
+    float *vp = mb, *bdt = mb + fe, *lam = mb + 2 * fe, *mu = mb + 3 * fe;
+    NA_CK(k_model_prep(g, d_vp, d_vs, d_rho, dt, vp, bdt, lam, mu, s));
     WaveDev w{};
     for (int f = 0; f < 9; f++) w.f[f] = wave + guard + f * fe;
     for (int a = 0; a < 3; a++) cp.ax[a] = tabs[a];
@@ -225,8 +225,8 @@ extern "C" jv_status jv_forward_noalloc(const jv_grid *grid, const float *d_vp, 
     KCfg kc;
     kc.variant = 2;
     for (int it = 0; it < nt; it++) {
-        NA_CK(k_vel_pml(g, cp, w, rho, vp, kc, s));
-        NA_CK(k_vel_phy(kFwd, g, w, rho, dt, 1, nullptr, nullptr, kc, s));
+        NA_CK(k_vel_pml(g, cp, w, bdt, vp, kc, s));
+        NA_CK(k_vel_phy(kFwd, g, w, bdt, dt, 1, nullptr, nullptr, kc, s));
         NA_CK(k_stress_pml(g, cp, w, lam, mu, vp, 0, kc, s));
         NA_CK(k_stress_phy(kFwd, g, w, lam, mu, dt, 1, wavelet, state, 0, kc, s));
         NA_CK(k_record(w, rec_d, (int)rec.size(), nt, state, 0, s));

@@ -154,6 +154,7 @@ struct jv_server {
     std::vector<std::thread> workers;
     std::vector<double> latencies_ms;
     long long n_completed = 0, n_failed = 0, n_cancelled = 0, n_reused = 0;
+    double device_ms = 0.0;  // device time of the completed requests' propagations
     std::list<Idle> idle;  // pooled contexts, most recently used first
     bool threshold_set = false;
 };
@@ -257,6 +258,8 @@ void worker_main(jv_server *s) {
         for (jv_ctx *c : evict) jv_close(c);  // their memory returns before the new context allocates
         jv_status st = run_request(s->device, q, &ctx);
         const std::string msg = st == JV_OK ? std::string() : jv_last_error();
+        double dev_ms = 0.0;
+        if (st == JV_OK) jv_last_timing(ctx, &dev_ms);
         if (st != JV_OK && ctx) {
             jv_close(ctx);  // a failed context is not pooled
             ctx = nullptr;
@@ -281,6 +284,7 @@ void worker_main(jv_server *s) {
                     s->latencies_ms.erase(s->latencies_ms.begin(), s->latencies_ms.begin() + kLatencyWindow / 2);
                 s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count());
                 s->n_completed++;
+                s->device_ms += dev_ms;
             } else {
                 s->n_failed++;
             }
@@ -442,6 +446,7 @@ jv_status jv_server_get_stats(jv_server *s, jv_server_stats *out) {
     out->bytes_in_use = s->in_use;
     out->reused = s->n_reused;
     out->pooled = (long long)s->idle.size();
+    out->device_ms = s->device_ms;
     out->budget = s->budget;
     jv::set_last_error("");
     return JV_OK;

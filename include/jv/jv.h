@@ -385,6 +385,11 @@ typedef struct jv_server_stats {
     size_t bytes_in_use, budget;    /* running requests and pooled idle contexts */
     long long reused;               /* requests that ran on a pooled context      */
     long long pooled;               /* idle contexts pooled now                   */
+    double device_ms;               /* device time of the completed requests'
+                                       propagations (CUDA events on each
+                                       context's stream, summed); with one slot,
+                                       against the wall time, how busy the
+                                       requests kept the GPU                     */
 } jv_server_stats;
 /* Device bytes a context holds for one request of this size with n_recv
  * receivers and an FP32 boundary store (an estimate from the layout; the
