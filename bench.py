@@ -870,6 +870,11 @@ def main():
         # the eight finalized images land in pinned host buffers, reused per shot
         himg = torch.empty((8, s.nz, s.ny, s.nx), dtype=torch.float32, pin_memory=True)
         hout = [himg[q].numpy() for q in range(8)]
+        # one untimed shot through the host path first: its first call sets up
+        # the device trace buffer, the copy stream and the finalize buffer once
+        # per context (about 0.3 s on cfg2), as the timed loop's warm-up does
+        ctx.rtm_shot(0, hobs)
+        ctx.finalize(out=hout)
         barrier()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):

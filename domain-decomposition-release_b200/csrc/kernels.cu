@@ -747,6 +747,20 @@ __device__ __forceinline__ void stress_group4(const GridDev &g, const WaveDev &w
     const int nvalid = min(4, g.px - pi0);
     const int sy = (int)g.sy, sz = (int)g.sz;
     const int i0 = (int)g.xoff + (pi0 + g.m) + sy * (pj + g.m) + sz * (pk + g.m);
+    // the group's DRAM-new lines, as in vel_prefetch4: the pointwise model
+    // and stress arrays, and the leading plane of each z stencil
+    pf_l2(lam, i0);
+    pf_l2(mu, i0);
+    pf_l2(w.f[SXX], i0);
+    pf_l2(w.f[SYY], i0);
+    pf_l2(w.f[SZZ], i0);
+    pf_l2(w.f[SXY], i0);
+    pf_l2(w.f[SXZ], i0);
+    pf_l2(w.f[SYZ], i0);
+    if (MODE != kFwd) pf_l2(w.f[SAU], i0);
+    pf_l2(w.f[VX], i0 + 4 * sz);
+    pf_l2(w.f[VY], i0 + 4 * sz);
+    pf_l2(w.f[VZ], i0 + 3 * sz);
     const float *cx[4];
     xcoefs<MODE>(pi0, g.px, rec_w, cx);
     const float *cy = scoef<MODE>(pj, g.py, rec_w);
