@@ -149,3 +149,30 @@ def test_stream_probe_rejects_bad_arguments_without_device():
         assert L.jv_stream_probe(0, nr, nw, n, reps, C.byref(g)) == jv.JV_EINVAL
     assert L.jv_stream_probe(0, 1, 1, 1024, 1, None) == jv.JV_EINVAL
     assert b"(25,11)" in L.jv_last_error() or b"bad argument" in L.jv_last_error()
+
+
+def test_python_structs_match_the_header(tmp_path):
+    """Every ctypes mirror of a jv.h struct has the C layout: the size and
+    each field's offset, from a C program compiled against the header."""
+    jv = pkg()
+    mirrors = {"jv_grid": jv.Grid, "jv_options": jv.Options, "jv_job": jv.Job, "jv_request": jv.Request,
+               "jv_server_stats": jv.ServerStats, "jv_argfile": jv.ArgFileC, "jv_frame": jv.Frame,
+               "jv_info": jv.Info}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "jv/jv.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'    printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'    printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, key, val = ln.split()
+        got[(cname, key)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)

@@ -63,6 +63,8 @@ def test_mixed_requests_match_each_run_alone():
     assert st["running"] == 0 and st["queued"] == 0
     assert 0 < st["bytes_in_use"] <= st["budget"] and st["pooled"] >= 1  # idle contexts stay pooled
     assert 0 < st["p50_ms"] <= st["p99_ms"] and st["mean_ms"] > 0
+    # each request's device time lies inside its submission-to-completion time
+    assert 0 < st["device_ms"] <= st["mean_ms"] * st["completed"]
 
 
 def _same_grid_models(k):
