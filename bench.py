@@ -772,6 +772,7 @@ def main():
     ctx.set_geometry(np.repeat(s.shots[:1], n_job, axis=0), s.recvs)
     mine = rep.shard_shots(n_job, rank, world)
     info = ctx.info()
+    kcfg = ctx.kernel_config()  # the knobs the context's creation-time timing chose
     nrec, nt = info.n_recv, info.nt
     obs = torch.empty((3, nrec, nt), dtype=torch.float32, device=f"cuda:{local}")
     ptrs = [obs[i].data_ptr() for i in range(3)]
@@ -973,6 +974,8 @@ def main():
                    "job": f"{n_job} shots at the survey's source position, shot s on rank s % {world}",
                    "parallelism": f"shot replicas x{world}" if world > 1 else "single GPU",
                    "boundary_store": args.store,
+                   "kernel_choice": {k: kcfg[k] for k in ("kernel_variant", "run_chunks", "tile_gx", "tile_gy",
+                                                          "min_blocks", "planes_per_thread", "autotune")},
                    "l2": "inputs larger than L2 (each wavefield set > 700 MB)"},
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "accuracy": accuracy, "modes": modes, "serving": serving,
         "batched_config": batched_cfg,
